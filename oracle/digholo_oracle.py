@@ -1,0 +1,589 @@
+"""FP64 numpy restatement of digHolo's batch-processing path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: it may be imported by
+tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, never by the
+digholo_b200 product.
+
+Parity status: pinned against the reference itself.  oracle/Makefile builds
+the unmodified reference (digHolo.cpp) into oracle/_ref, and
+tests/test_oracle_pin.py runs both on the same synthetic holograms (and on the
+committed fixtures in tests/golden/, generated by tests/golden/make_golden.py
+from that build).  The reference ships no golden vectors or known-answer
+tests of its own.
+
+It restates, step by step, the work of digHoloProcessBatch
+(digHolo.cpp:4693-4728):
+
+  fft_windows         FFT window snap/clamp           digHolo.cpp:7267-7378
+  k_axes / xy_axes    Fourier and camera axes         digHolo.cpp:2843-2874, 7720-7733
+  ifft_windows        IFFT window bounds              digHolo.cpp:7868-8048
+  ifft_axes           reconstructed-plane axes        digHolo.cpp:8183-8203
+  copy_window         Fourier window copy             digHolo.cpp:1808-2122
+  field_analysis      power / CoM / max / Aeff        digHolo.cpp:2354-2654, 9103-9176
+  reference_wave      separable tilt/defocus wave     digHolo.cpp:10201-10504
+  apply_tilt          -conj(A.ref) and int16 rounding digHolo.cpp:2701-2837
+  hg_basis            int16 HG modes and scales       digHolo.cpp:1269-1484, 10543-10645
+  overlap             separable HG overlap            digHolo.cpp:2149-2341, 9756-9815
+
+Two flavours are produced by :func:`process_batch`:
+
+* ``quantised``: the reference's own storage formats (int16 fields with scale
+  32767/max|E|, 14-bit reference wave, int16 HG modes with per-mode scales),
+  emulating its float32 arithmetic where that decides a rounding;
+* ``exact``: the same mathematics with no quantisation, everything in FP64
+  (the "FP64 oracle" that FP32 GPU results are scored against).
+
+Deliberate difference: the reference applies the overlap's int16->float
+scale only inside its ``pixelIdy == pixelCountY - 16`` branch
+(digHolo.cpp:2318-2331), so when the reconstructed field is exactly 16 rows
+high the scale is never applied and raw integer sums come out.  The
+quantised flavour here applies the scale always; ``reference_unscaled_16``
+reproduces the reference's behaviour for the pinning test.
+"""
+import math
+
+import numpy as np
+
+F32 = np.float32
+PI_F = F32(3.14159265358979323846264338327950288)  # const float pi, digHolo.cpp:89
+PI_D = 3.14159265358979323846264338327950288      # piD, digHolo.cpp:3633
+UNIT_ANGLE = F32(PI_F / F32(180.0))                # DIGHOLO_UNIT_ANGLE (pi/180.0f), digHolo.h:192
+PIXEL_QUANTA = 16
+
+
+class Config:
+    """The fields of digHoloConfig (digHolo.cpp:3323-3372) that the batch path reads."""
+
+    def __init__(self, frame_width=320, frame_height=256, pixel_size=20e-6, pol_count=1,
+                 fft_window=(0, 0), window_radius_deg=0.4, resolution_mode=0,
+                 wavelength=1565e-9, beam_centre=None, tilt_deg=None, defocus=None,
+                 waist=None, max_mg=0, fill_factor=1, pol_lock_tilt=0, pol_lock_defocus=0,
+                 pol_lock_waist=1):
+        self.frame_width = frame_width
+        self.frame_height = frame_height
+        self.pixel_size = F32(pixel_size)
+        self.pol_count = pol_count
+        self.fft_window = fft_window
+        self.window_radius_deg = F32(window_radius_deg)
+        self.resolution_mode = resolution_mode
+        self.wavelength = F32(wavelength)
+        self.beam_centre = [[F32(0), F32(0)], [F32(0), F32(0)]] if beam_centre is None else \
+            [[F32(v) for v in bc] for bc in beam_centre]
+        self.tilt_deg = [[F32(-0.75), F32(0.75)], [F32(-0.75), F32(0.75)]] if tilt_deg is None else \
+            [[F32(v) for v in t] for t in tilt_deg]
+        self.defocus = [F32(0), F32(0)] if defocus is None else [F32(v) for v in defocus]
+        self.waist = [F32(510), F32(510)] if waist is None else [F32(v) for v in waist]
+        self.max_mg = max_mg
+        self.fill_factor = fill_factor
+        self.pol_lock_tilt = pol_lock_tilt
+        self.pol_lock_defocus = pol_lock_defocus
+        self.pol_lock_waist = pol_lock_waist
+        while len(self.beam_centre) < 2:
+            self.beam_centre.append([F32(0), F32(0)])
+        while len(self.tilt_deg) < 2:
+            self.tilt_deg.append([F32(-0.75), F32(0.75)])
+        while len(self.defocus) < 2:
+            self.defocus.append(F32(0))
+        while len(self.waist) < 2:
+            self.waist.append(F32(510))
+
+
+def _round_half_away(x):
+    return math.floor(x + 0.5) if x >= 0 else -math.floor(-x + 0.5)
+
+
+def fft_windows(cfg):
+    """FFT window size and per-polarisation corners (digHolo.cpp:7283-7378)."""
+    fx = cfg.fft_window[0] if cfg.fft_window[0] > 0 else cfg.frame_width // cfg.pol_count
+    fy = cfg.fft_window[1] if cfg.fft_window[1] > 0 else cfg.frame_height
+    W = PIXEL_QUANTA * (fx // PIXEL_QUANTA)
+    H = PIXEL_QUANTA * (fy // PIXEL_QUANTA)
+    W = max(W, 16)
+    H = max(H, 16)
+    W = min(W, cfg.frame_width)
+    H = min(H, cfg.frame_height)
+    block = 16  # ALIGN / sizeof(float), digHolo.cpp:7311
+    cxs, cys = [], []
+    for pol in range(cfg.pol_count):
+        bcx = F32(cfg.beam_centre[pol][0])
+        bcy = F32(cfg.beam_centre[pol][1])
+        CX = F32(F32(bcx / cfg.pixel_size) + F32(cfg.frame_width // 2))
+        CY = F32(F32(bcy / cfg.pixel_size) + F32(cfg.frame_height // 2))
+        cx = int(_round_half_away(float(F32(F32(CX - F32(W // 2)) / F32(block))))) * block
+        cy = int(_round_half_away(float(F32(CY - F32(H // 2)))))
+        cx = max(cx, 0)
+        cy = max(cy, 0)
+        if cx + W > cfg.frame_width:
+            cx = cfg.frame_width - W
+        if cy + H > cfg.frame_height:
+            cy = cfg.frame_height - H
+        cxs.append(cx)
+        cys.append(cy)
+    return W, H, cxs, cys
+
+
+def _gen_axis_shifted(n, step):
+    return np.array([F32(step) * F32(i if i <= n // 2 else i - n) for i in range(n)], dtype=F32)
+
+
+def _gen_axis_centred(n, step):
+    return np.array([F32(i - n // 2) * F32(step) for i in range(n)], dtype=F32)
+
+
+def k_axes(W, H, pixel_size):
+    """fftshifted kx, ky axes of the FFT plane (digHolo.cpp:7724-7733)."""
+    period = F32(2.0 * float(pixel_size))
+    kfx = F32(2 * (2.0 * PI_D / float(period)) / W)
+    kfy = F32(2 * (2.0 * PI_D / float(period)) / H)
+    return _gen_axis_shifted(W, kfx), _gen_axis_shifted(H, kfy)
+
+
+def xy_axes(W, H, pixel_size):
+    """Camera-plane axes of the FFT window (digHolo.cpp:7732)."""
+    return _gen_axis_centred(W, pixel_size), _gen_axis_centred(H, pixel_size)
+
+
+def _tilts_rad(cfg):
+    out = []
+    for pol in range(cfg.pol_count):
+        src = 0 if cfg.pol_lock_tilt else pol
+        out.append((F32(cfg.tilt_deg[src][0] * UNIT_ANGLE), F32(cfg.tilt_deg[src][1] * UNIT_ANGLE)))
+    return out
+
+
+def ifft_windows(cfg, W, H, kx, ky):
+    """IFFT window size and corners (digHolo.cpp:7868-8048), single wavelength."""
+    lam = cfg.wavelength
+    k0max = F32(F32(2) * PI_F / lam)
+    k0min = k0max
+    dkx = F32(kx[1] - kx[0])
+    dky = F32(ky[1] - ky[0])
+    r0 = F32(cfg.window_radius_deg * UNIT_ANGLE)
+    tilts = _tilts_rad(cfg)
+    woi_cx, woi_cy, ww, wh = [], [], [], []
+    for pol in range(cfg.pol_count):
+        tx, ty = tilts[pol]
+        maxEX = F32(float(F32(F32(F32(tx + r0) * k0max) / dkx)) + W / 2.0)
+        maxEY = F32(float(F32(F32(F32(ty + r0) * k0max) / dky)) + H / 2.0)
+        minSX = F32(float(F32(F32(F32(tx - r0) * k0min) / dkx)) + W / 2.0)
+        minSY = F32(float(F32(F32(F32(ty - r0) * k0min) / dky)) + H / 2.0)
+        woi_cx.append(int(_round_half_away(float(F32(maxEX + minSX)) / 4.0)) * 2)
+        woi_cy.append(int(_round_half_away(float(F32(maxEY + minSY)) / 4.0)) * 2)
+        wpol = int(F32(F32(maxEX - minSX) + F32(1)))
+        hpol = int(F32(F32(maxEY - minSY) + F32(1)))
+        wpol = int(F32(16) * F32(math.ceil(float(F32(F32(wpol) / F32(16))))))
+        hpol = int(F32(16) * F32(math.ceil(float(F32(F32(hpol) / F32(16))))))
+        ww.append(wpol)
+        wh.append(hpol)
+    w = max(max(ww), 16)
+    h = max(max(wh), 16)
+    sx, sy = [], []
+    for pol in range(cfg.pol_count):
+        nsx = int(woi_cx[pol] - w / 2.0)
+        if nsx < W // 2:
+            nsx = W // 2
+        if nsx < 0:
+            nsx = 0
+        if nsx + w > W:
+            nsx = W - w
+        nsy = int(woi_cy[pol] - h / 2.0)
+        sx.append(nsx)
+        sy.append(nsy)
+    return w, h, sx, sy
+
+
+def ifft_axes(cfg, W, H, w, h):
+    """Axes of the reconstructed plane (digHolo.cpp:8183-8203)."""
+    if cfg.resolution_mode == 0:
+        w, h = W, H
+    psx = F32(F32(cfg.pixel_size * F32(W)) / F32(w))
+    psy = F32(F32(cfg.pixel_size * F32(H)) / F32(h))
+    return _gen_axis_centred(w, psx), _gen_axis_centred(h, psy)
+
+
+def xcsc(x):
+    """x / sin(x), 1 at x = 0 (the inverse pixel sinc, digHolo.cpp:820-866)."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.ones_like(x)
+    nz = x != 0
+    out[nz] = x[nz] / np.sin(x[nz])
+    return out
+
+
+def copy_window(F, cfg, pol, W, H, w, h, SX, SY, cx, cy, kx, ky):
+    """Fourier-window selection for one polarisation (digHolo.cpp:1808-2122).
+
+    F: (..., H, W/2+1) complex R2C planes.  Returns (..., h, w) in low-res
+    mode or (..., H, W) in full-res mode.  Single frame per output
+    (avgCount = 1) and no batch calibration.
+    """
+    lowres = cfg.resolution_mode == 1
+    fw, fh = cfg.frame_width, cfg.frame_height
+    p = cfg.pixel_size
+    cx0 = (cx + W // 2) - fw // 2
+    cy0 = (cy + H // 2) - fh // 2
+    bcx = float(F32(cfg.beam_centre[pol][0] - F32(F32(cx0) * p)))
+    bcy = float(F32(cfg.beam_centre[pol][1] - F32(F32(cy0) * p)))
+    src = 0 if cfg.pol_lock_tilt else pol
+    # digHolo.cpp:8588-8589, 8627-8630 (per-polarisation tilt, sin of the angle)
+    tx = F32(cfg.tilt_deg[pol][0] * UNIT_ANGLE)
+    ty = F32(cfg.tilt_deg[pol][1] * UNIT_ANGLE)
+    del src
+    k0_f = F32(F32(2) * PI_F / cfg.wavelength)
+    kx0_f = F32(k0_f * F32(math.sin(float(tx))))
+    ky0_f = F32(k0_f * F32(math.sin(float(ty))))
+    kr_f = F32(k0_f * F32(math.sin(float(F32(cfg.window_radius_deg * UNIT_ANGLE)))))
+    r02_f = F32(kr_f * kr_f)
+    ifft_len = (w * h) if lowres else (W * H)
+    norm = 1.0 / math.sqrt(float(W * H) * float(ifft_len))
+    shape = F.shape[:-2]
+    out = np.zeros(shape + ((h, w) if lowres else (H, W)), dtype=np.complex128)
+    ky_shift = abs(float(ky[1] - ky[0]) * H)
+    SX0 = SX - W // 2
+    cols = np.arange(w) + SX0
+    kxv = kx[cols].astype(np.float64)
+    sinc_x = xcsc(kxv * (0.5 * float(p))) if cfg.fill_factor else np.ones(w)
+    for j in range(h):
+        jsy = j + SY
+        row = (jsy + H // 2) % H
+        kyv = float(ky[row])
+        shift = ky_shift if jsy < 0 else (-ky_shift if jsy > H else 0.0)
+        # the mask test in float32, as digHolo.cpp:2006-2019 evaluates it
+        dky = F32(F32(ky[row]) - F32(ky0_f + F32(shift)))
+        dkx = (kx[cols] - kx0_f).astype(F32)
+        dr2 = (dkx * dkx).astype(F32) + F32(dky * dky)
+        inside = dr2.astype(F32) <= r02_f
+        env = sinc_x * (xcsc(np.array([kyv * 0.5 * float(p)]))[0] if cfg.fill_factor else 1.0)
+        adj = np.where(inside, norm * env, 0.0) * np.exp(1j * (kxv * bcx + kyv * bcy))
+        vals = F[..., row, cols] * adj
+        if lowres:
+            out[..., j, :] = vals
+        else:
+            out[..., row, cols % W] = vals
+    return out
+
+
+def field_analysis(E, x, y):
+    """Per-field statistics over the whole plane (digHolo.cpp:2354-2654 with
+    windowRadius = 0, aggregated as in digHolo.cpp:9103-9176).
+
+    E: (B, h, w) complex.  Returns a dict of (B+1,) arrays; entry B is the
+    analysis of the intensity summed over the batch.  MAXABS is stored as
+    32767 / max|E| like the reference.
+    """
+    B, ny, nx = E.shape
+    I = (np.abs(E) ** 2) / (nx * ny)
+    Isum = np.cumsum(I, axis=0)[-1:]
+    allI = np.concatenate([I, Isum], axis=0)
+    X = x.astype(np.float64)[None, None, :]
+    Y = y.astype(np.float64)[None, :, None]
+    P = allI.sum(axis=(1, 2))
+    comx = (allI * X).sum(axis=(1, 2)) / P
+    comy = (allI * Y).sum(axis=(1, 2)) / P
+    E4 = (allI ** 2).sum(axis=(1, 2))
+    dA = abs(float(x[2] - x[1])) * abs(float(y[2] - y[1]))
+    aeff = dA * P * P / E4
+    mx = np.sqrt(np.concatenate([(np.abs(E) ** 2).reshape(B, -1).max(axis=1),
+                                 [allI.reshape(B + 1, -1)[-1].max()]]))
+    return {"power": P, "comx": comx, "comy": comy, "aeff": aeff, "maxabs": mx,
+            "scale": np.array([float(F32(32767.0 / m)) if m > 0 else np.inf for m in mx])}
+
+
+def _safe_stats(E, x, y):
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return field_analysis(E, x, y)
+
+
+def reference_wave(cfg, pol, x, y, W, H, SX, SY, dkx, dky, quantised=True):
+    """Separable reference wave for one polarisation (digHolo.cpp:10201-10504).
+
+    Returns (refX, refY) complex arrays.  With ``quantised`` the values are
+    the reference's 14-bit integers (scale 16383) as complex int pairs;
+    otherwise exact unit-modulus FP64 values.
+    """
+    src_t = 0 if cfg.pol_lock_tilt else pol
+    src_d = 0 if cfg.pol_lock_defocus else pol
+    tx = F32(cfg.tilt_deg[src_t][0] * UNIT_ANGLE)
+    ty = F32(cfg.tilt_deg[src_t][1] * UNIT_ANGLE)
+    offx = F32(0)
+    offy = F32(0)
+    if cfg.resolution_mode == 1:
+        offx = F32((SX[src_t] - W / 2.0 - 0) * float(dkx))
+        offy = F32((SY[src_t] - H / 2.0) * float(dky))
+    dioptre = cfg.defocus[src_d]
+    lam = cfg.wavelength
+    k0 = F32(2.0 * float(PI_F) / float(lam))
+    kxv = F32(F32(-k0 * tx) + offx)
+    kyv = F32(F32(-k0 * ty) + offy)
+    kx0 = kxv if offx == 0 else F32(k0 * F32(-tx))
+    ky0 = kyv if offy == 0 else F32(k0 * F32(-ty))
+    focal = F32(F32(-PI_F * dioptre) / lam)
+    cxp = F32(cfg.beam_centre[pol][0])
+    cyp = F32(cfg.beam_centre[pol][1])
+    out = []
+    for axis, k, piston in ((x, kxv, F32(cxp * kx0)), (y, kyv, F32(cyp * ky0))):
+        r = axis.astype(F32)
+        if quantised:
+            kr = (k.astype(np.float64) * r.astype(np.float64) + float(piston)).astype(F32)  # fmadd
+            arg = (kr + (focal * (r * r)).astype(F32)).astype(F32)
+            c = np.cos(arg.astype(np.float64)).astype(F32)
+            s = np.sin(arg.astype(np.float64)).astype(F32)
+            re = np.clip(np.rint((F32(16383.0) * c).astype(F32)), -32768, 32767).astype(np.int32)
+            im = np.clip(np.rint((F32(16383.0) * s).astype(F32)), -32768, 32767).astype(np.int32)
+            out.append(re + 1j * im)
+        else:
+            arg = float(k) * r.astype(np.float64) + float(piston) + float(focal) * r.astype(np.float64) ** 2
+            out.append(np.exp(1j * arg))
+    return out[0], out[1]
+
+
+def apply_tilt(E, refx, refy, scale, quantised=True):
+    """V = -conj(A . refX . refY) and int16 rounding (digHolo.cpp:2701-2837).
+
+    E: (B, h, w) complex; scale: (B,) float32 scales 32767/max|E|.
+    Returns (V complex FP64 before rounding, R int16, I int16).
+    """
+    if quantised:
+        xr, xi = refx.real.astype(np.int64), refx.imag.astype(np.int64)
+        yr, yi = refy.real.astype(np.int64), refy.imag.astype(np.int64)
+        adj_r = (yr[:, None] * xr[None, :] - yi[:, None] * xi[None, :]).astype(F32)
+        adj_i = (yr[:, None] * xi[None, :] + yi[:, None] * xr[None, :]).astype(F32)
+        k = F32(1.0 / (16383.0 * 16383.0))
+        adj = (adj_r * k).astype(np.float64) + 1j * (adj_i * k).astype(np.float64)
+    else:
+        adj = refy[:, None] * refx[None, :]
+    V = -np.conj(E * adj[None])
+    sc = np.asarray(scale, dtype=np.float64)[:, None, None]
+    with np.errstate(invalid="ignore", over="ignore"):
+        r = np.rint(V.real * sc)
+        i = np.rint(V.imag * sc)
+    # a field with no power has scale 32767/0 = inf; the reference's
+    # float->int32 conversion then yields INT_MIN, saturated to -32768
+    bad_r = ~np.isfinite(r)
+    bad_i = ~np.isfinite(i)
+    r[bad_r] = -32768
+    i[bad_i] = -32768
+    R = np.clip(r, -32768, 32767).astype(np.int16)
+    I = np.clip(i, -32768, 32767).astype(np.int16)
+    return V, R, I
+
+
+def hg_modes(axis, w0, count):
+    """Unit-power HG modes on a float32 axis as digHolo builds them
+    (digHolo.cpp:1269-1433): dX from the axis end points, u = sqrt(2) x / w0,
+    HG_m = sqrt(dX / w0) * 2^(1/4) * psi_m(u), psi_m the normalised Hermite
+    function (FP64 three-term recurrence, digHolo.cpp:1345-1388)."""
+    ax = axis.astype(np.float64)
+    L = ax.size
+    dX = abs((ax[L - 1] - ax[0]) / (L - 1))
+    W0 = float(w0)
+    # u as the reference forms it: the first four axis samples scaled, then
+    # advanced four samples at a time by 4*dX*sqrt(2)/w0 (digHolo.cpp:1287-1294)
+    step = 4.0 * dX * (math.sqrt(2) / W0)
+    lanes = (math.sqrt(2.0) / W0) * ax[:4]
+    blocks = np.concatenate([[0.0], np.cumsum(np.full(L // 4 - 1, step))]) if L >= 8 else np.zeros(L // 4)
+    u = (lanes[None, :] + blocks[:, None]).reshape(-1)
+    if u.size < L:
+        u = math.sqrt(2.0) / W0 * ax
+    norm = (1.0 / math.sqrt(W0)) * math.sqrt(dX) / math.sqrt(math.sqrt(0.5))
+    modes = np.zeros((count, L))
+    g = np.exp(-0.5 * u * u)
+    h0 = 0.7511255444649425 * g  # pi^-0.25
+    modes[0] = h0
+    if count > 1:
+        modes[1] = 1.0622519320271970 * u * g  # sqrt(2) pi^-0.25
+    for n in range(2, count):
+        modes[n] = math.sqrt(2.0 / n) * u * modes[n - 1] - math.sqrt((n - 1.0) / n) * modes[n - 2]
+    return modes * norm
+
+
+def quantise_modes(modes):
+    """int16 modes and scales (digHolo.cpp:1436-1471): scale 32767/max|mode|,
+    float32 multiply, round half to even, saturating pack."""
+    mx = np.abs(modes).max(axis=1)
+    sf = 32767.0 / mx
+    q = np.clip(np.rint((modes.astype(F32) * sf.astype(F32)[:, None]).astype(F32)), -32768, 32767)
+    return q.astype(np.int16), (1.0 / sf).astype(F32)
+
+
+def basis_axes_modes(cfg, pol, xax, yax, quantised=True):
+    """HG modes along x and y for one polarisation (digHolo.cpp:10506-10645).
+
+    Square pixels: one set of modes on the longer axis; the shorter axis uses
+    its centred sub-range.  Returns (Hx, Hy, sx, sy) with Hx (G, nx), Hy (G, ny).
+    """
+    G = cfg.max_mg
+    w0 = cfg.waist[0] if (cfg.pol_lock_waist or pol == 0) else cfg.waist[pol]
+    if w0 == 0:
+        w0 = F32(400e-6)
+    psx = F32(xax[1] - xax[0])
+    psy = F32(yax[1] - yax[0])
+    nx, ny = xax.size, yax.size
+    if psx == psy:
+        long_ax = xax if nx >= ny else yax
+        m = hg_modes(long_ax, w0, G)
+        if quantised:
+            q, s = quantise_modes(m)
+        else:
+            q, s = m, np.ones(G, dtype=F32)
+        L = long_ax.size
+        off = (L - min(nx, ny)) // 2
+        if nx >= ny:
+            return q[:, :nx], q[:, off:off + ny], s, s
+        return q[:, off:off + nx], q[:, :ny], s, s
+    mx = hg_modes(xax, w0, G)
+    my = hg_modes(yax, w0, G)
+    if quantised:
+        qx, sx = quantise_modes(mx)
+        qy, sy = quantise_modes(my)
+        return qx, qy, sx, sy
+    return mx, my, np.ones(G, dtype=F32), np.ones(G, dtype=F32)
+
+
+def hg_index(max_mg):
+    """Mode enumeration (digHolo.cpp:1245-1265): list of (m, n) per mode index."""
+    out = []
+    for g in range(max(max_mg, 1)):
+        for k in range(g + 1):
+            out.append((g - k, k))
+    return out
+
+
+def overlap(R, I, Hx, Hy, sx, sy, field_scale, max_mg, quantised=True):
+    """Separable overlap c_mn = sum_y Hy_n(y) sum_x Hx_m(x) F(x, y)
+    (digHolo.cpp:2149-2341), no conjugation.  R, I: (B, h, w) int16 (or
+    float) field; field_scale: (B,) multiplier to real units.  Returns (B, M)."""
+    idx = hg_index(max_mg)
+    if quantised:
+        Fr = R.astype(np.int64)
+        Fi = I.astype(np.int64)
+        Tx_r = np.einsum("byx,mx->bym", Fr, Hx.astype(np.int64))
+        Tx_i = np.einsum("byx,mx->bym", Fi, Hx.astype(np.int64))
+        Cr = np.einsum("bym,ny->bmn", Tx_r, Hy.astype(np.int64)).astype(np.float64)
+        Ci = np.einsum("bym,ny->bmn", Tx_i, Hy.astype(np.int64)).astype(np.float64)
+    else:
+        Cr = np.einsum("byx,mx,ny->bmn", R, Hx, Hy)
+        Ci = np.einsum("byx,mx,ny->bmn", I, Hx, Hy)
+    out = np.zeros((R.shape[0], len(idx)), dtype=np.complex128)
+    fs = np.asarray(field_scale, dtype=np.float64)
+    for k, (m, n) in enumerate(idx):
+        s = float(sx[m]) * float(sy[n])
+        out[:, k] = (Cr[:, m, n] + 1j * Ci[:, m, n]) * s * fs
+    return out
+
+
+def r2c_windows(frames, cfg, W, H, cxs, cys):
+    """FP64 R2C of each polarisation's FFT window: (B, P, H, W/2+1)."""
+    f = np.asarray(frames, dtype=np.float64)
+    out = []
+    for pol in range(cfg.pol_count):
+        win = f[:, cys[pol]:cys[pol] + H, cxs[pol]:cxs[pol] + W]
+        out.append(np.fft.rfft2(win))
+    return np.stack(out, axis=1)
+
+
+def process_batch(frames, cfg, quantised=True):
+    """Run the batch path on ``frames`` (B, frameHeight, frameWidth).
+
+    Returns a dict with: geometry, ``window`` (B, P, h, w) Fourier windows,
+    ``field_untilted`` (B, P, ny, nx), ``field`` (B, P, ny, nx) complex
+    (quantised: int16 x 1/scale, like digHoloGetFields), ``R``/``I`` int16,
+    ``scale`` (B, P), ``coefs`` (B, P, M), ``stats`` per polarisation.
+    """
+    frames = np.asarray(frames)
+    B = frames.shape[0]
+    P = cfg.pol_count
+    W, H, cxs, cys = fft_windows(cfg)
+    kx, ky = k_axes(W, H, cfg.pixel_size)
+    w, h, SX, SY = ifft_windows(cfg, W, H, kx, ky)
+    xax, yax = ifft_axes(cfg, W, H, w, h)
+    nx, ny = xax.size, yax.size
+    Fplanes = r2c_windows(frames, cfg, W, H, cxs, cys)
+    res = {"W": W, "H": H, "cx": cxs, "cy": cys, "w": w, "h": h, "SX": SX, "SY": SY,
+           "x": xax, "y": yax, "kx": kx, "ky": ky}
+    windows = np.zeros((B, P, h if cfg.resolution_mode else H, w if cfg.resolution_mode else W),
+                       dtype=np.complex128)
+    untilted = np.zeros((B, P, ny, nx), dtype=np.complex128)
+    field = np.zeros((B, P, ny, nx), dtype=np.complex128)
+    field_v = np.zeros((B, P, ny, nx), dtype=np.complex128)
+    Rs = np.zeros((B, P, ny, nx), dtype=np.int16)
+    Is = np.zeros((B, P, ny, nx), dtype=np.int16)
+    scales = np.zeros((B, P))
+    stats = []
+    M = len(hg_index(cfg.max_mg)) if cfg.max_mg > 0 else 0
+    coefs = np.zeros((B, P, M), dtype=np.complex128)
+    for pol in range(P):
+        win = copy_window(Fplanes[:, pol], cfg, pol, W, H, w, h, SX[pol], SY[pol], cxs[pol], cys[pol], kx, ky)
+        windows[:, pol] = win
+        E = np.fft.ifft2(win) * (win.shape[-1] * win.shape[-2])
+        untilted[:, pol] = E
+        st = _safe_stats(E, xax, yax)
+        stats.append(st)
+        scale = st["scale"][:B]
+        scales[:, pol] = scale
+        refx, refy = reference_wave(cfg, pol, xax, yax, W, H, SX, SY, kx[1] - kx[0], ky[1] - ky[0], quantised)
+        V, R, I = apply_tilt(E, refx, refy, scale, quantised)
+        field_v[:, pol] = V
+        Rs[:, pol] = R
+        Is[:, pol] = I
+        if quantised:
+            inv = np.array([float(F32(1.0 / s)) if np.isfinite(s) else 0.0 for s in scale])
+            field[:, pol] = (R.astype(np.float64) + 1j * I.astype(np.float64)) * inv[:, None, None]
+        else:
+            field[:, pol] = V
+        if M:
+            Hx, Hy, sx, sy = basis_axes_modes(cfg, pol, xax, yax, quantised)
+            if quantised:
+                fs = np.array([float(F32(F32(1.0) / F32(s))) if np.isfinite(s) else 0.0 for s in scale])
+                coefs[:, pol] = overlap(R, I, Hx, Hy, sx, sy, fs, cfg.max_mg, True)
+            else:
+                coefs[:, pol] = overlap(V.real, V.imag, Hx, Hy, sx, sy, np.ones(B), cfg.max_mg, False)
+    res.update(window=windows, field_untilted=untilted, field=field, field_v=field_v,
+               R=Rs, I=Is, scale=scales, coefs=coefs, stats=stats)
+    return res
+
+
+def reference_unscaled_16(coefs, cfg, res):
+    """What digHoloProcessBatch returns when the field is 16 rows high: the
+    overlap without its final scale (digHolo.cpp:2318-2331).  Divides the
+    properly scaled quantised coefficients by that scale."""
+    xax, yax = res["x"], res["y"]
+    out = np.array(coefs, copy=True)
+    idx = hg_index(cfg.max_mg)
+    for pol in range(cfg.pol_count):
+        _, _, sx, sy = basis_axes_modes(cfg, pol, xax, yax, True)
+        fs = np.array([float(F32(F32(1.0) / F32(s))) for s in res["scale"][:, pol]])
+        for k, (m, n) in enumerate(idx):
+            out[:, pol, k] = out[:, pol, k] / (float(sx[m]) * float(sy[n]) * fs)
+    return out
+
+
+# ---------------------------------------------------------------- metrics
+
+def power_meter(coefs, pol_independent=False, goal_uses_svd=True):
+    """IL / MDL of the batch coefficient matrix (digHolo.cpp:10714-11130) for
+    a single wavelength, batchCount > 1, basis output modes.
+
+    coefs: (B, P, M) complex.  Returns dict with linear 'il', 'mdl' from the
+    SVD path (used when the goal is MDL and for reported metrics) and
+    'il_frob' from the Frobenius path (insertionLoss256, digHolo.cpp:3105-3143),
+    plus their values in dB (10 log10, digHolo.cpp:12188).
+    """
+    B, P, M = coefs.shape
+    independent = pol_independent or P == 1
+    mats = []
+    if P == 1 or not independent:
+        mats.append(coefs.reshape(B, P * M).T)       # (modes, batch)
+    else:
+        for pol in range(P):
+            mats.append(coefs[:, pol, :].T)
+    svals = []
+    for A in mats:
+        svals.append(np.linalg.svd(A, compute_uv=False))
+    s = np.concatenate(svals)
+    il = float(np.mean(s ** 2))
+    mdl = float(s.min() ** 2 / s.max() ** 2)
+    il_frob = float(sum((np.abs(A) ** 2).sum() / B for A in mats))
+    return {"il": il, "mdl": mdl, "il_frob": il_frob,
+            "il_db": 10 * math.log10(il), "mdl_db": 10 * math.log10(mdl),
+            "il_frob_db": 10 * math.log10(il_frob)}
