@@ -1,0 +1,506 @@
+// sm_100a kernels for the digHolo batch path.
+//
+//   k_forward : frame window -> pruned R2C FFT -> Fourier window ops
+//               (replaces convert_int16tofloat32 digHolo.cpp:1201, the FFTW
+//               r2c batch digHolo.cpp:7184-7260 and digHoloCopyWindow
+//               digHolo.cpp:1808-2122)
+//   k_inverse : window IFFT -> field statistics -> reference wave, -conj,
+//               int16 rounding -> separable HG overlap
+//               (replaces the FFTW c2c backward digHolo.cpp:8734,
+//               digHoloFieldAnalysis digHolo.cpp:2354, applyTilt16
+//               digHolo.cpp:2701 and overlapFieldSeparable16 digHolo.cpp:2149)
+//   k_basis   : FP64 Hermite-Gaussian recurrence -> int16 modes + scales
+//               (replaces HGbasisXY1D digHolo.cpp:1269-1484)
+//   k_fields_to_c64 : int16 field -> complex64 x 1/scale (digHoloGetFields,
+//               digHolo.cpp:4930-4981)
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "dh_common.cuh"
+#include "dh_params.h"
+
+using namespace dh;
+
+namespace {
+
+constexpr int FWD_THREADS = 256;
+constexpr int INV_THREADS = 512;
+// Row-FFT staging budget of the forward kernel (complex elements).
+constexpr int FWD_ROWBUF_ELEMS = 4096;
+
+__device__ __forceinline__ int wrapMod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ void load8(const void* frames, int u16, long long idx, float* v) {
+    if (u16) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(frames) + idx));
+        v[0] = (float)(q.x & 0xFFFFu); v[1] = (float)(q.x >> 16);
+        v[2] = (float)(q.y & 0xFFFFu); v[3] = (float)(q.y >> 16);
+        v[4] = (float)(q.z & 0xFFFFu); v[5] = (float)(q.z >> 16);
+        v[6] = (float)(q.w & 0xFFFFu); v[7] = (float)(q.w >> 16);
+    } else {
+        const float4* s = reinterpret_cast<const float4*>(static_cast<const float*>(frames) + idx);
+        const float4 a = __ldg(s), b = __ldg(s + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    }
+}
+
+}  // namespace
+
+// One block per (frame, polarisation, column chunk).  The window rows are
+// staged in blocks of RB rows, transformed as packed half-length complex
+// FFTs, and only the kx columns of the IFFT window are kept (R2C split
+// post-processing).  The kept columns are then transformed along y and only
+// the ky rows of the IFFT window are kept.
+__global__ void __launch_bounds__(FWD_THREADS) k_forward(DhFwdParams p) {
+    extern __shared__ float2 sm[];
+    const int W = 1 << p.logW, H = 1 << p.logH;
+    const int logN = p.logW - 1, N = W >> 1;
+    const int WC = p.colChunk;
+    const int chunks = p.w / WC;
+    int unit = blockIdx.x;
+    const int chunk = unit % chunks;
+    unit /= chunks;
+    const int pol = unit % p.polCount;
+    const int frame = unit / p.polCount;
+    int RB = FWD_ROWBUF_ELEMS / N;
+    if (RB > H) RB = H;
+    float2* rowbuf = sm;
+    float2* colbuf = sm + RB * N;
+    const int kStart = p.sx0[pol] + chunk * WC;
+    const long long base = (long long)frame * p.frameStride + (long long)p.cy[pol] * p.frameWidth + p.cx[pol];
+    const int vecPerRow = W >> 3;
+
+    for (int r0 = 0; r0 < H; r0 += RB) {
+        for (int e = threadIdx.x; e < RB * vecPerRow; e += blockDim.x) {
+            const int r = e / vecPerRow, v = e - r * vecPerRow;
+            float x[8];
+            load8(p.frames, p.inputU16, base + (long long)(r0 + r) * p.frameWidth + v * 8, x);
+            float2* dst = rowbuf + r * N;
+#pragma unroll
+            for (int q = 0; q < 4; q++) dst[bitrev(v * 4 + q, logN)] = make_float2(x[2 * q], x[2 * q + 1]);
+        }
+        __syncthreads();
+        fft_dit(rowbuf, RB, N, 1, logN, false, false, p.twiddle);
+        for (int e = threadIdx.x; e < RB * WC; e += blockDim.x) {
+            const int r = e / WC, c = e - r * WC;
+            const int k = kStart + c;
+            const float2 zk = rowbuf[r * N + (k & (N - 1))];
+            const float2 zc = cconj(rowbuf[r * N + ((N - k) & (N - 1))]);
+            const float2 even = cscale(cadd(zk, zc), 0.5f);
+            const float2 d = csub(zk, zc);
+            const float2 odd = make_float2(0.5f * d.y, -0.5f * d.x);  // -i/2 (zk - zc)
+            const float2 wk = __ldg(&p.twiddle[k << (TW_LOG - p.logW)]);
+            colbuf[bitrev(r0 + r, p.logH) * WC + c] = cadd(even, cmul(wk, odd));
+        }
+        __syncthreads();
+    }
+    fft_dit(colbuf, WC, 1, WC, p.logH, false, true, p.twiddle);
+
+    float2 bc = make_float2(1.0f, 0.0f);
+    if (p.batchCal && p.batchCalCount > 0)
+        bc = p.batchCal[pol * p.batchCalCount + ((p.frameOffset + frame) % p.batchCalCount)];
+    const float kx0 = p.kx0[pol], ky0 = p.ky0[pol], r02 = p.r02[pol];
+    const float bcx = p.bcx[pol], bcy = p.bcy[pol];
+    for (int e = threadIdx.x; e < p.h * WC; e += blockDim.x) {
+        const int j = e / WC, c = e - j * WC;
+        const int jSY = j + p.sy[pol];
+        const int row = wrapMod(jSY + H / 2, H);
+        float2 Y = colbuf[row * WC + c];
+        Y = cmul(Y, bc);
+        const float kx = p.kxAxis[kStart + c];
+        const float ky = p.kyAxis[row];
+        const float shift = jSY < 0 ? p.kyShift : (jSY > H ? -p.kyShift : 0.0f);
+        // the mask test in float32 as digHolo.cpp:1984-2019 evaluates it
+        const float dky = __fsub_rn(ky, __fadd_rn(ky0, shift));
+        const float dkx = __fsub_rn(kx, kx0);
+        const float dr2 = __fadd_rn(__fmul_rn(dkx, dkx), __fmul_rn(dky, dky));
+        float env = 1.0f;
+        if (p.fillFactor) env = xcsc(kx * p.halfPixel) * xcsc(ky * p.halfPixel);
+        const float normF = (dr2 <= r02) ? env * p.norm : 0.0f;
+        const float arg = __fadd_rn(__fmul_rn(bcx, kx), __fmul_rn(ky, bcy));
+        float sn, cs;
+        sincosf(arg, &sn, &cs);
+        const float2 adj = make_float2(cs * normF, sn * normF);
+        const size_t o = ((size_t)(frame * p.polCount + pol) * p.h + j) * p.w + chunk * WC + c;
+        p.window[o] = cmul(Y, adj);
+    }
+}
+
+namespace {
+
+struct Stat6 {
+    float maxI;
+    int maxIdx;
+    float P, cx, cy, cyw, e4;
+};
+
+__device__ __forceinline__ void statCombine(Stat6& a, const Stat6& b) {
+    if (b.maxI > a.maxI || (b.maxI == a.maxI && b.maxIdx > a.maxIdx)) { a.maxI = b.maxI; a.maxIdx = b.maxIdx; }
+    a.P += b.P; a.cx += b.cx; a.cy += b.cy; a.cyw += b.cyw; a.e4 += b.e4;
+}
+
+__device__ Stat6 blockReduceStat(Stat6 s, Stat6* scratch) {
+    for (int off = 16; off > 0; off >>= 1) {
+        Stat6 o;
+        o.maxI = __shfl_down_sync(0xffffffffu, s.maxI, off);
+        o.maxIdx = __shfl_down_sync(0xffffffffu, s.maxIdx, off);
+        o.P = __shfl_down_sync(0xffffffffu, s.P, off);
+        o.cx = __shfl_down_sync(0xffffffffu, s.cx, off);
+        o.cy = __shfl_down_sync(0xffffffffu, s.cy, off);
+        o.cyw = __shfl_down_sync(0xffffffffu, s.cyw, off);
+        o.e4 = __shfl_down_sync(0xffffffffu, s.e4, off);
+        statCombine(s, o);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) scratch[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Stat6 t = scratch[0];
+        for (int i = 1; i < (int)(blockDim.x >> 5); i++) statCombine(t, scratch[i]);
+        scratch[0] = t;
+    }
+    __syncthreads();
+    return scratch[0];
+}
+
+}  // namespace
+
+// One block per (frame, polarisation).
+__global__ void __launch_bounds__(INV_THREADS) k_inverse(DhInvParams p) {
+    extern __shared__ float2 sm[];
+    const int unit = blockIdx.x;
+    const int pol = unit % p.polCount;
+    const int frame = unit / p.polCount;
+    const int w = 1 << p.logw, h = 1 << p.logh;
+    const int W = 1 << p.logW, H = 1 << p.logH;
+    const int lognx = p.lowres ? p.logw : p.logW;
+    const int logny = p.lowres ? p.logh : p.logH;
+    const int nx = 1 << lognx, ny = 1 << logny;
+    const int npix = nx * ny;
+    const int ld = nx + 1;                           // padded row stride of the field in shared memory
+    float2* fld = sm;
+    float2* colbuf = fld + (size_t)ny * ld;          // full-res only: H * w
+    float* extra = reinterpret_cast<float*>(colbuf + (p.lowres ? 0 : H * w));
+    const float2* win = p.window + (size_t)unit * h * w;
+
+    if (p.lowres) {
+        for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
+            const int j = e >> p.logw, c = e & (w - 1);
+            fld[bitrev(j, p.logh) * ld + bitrev(c, p.logw)] = win[e];
+        }
+        __syncthreads();
+        fft_dit(fld, h, ld, 1, p.logw, true, false, p.twiddle);
+        fft_dit(fld, w, 1, ld, p.logh, true, true, p.twiddle);
+    } else {
+        for (int e = threadIdx.x; e < H * w; e += blockDim.x) colbuf[e] = make_float2(0.f, 0.f);
+        for (int e = threadIdx.x; e < ny * ld; e += blockDim.x) fld[e] = make_float2(0.f, 0.f);
+        __syncthreads();
+        const int syp = p.sy[pol];
+        for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
+            const int j = e >> p.logw, c = e & (w - 1);
+            const int row = wrapMod(j + syp + H / 2, H);
+            colbuf[bitrev(row, p.logH) * w + c] = win[e];
+        }
+        __syncthreads();
+        fft_dit(colbuf, w, 1, w, p.logH, true, true, p.twiddle);
+        const int sx0 = p.sx0[pol];
+        for (int e = threadIdx.x; e < H * w; e += blockDim.x) {
+            const int y = e >> p.logw, c = e & (w - 1);
+            fld[y * ld + bitrev((sx0 + c) & (W - 1), p.logW)] = colbuf[e];
+        }
+        __syncthreads();
+        fft_dit(fld, H, ld, 1, p.logW, true, false, p.twiddle);
+    }
+
+    // Field statistics over the whole untilted field (windowRadius = 0,
+    // digHolo.cpp:8866-8870): power, centre of mass, max|E|, E^4.
+    Stat6* scratch = reinterpret_cast<Stat6*>(extra);
+    const float inv = (float)(1.0 / ((double)nx * (double)ny));
+    const float yShift = fabsf((p.yAxis[1] - p.yAxis[0]) * (float)ny);
+    Stat6 st = {0.f, -1, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int y = e >> lognx, x = e & (nx - 1);
+        const float2 a = fld[y * ld + x];
+        const float I0 = fmaf(a.x, a.x, a.y * a.y);
+        const float I = I0 * inv;
+        const int idx = 2 * y * nx + x;
+        if (I0 > st.maxI || (I0 == st.maxI && idx > st.maxIdx)) { st.maxI = I0; st.maxIdx = idx; }
+        const float yv = p.yAxis[y];
+        st.P += I;
+        st.cx = fmaf(p.xAxis[x], I, st.cx);
+        st.cy = fmaf(yv, I, st.cy);
+        st.cyw = fmaf(yv + (yv < 0.f ? yShift : 0.f), I, st.cyw);
+        st.e4 = fmaf(I, I, st.e4);
+    }
+    st = blockReduceStat(st, scratch);
+    const float maxAbs = sqrtf(st.maxI);
+    const float scale = (float)(32767.0 / (double)maxAbs);
+    if (threadIdx.x == 0) {
+        const int S = p.statsStride;
+        float* s = p.stats;
+        const int col = pol * S + frame;
+        const int per = p.polCount * S;
+        s[0 * per + col] = st.P;
+        s[1 * per + col] = st.cx / st.P;
+        s[2 * per + col] = st.cy / st.P;
+        s[3 * per + col] = scale;
+        s[4 * per + col] = __int_as_float(st.maxIdx);
+        s[5 * per + col] = p.dA * (st.P * st.P / st.e4);
+        s[6 * per + col] = st.cyw / st.P;
+    }
+
+    // Reference wave, -conj(A . ref), int16 rounding (digHolo.cpp:2741-2833).
+    const short* ref = p.refWave + (size_t)pol * 2 * (nx + ny);
+    const float K = (float)(1.0 / (16383.0 * 16383.0));
+    const size_t fieldOff = (size_t)unit * npix;
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int y = e >> lognx, x = e & (nx - 1);
+        const int xr = ref[x], xi = ref[nx + x];
+        const int yr = ref[2 * nx + y], yi = ref[2 * nx + ny + y];
+        const float adjR = (float)(yr * xr - yi * xi) * K;
+        const float adjI = (float)(yr * xi + yi * xr) * K;
+        const float2 a = fld[y * ld + x];
+        const float vr = __fsub_rn(__fmul_rn(a.y, adjI), __fmul_rn(a.x, adjR));
+        const float vi = __fadd_rn(__fmul_rn(a.x, adjI), __fmul_rn(a.y, adjR));
+        if (p.field32) {
+            // float path: the same -conj(A . ref) with the unquantised wave
+            const float* rf = p.refWaveF + (size_t)pol * 2 * (nx + ny);
+            const float2 rx = make_float2(rf[x], rf[nx + x]);
+            const float2 ry = make_float2(rf[2 * nx + y], rf[2 * nx + ny + y]);
+            const float2 v = cmul(a, cmul(ry, rx));
+            p.field32[fieldOff + e] = make_float2(-v.x, v.y);
+        }
+        const float fr = rintf(scale * vr), fi = rintf(scale * vi);
+        // float -> int32 with the x86 convention (NaN / overflow -> INT_MIN),
+        // then saturate to int16 (digHolo.cpp:2822-2829)
+        const int ir = (fr >= -2147483648.0f && fr < 2147483648.0f) ? (int)fr : INT32_MIN;
+        const int ii = (fi >= -2147483648.0f && fi < 2147483648.0f) ? (int)fi : INT32_MIN;
+        const short sr = (short)max(-32768, min(32767, ir));
+        const short si = (short)max(-32768, min(32767, ii));
+        p.fieldR[fieldOff + e] = sr;
+        p.fieldI[fieldOff + e] = si;
+        fld[y * ld + x] = make_float2((float)sr, (float)si);
+    }
+    __syncthreads();
+
+    if (p.maxMG <= 0) return;
+
+    // Separable overlap on the int16 field (digHolo.cpp:2149-2341):
+    // T[y][m] = sum_x F[y][x] Hx[m][x];  c_mn = sum_y Hy[n][y] T[y][m].
+    const int G = p.maxMG;
+    float* hx = extra;                 // [G][nx]
+    float* hy = hx + G * nx;           // [G][ny]
+    float2* T = reinterpret_cast<float2*>(hy + G * ny);   // [ny][G]
+    const short* gx = p.hgX + (size_t)pol * G * nx;
+    const short* gy = p.hgY + (size_t)pol * G * ny;
+    for (int e = threadIdx.x; e < G * nx; e += blockDim.x) hx[e] = (float)gx[e];
+    for (int e = threadIdx.x; e < G * ny; e += blockDim.x) hy[e] = (float)gy[e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < ny * G; e += blockDim.x) {
+        const int m = e >> logny, y = e & (ny - 1);
+        const float2* row = fld + y * ld;
+        const float* hm = hx + m * nx;
+        float ar = 0.f, ai = 0.f;
+        for (int x = 0; x < nx; x++) {
+            const float2 f = row[x];
+            const float hv = hm[x];
+            ar = fmaf(f.x, hv, ar);
+            ai = fmaf(f.y, hv, ai);
+        }
+        T[y * G + m] = make_float2(ar, ai);
+    }
+    __syncthreads();
+    const float fieldScale = 1.0f / scale;
+    const float* sxp = p.hgScaleX + pol * G;
+    const float* syp = p.hgScaleY + pol * G;
+    for (int mode = threadIdx.x; mode < p.modeCount; mode += blockDim.x) {
+        // mode -> (m, n): group g, n = mode - g(g+1)/2, m = g - n (digHolo.cpp:1245-1265)
+        int g = (int)((sqrtf(8.0f * mode + 1.0f) - 1.0f) * 0.5f);
+        while ((g + 1) * (g + 2) / 2 <= mode) g++;
+        while (g * (g + 1) / 2 > mode) g--;
+        const int n = mode - g * (g + 1) / 2;
+        const int m = g - n;
+        const float* hn = hy + n * ny;
+        float cr = 0.f, ci = 0.f;
+        for (int y = 0; y < ny; y++) {
+            const float2 t = T[y * G + m];
+            cr = fmaf(hn[y], t.x, cr);
+            ci = fmaf(hn[y], t.y, ci);
+        }
+        const float ms = (float)((double)sxp[m] * (double)syp[n] * (double)fieldScale);
+        p.coefs[(size_t)frame * p.polCount * p.modeCount + pol * p.modeCount + mode] = make_float2(cr * ms, ci * ms);
+    }
+}
+
+// One block per axis; blockDim >= 256, up to 4 samples per thread.
+__global__ void __launch_bounds__(1024) k_basis(DhBasisParams p) {
+    __shared__ double red[32];
+    __shared__ double sMax;
+    const int L = p.count;
+    const double W0 = p.w0;
+    const double x0 = (double)p.axis[0], xL = (double)p.axis[L - 1];
+    const double dX = fabs((xL - x0) / (double)(L - 1));
+    const double axisScale = sqrt(2.0) / W0;
+    const double step = 4.0 * dX * (sqrt(2.0) / W0);
+    const double norm = (1.0 / sqrt(W0)) * sqrt(dX) / sqrt(sqrt(0.5));
+    constexpr int PER = 4;
+    double u[PER], h0[PER], h1[PER];
+    int idx[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int i = threadIdx.x + q * blockDim.x;
+        idx[q] = i;
+        u[q] = 0.0;
+        if (i < L) {
+            // u as digHolo forms it: lane value plus (i/4) sequential steps
+            double v = axisScale * (double)p.axis[i & 3];
+            for (int b = 0; b < (i >> 2); b++) v += step;
+            u[q] = v;
+        }
+        h0[q] = 0.0;
+        h1[q] = 0.0;
+    }
+    for (int mode = 0; mode < p.modes; mode++) {
+        double val[PER];
+        double localMax = 0.0;
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            double v = 0.0;
+            if (idx[q] < L) {
+                if (mode == 0) v = 0.7511255444649425 * exp(-0.5 * u[q] * u[q]);
+                else if (mode == 1) v = 1.0622519320271970 * u[q] * exp(-0.5 * u[q] * u[q]);
+                else v = sqrt(2.0 / mode) * u[q] * h1[q] - sqrt((mode - 1.0) / mode) * h0[q];
+            }
+            h0[q] = h1[q];
+            h1[q] = v;
+            val[q] = norm * v;
+            localMax = fmax(localMax, fabs(val[q]));
+        }
+        for (int off = 16; off > 0; off >>= 1) localMax = fmax(localMax, __shfl_down_sync(0xffffffffu, localMax, off));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = localMax;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double mx = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); i++) mx = fmax(mx, red[i]);
+            sMax = mx;
+        }
+        __syncthreads();
+        const double sf = 32767.0 / sMax;
+        const float sff = (float)sf;
+        if (threadIdx.x == 0) p.scale[mode] = (float)(1.0 / sf);
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            if (idx[q] < L) {
+                const float r = rintf(__fmul_rn((float)val[q], sff));
+                const int ir = (r >= -2147483648.0f && r < 2147483648.0f) ? (int)r : INT32_MIN;
+                p.out16[(size_t)mode * L + idx[q]] = (short)max(-32768, min(32767, ir));
+                if (p.outF) p.outF[(size_t)mode * L + idx[q]] = (float)val[q];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// int16 field -> complex64 x (1/scale) (digHolo.cpp:4947-4981).
+__global__ void k_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
+                                int polCount, int frameCount, int npix, float2* out) {
+    const size_t total = (size_t)frameCount * polCount * npix;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t unit = e / npix;
+        const int pol = (int)(unit % polCount);
+        const int frame = (int)(unit / polCount);
+        const float scale = stats[3 * polCount * statsStride + pol * statsStride + frame];
+        const float inv = (float)(1.0 / (double)scale);
+        out[e] = make_float2((float)R[e] * inv, (float)I[e] * inv);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+size_t dh_forward_smem_bytes(int logW, int logH, int colChunk) {
+    const int N = 1 << (logW - 1);
+    int RB = FWD_ROWBUF_ELEMS / N;
+    if (RB > (1 << logH)) RB = 1 << logH;
+    return sizeof(float2) * ((size_t)RB * N + (size_t)(1 << logH) * colChunk);
+}
+
+cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s) {
+    const size_t smem = dh_forward_smem_bytes(p.logW, p.logH, p.colChunk);
+    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long blocks = (long long)p.frameCount * p.polCount * (p.w / p.colChunk);
+    k_forward<<<(unsigned)blocks, FWD_THREADS, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+size_t dh_inverse_smem_bytes(const DhInvParams& p) {
+    const int nx = p.lowres ? (1 << p.logw) : (1 << p.logW);
+    const int ny = p.lowres ? (1 << p.logh) : (1 << p.logH);
+    size_t bytes = sizeof(float2) * (size_t)(nx + 1) * ny;
+    if (!p.lowres) bytes += sizeof(float2) * (size_t)(1 << p.logH) * (1 << p.logw);
+    size_t extra = sizeof(Stat6) * (INV_THREADS / 32);
+    if (p.maxMG > 0) {
+        const size_t ov = sizeof(float) * (size_t)p.maxMG * (nx + ny) + sizeof(float2) * (size_t)ny * p.maxMG;
+        if (ov > extra) extra = ov;
+    }
+    return bytes + extra;
+}
+
+cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
+    const size_t smem = dh_inverse_smem_bytes(p);
+    cudaError_t e = cudaFuncSetAttribute(k_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_inverse<<<(unsigned)(p.frameCount * p.polCount), INV_THREADS, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s) {
+    int threads = (p.count + 3) / 4;
+    threads = ((threads + 31) / 32) * 32;
+    if (threads < 32) threads = 32;
+    if (threads > 1024) return cudaErrorInvalidValue;
+    k_basis<<<1, threads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
+                                    int polCount, int frameCount, int npix, float2* out, cudaStream_t s) {
+    const size_t total = (size_t)frameCount * polCount * npix;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    k_fields_to_c64<<<blocks, 256, 0, s>>>(R, I, stats, statsStride, polCount, frameCount, npix, out);
+    return cudaGetLastError();
+}
+
+// Sum over the batch of |E|^2 / (nx ny) per pixel, from the int16 fields
+// (the batch-sum intensity of digHoloFieldAnalysis, digHolo.cpp:2519-2568).
+__global__ void k_batchsum(const short* R, const short* I, const float* stats, int statsStride,
+                           int polCount, int frameCount, int npix, float* out) {
+    const float inv = 1.0f / (float)npix;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < polCount * npix; e += gridDim.x * blockDim.x) {
+        const int pol = e / npix, pix = e - pol * npix;
+        float acc = 0.f;
+        for (int f = 0; f < frameCount; f++) {
+            const float scale = stats[3 * polCount * statsStride + pol * statsStride + f];
+            const float s = (float)(1.0 / (double)scale);
+            const size_t o = ((size_t)f * polCount + pol) * npix + pix;
+            const float r = (float)R[o] * s, i = (float)I[o] * s;
+            acc += (r * r + i * i) * inv;
+        }
+        out[e] = acc;
+    }
+}
+
+cudaError_t dh_launch_batchsum(const short* R, const short* I, const float* stats, int statsStride,
+                               int polCount, int frameCount, int npix, float* out, cudaStream_t s) {
+    int blocks = (polCount * npix + 255) / 256;
+    if (blocks < 1) blocks = 1;
+    k_batchsum<<<blocks, 256, 0, s>>>(R, I, stats, statsStride, polCount, frameCount, npix, out);
+    return cudaGetLastError();
+}

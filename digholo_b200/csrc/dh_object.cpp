@@ -1,0 +1,765 @@
+// Host runtime of digholo_b200: window geometry (float32 emulation of the
+// reference), device buffer management, and the stage launches behind
+// digHoloProcessBatch.
+#include "dh_object.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
+cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
+size_t dh_inverse_smem_bytes(const DhInvParams& p);
+cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
+cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
+cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
+                                    int polCount, int frameCount, int npix, float2* out, cudaStream_t s);
+cudaError_t dh_launch_batchsum(const short* R, const short* I, const float* stats, int statsStride,
+                               int polCount, int frameCount, int npix, float* out, cudaStream_t s);
+
+namespace dh {
+
+static const float PI_F = 3.14159265358979323846264338327950288f;   // digHolo.cpp:89
+static const double PI_D = 3.14159265358979323846264338327950288;   // digHolo.cpp:3633
+static const float UNIT_ANGLE = PI_F / 180.0f;                       // digHolo.h:192
+static const int PIXEL_QUANTA = 16;                                  // digHolo.cpp:94
+
+cudaError_t DevBuf::ensure(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) { ptr = nullptr; bytes = 0; return e; }
+    bytes = n;
+    return cudaSuccess;
+}
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+bool HostBuf::ensure(size_t n) {
+    if (n <= bytes && ptr) return true;
+    release();
+    if (n == 0) return true;
+    if (cudaMallocHost(&ptr, n) != cudaSuccess) { ptr = nullptr; bytes = 0; return false; }
+    bytes = n;
+    return true;
+}
+void HostBuf::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+bool isPow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+int ilog2(int v) { int l = 0; while ((1 << l) < v) l++; return l; }
+
+static int fail(Object& o, int code, const char* what) {
+    o.lastError = what;
+    if (o.cfg.verbosity >= 1) { fprintf(stderr, "digholo_b200: %s\n", what); fflush(stderr); }
+    return code;
+}
+static int failCuda(Object& o, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    o.lastError = m;
+    fprintf(stderr, "digholo_b200: %s\n", m.c_str());
+    fflush(stderr);
+    return ERR_ERROR;
+}
+#define DH_CUDA(o, call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return failCuda(o, e_, #call); } while (0)
+
+// ------------------------------------------------------------------ geometry
+
+static void axisShifted(int n, float step, std::vector<float>& a) {
+    a.resize(n);
+    for (int i = 0; i < n; i++) a[i] = step * (float)(i <= n / 2 ? i : i - n);
+}
+static void axisCentred(int n, float step, std::vector<float>& a) {
+    a.resize(n);
+    for (int i = 0; i < n; i++) a[i] = (float)(i - n / 2) * step;
+}
+
+// digHolo.cpp:7283-7378 and 7720-7733
+void fftWindowGeometry(const Config& c, int P, Geometry& g) {
+    const int fx = c.fftWindowSizeX > 0 ? c.fftWindowSizeX : c.frameWidth / P;
+    const int fy = c.fftWindowSizeY > 0 ? c.fftWindowSizeY : c.frameHeight;
+    int W = PIXEL_QUANTA * (fx / PIXEL_QUANTA);
+    int H = PIXEL_QUANTA * (fy / PIXEL_QUANTA);
+    W = std::max(W, 16);
+    H = std::max(H, 16);
+    W = std::min(W, c.frameWidth);
+    H = std::min(H, c.frameHeight);
+    const int block = 16;  // ALIGN / sizeof(float)
+    for (int pol = 0; pol < P; pol++) {
+        const float CX = (c.beamCentreX[pol] / c.pixelSize) + (float)(c.frameWidth / 2);
+        const float CY = (c.beamCentreY[pol] / c.pixelSize) + (float)(c.frameHeight / 2);
+        int cx = (int)std::round((CX - (float)(W / 2)) / (float)block) * block;
+        int cy = (int)std::round(CY - (float)(H / 2));
+        if (cx < 0) cx = 0;
+        if (cy < 0) cy = 0;
+        if (cx + W > c.frameWidth) cx = c.frameWidth - W;
+        if (cy + H > c.frameHeight) cy = c.frameHeight - H;
+        g.cx[pol] = cx;
+        g.cy[pol] = cy;
+    }
+    g.W = W;
+    g.H = H;
+    const float period = (float)(2.0 * c.pixelSize);
+    const float kfx = (float)(2 * (2.0 * PI_D / period) / W);
+    const float kfy = (float)(2 * (2.0 * PI_D / period) / H);
+    axisShifted(W, kfx, g.kx);
+    axisShifted(H, kfy, g.ky);
+    axisCentred(W, c.pixelSize, g.xFull);
+    axisCentred(H, c.pixelSize, g.yFull);
+}
+
+// digHolo.cpp:7868-8048 (single wavelength) and 8183-8203
+void ifftWindowGeometry(const Config& c, int P, Geometry& g) {
+    const float lam = c.wavelengthCentre;
+    const float k0Max = 2 * PI_F / lam;
+    const float k0Min = k0Max;
+    const float dkx = g.kx[1] - g.kx[0];
+    const float dky = g.ky[1] - g.ky[0];
+    const float r0 = c.apertureSize * UNIT_ANGLE;
+    int woiCX[POLMAX], woiCY[POLMAX];
+    int w = 0, h = 0;
+    for (int pol = 0; pol < P; pol++) {
+        const int src = c.polLockTilt ? 0 : pol;
+        const float tx = c.zern[src][ZERN_TILTX] * UNIT_ANGLE;
+        const float ty = c.zern[src][ZERN_TILTY] * UNIT_ANGLE;
+        const float maxEX = (float)(((tx + r0) * k0Max) / dkx + g.W / 2.0);
+        const float maxEY = (float)(((ty + r0) * k0Max) / dky + g.H / 2.0);
+        const float minSX = (float)(((tx - r0) * k0Min) / dkx + g.W / 2.0);
+        const float minSY = (float)(((ty - r0) * k0Min) / dky + g.H / 2.0);
+        woiCX[pol] = (int)std::round((maxEX + minSX) / 4.0) * 2;
+        woiCY[pol] = (int)std::round((maxEY + minSY) / 4.0) * 2;
+        int wp = (int)(maxEX - minSX + 1);
+        int hp = (int)(maxEY - minSY + 1);
+        wp = (int)(16 * std::ceil((1.0f * wp) / 16));
+        hp = (int)(16 * std::ceil((1.0f * hp) / 16));
+        w = std::max(w, wp);
+        h = std::max(h, hp);
+    }
+    if (h < 16) h = 16;
+    if (w < 16) w = 16;
+    for (int pol = 0; pol < P; pol++) {
+        int sx = (int)(woiCX[pol] - w / 2.0);
+        if (sx < g.W / 2) sx = g.W / 2;
+        if (sx < 0) sx = 0;
+        if (sx + w > g.W) sx = g.W - w;
+        g.SX[pol] = sx;
+        g.SY[pol] = (int)(woiCY[pol] - h / 2.0);
+    }
+    g.w = w;
+    g.h = h;
+    const int nx = c.resolutionIdx ? w : g.W;
+    const int ny = c.resolutionIdx ? h : g.H;
+    g.nx = nx;
+    g.ny = ny;
+    const float psx = ((c.pixelSize) * g.W) / nx;
+    const float psy = ((c.pixelSize) * g.H) / ny;
+    axisCentred(nx, psx, g.x);
+    axisCentred(ny, psy, g.y);
+}
+
+// Separable 14-bit reference wave per polarisation (digHolo.cpp:10201-10504):
+// out[pol][0..nx) Xr, [nx..2nx) Xi, [2nx..2nx+ny) Yr, [2nx+ny..) Yi.
+void referenceWave(const Config& c, int P, const Geometry& g, std::vector<short>& out, std::vector<float>* outF) {
+    const int nx = g.nx, ny = g.ny;
+    if (outF) outF->assign((size_t)P * 2 * (nx + ny), 0.f);
+    const std::vector<float>& xa = c.resolutionIdx ? g.x : g.xFull;
+    const std::vector<float>& ya = c.resolutionIdx ? g.y : g.yFull;
+    out.assign((size_t)P * 2 * (nx + ny), 0);
+    const float dkx = g.kx[1] - g.kx[0];
+    const float dky = g.ky[1] - g.ky[0];
+    for (int pol = 0; pol < P; pol++) {
+        const int st = c.polLockTilt ? 0 : pol;
+        const int sd = c.polLockDefocus ? 0 : pol;
+        const float tx = c.zern[st][ZERN_TILTX] * UNIT_ANGLE;
+        const float ty = c.zern[st][ZERN_TILTY] * UNIT_ANGLE;
+        float offx = 0.f, offy = 0.f;
+        if (c.resolutionIdx == 1) {
+            offx = (float)((g.SX[st] - g.W / 2.0 - 0) * dkx);
+            offy = (float)((g.SY[st] - g.H / 2.0) * dky);
+        }
+        const float dioptre = c.zern[sd][ZERN_DEFOCUS];
+        const float lam = c.wavelengthCentre;
+        const float k0 = (float)(2.0 * PI_F / lam);
+        const float kx = -k0 * tx + offx;
+        const float ky = -k0 * ty + offy;
+        const float kx0 = offx == 0 ? kx : k0 * (-tx);
+        const float ky0 = offy == 0 ? ky : k0 * (-ty);
+        const float focal = (float)(-PI_F * dioptre / lam);
+        const float pistX = c.beamCentreX[pol] * kx0;
+        const float pistY = c.beamCentreY[pol] * ky0;
+        short* o = &out[(size_t)pol * 2 * (nx + ny)];
+        for (int axis = 0; axis < 2; axis++) {
+            const std::vector<float>& a = axis == 0 ? xa : ya;
+            const int n = axis == 0 ? nx : ny;
+            const float k = axis == 0 ? kx : ky;
+            const float piston = axis == 0 ? pistX : pistY;
+            short* re = axis == 0 ? o : o + 2 * nx;
+            short* im = axis == 0 ? o + nx : o + 2 * nx + ny;
+            for (int i = 0; i < n; i++) {
+                const float r = a[i];
+                const float kr = std::fma(k, r, piston);
+                const float arg = kr + focal * (r * r);
+                const float cs = (float)std::cos((double)arg);
+                const float sn = (float)std::sin((double)arg);
+                const float vr = std::nearbyint(16383.0f * cs);
+                const float vi = std::nearbyint(16383.0f * sn);
+                re[i] = (short)std::max(-32768.f, std::min(32767.f, vr));
+                im[i] = (short)std::max(-32768.f, std::min(32767.f, vi));
+                if (outF) {
+                    float* f = outF->data() + (size_t)pol * 2 * (nx + ny) + (re - o);
+                    f[i] = cs;
+                    f[i + (im - re)] = sn;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ device
+
+int objInitDevice(Object& o) {
+    if (o.device >= 0) {
+        cudaSetDevice(o.device);
+        return ERR_SUCCESS;
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return fail(o, ERR_ERROR, "no CUDA device available: digholo_b200 runs on the GPU only");
+    int dev = 0;
+    DH_CUDA(o, cudaGetDevice(&dev));
+    o.device = dev;
+    if (!o.stream) DH_CUDA(o, cudaStreamCreateWithFlags(&o.stream, cudaStreamNonBlocking));
+    DH_CUDA(o, cudaStreamCreateWithFlags(&o.copyStream, cudaStreamNonBlocking));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy[0], cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy[1], cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventCreate(&o.evStart));
+    DH_CUDA(o, cudaEventCreate(&o.evStop));
+    for (auto& e : o.evStage) DH_CUDA(o, cudaEventCreate(&e));
+    // twiddle(k) = exp(-2 pi i k / 4096), double precision rounded to float
+    std::vector<float> tw(2 * 4096);
+    for (int k = 0; k < 4096; k++) {
+        const double a = -2.0 * PI_D * (double)k / 4096.0;
+        tw[2 * k] = (float)std::cos(a);
+        tw[2 * k + 1] = (float)std::sin(a);
+    }
+    DH_CUDA(o, o.dTwiddle.ensure(tw.size() * sizeof(float)));
+    DH_CUDA(o, cudaMemcpy(o.dTwiddle.ptr, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return ERR_SUCCESS;
+}
+
+static int isDevicePointer(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Checks the configuration against what the fused kernels support.
+static int checkSupported(Object& o) {
+    const Geometry& g = o.geo;
+    if (!isPow2(g.W) || !isPow2(g.H) || g.W > 2048 || g.H > 2048)
+        return fail(o, ERR_INVALIDDIMENSION, "FFT window sides must be powers of two up to 2048 on this build");
+    if (!isPow2(g.w) || !isPow2(g.h))
+        return fail(o, ERR_INVALIDDIMENSION, "IFFT window sides must be powers of two on this build");
+    if (o.avgCount != 1) return fail(o, ERR_INVALIDARGUMENT, "frame averaging (avgCount > 1) is not supported on this build");
+    if (o.framesTransposed) return fail(o, ERR_INVALIDARGUMENT, "transposed uint16 input is not supported on this build");
+    return ERR_SUCCESS;
+}
+
+static int colChunkFor(const Geometry& g) {
+    // Keep the column buffer of the forward kernel within 128 KB.
+    int wc = g.w;
+    while ((size_t)g.H * wc * sizeof(float2) > 128 * 1024 && wc > 1) wc >>= 1;
+    return wc;
+}
+
+// Resolve the frame source for frames [f0, f1): device pointer in place, or
+// a strided copy of the FFT windows from host memory into the staging buffer.
+static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
+    const Geometry& g = o.geo;
+    const int P = o.polCount;
+    const size_t es = o.framesU16 ? 2 : 4;
+    if (o.framesOnDevice) {
+        fp.frames = o.frames;
+        fp.frameWidth = o.cfg.frameWidth;
+        fp.frameStride = (long long)o.cfg.frameWidth * o.cfg.frameHeight;
+        for (int p = 0; p < P; p++) { fp.cx[p] = g.cx[p]; fp.cy[p] = g.cy[p]; }
+        return ERR_SUCCESS;
+    }
+    const size_t frameBytes = (size_t)P * g.H * g.W * es;
+    DH_CUDA(o, o.dFrames.ensure(frameBytes * (size_t)o.batchCount));
+    for (int p = 0; p < P; p++) {
+        cudaMemcpy3DParms m;
+        memset(&m, 0, sizeof(m));
+        m.srcPtr = make_cudaPitchedPtr(const_cast<void*>(o.frames), (size_t)o.cfg.frameWidth * es,
+                                       (size_t)o.cfg.frameWidth * es, (size_t)o.cfg.frameHeight);
+        m.srcPos = make_cudaPos((size_t)g.cx[p] * es, (size_t)g.cy[p], (size_t)f0);
+        m.dstPtr = make_cudaPitchedPtr(o.dFrames.ptr, (size_t)g.W * es, (size_t)g.W * es, (size_t)P * g.H);
+        m.dstPos = make_cudaPos(0, (size_t)p * g.H, (size_t)f0);
+        m.extent = make_cudaExtent((size_t)g.W * es, (size_t)g.H, (size_t)(f1 - f0));
+        m.kind = cudaMemcpyHostToDevice;
+        DH_CUDA(o, cudaMemcpy3DAsync(&m, async ? o.copyStream : o.stream));
+    }
+    fp.frames = o.dFrames.ptr;
+    fp.frameWidth = g.W;
+    fp.frameStride = (long long)P * g.H * g.W;
+    for (int p = 0; p < P; p++) { fp.cx[p] = 0; fp.cy[p] = p * g.H; }
+    return ERR_SUCCESS;
+}
+
+static void forwardParams(Object& o, DhFwdParams& fp) {
+    const Config& c = o.cfg;
+    const Geometry& g = o.geo;
+    memset(&fp, 0, sizeof(fp));
+    fp.inputU16 = o.framesU16;
+    fp.polCount = o.polCount;
+    fp.logW = ilog2(g.W);
+    fp.logH = ilog2(g.H);
+    fp.w = g.w;
+    fp.h = g.h;
+    fp.colChunk = colChunkFor(g);
+    const float lam = c.wavelengthCentre;
+    const float k0 = 2 * PI_F / lam;                       // digHolo.cpp:8626
+    const float ap = c.apertureSize * UNIT_ANGLE;
+    const float kr = k0 * sinf(ap);
+    for (int p = 0; p < o.polCount; p++) {
+        fp.sx0[p] = g.SX[p] - g.W / 2;
+        fp.sy[p] = g.SY[p];
+        const int cx0 = (g.cx[p] + g.W / 2) - c.frameWidth / 2;   // digHolo.cpp:8580-8584
+        const int cy0 = (g.cy[p] + g.H / 2) - c.frameHeight / 2;
+        fp.bcx[p] = c.beamCentreX[p] - (cx0) * c.pixelSize;
+        fp.bcy[p] = c.beamCentreY[p] - (cy0) * c.pixelSize;
+        const float tx = c.zern[p][ZERN_TILTX] * UNIT_ANGLE;       // digHolo.cpp:8588-8589
+        const float ty = c.zern[p][ZERN_TILTY] * UNIT_ANGLE;
+        fp.kx0[p] = k0 * sinf(tx);
+        fp.ky0[p] = k0 * sinf(ty);
+        fp.r02[p] = kr * kr;
+    }
+    fp.kyShift = fabsf((g.ky[1] - g.ky[0]) * g.H);
+    const double fftLength = 1.0 * g.W * g.H;
+    const double ifftLength = c.resolutionIdx ? 1.0 * g.w * g.h : fftLength;
+    fp.norm = (float)(1.0 / sqrt(fftLength * ifftLength));
+    fp.halfPixel = 0.5f * c.pixelSize;
+    fp.fillFactor = c.fillFactorCorrection;
+    fp.kxAxis = o.dKx.as<float>();
+    fp.kyAxis = o.dKy.as<float>();
+    if (o.batchCalEnabled && o.batchCalCount > 0 && o.dBatchCal.ptr) {
+        fp.batchCal = o.dBatchCal.as<float2>();
+        fp.batchCalCount = o.batchCalCount;
+    }
+    fp.window = o.dWindow.as<float2>();
+    fp.twiddle = o.dTwiddle.as<float2>();
+}
+
+// digHoloFFT_SetWindow + digHoloIFFT_SetWindow: geometry, axes, buffers.
+static int prepare(Object& o) {
+    int r = objInitDevice(o);
+    if (r) return r;
+    Config& c = o.cfg;
+    if (!o.frames) return fail(o, ERR_NULLPOINTER, "frame buffer not set");
+    if (c.batchCount <= 0) c.batchCount = 1;
+    o.batchCount = c.batchCount;
+    o.avgCount = c.avgCount;
+    o.polCount = c.polCount;
+    // the reference stores the default window size back into the config (digHolo.cpp:7283-7290)
+    if (c.fftWindowSizeX <= 0) c.fftWindowSizeX = c.frameWidth / c.polCount;
+    if (c.fftWindowSizeY <= 0) c.fftWindowSizeY = c.frameHeight;
+    fftWindowGeometry(c, o.polCount, o.geo);
+    ifftWindowGeometry(c, o.polCount, o.geo);
+    r = checkSupported(o);
+    if (r) return r;
+    const Geometry& g = o.geo;
+    if (!o.framesOnDevice) {
+        o.framesOnDevice = isDevicePointer(o.frames);
+    }
+    if (o.framesOnDevice) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(o.frames);
+        if (a % 16) return fail(o, ERR_INVALIDARGUMENT, "device frame buffer must be 16-byte aligned");
+    }
+    DH_CUDA(o, o.dKx.ensure(g.W * sizeof(float)));
+    DH_CUDA(o, o.dKy.ensure(g.H * sizeof(float)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dKx.ptr, g.kx.data(), g.W * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.dKy.ptr, g.ky.data(), g.H * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    DH_CUDA(o, o.dX.ensure(g.nx * sizeof(float)));
+    DH_CUDA(o, o.dY.ensure(g.ny * sizeof(float)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dX.ptr, g.x.data(), g.nx * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.dY.ptr, g.y.data(), g.ny * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    const size_t B = (size_t)o.batchCount, P = (size_t)o.polCount;
+    DH_CUDA(o, o.dWindow.ensure(B * P * g.w * g.h * sizeof(float2)));
+    const size_t npix = (size_t)g.nx * g.ny;
+    DH_CUDA(o, o.dFieldR.ensure(B * P * npix * sizeof(short)));
+    DH_CUDA(o, o.dFieldI.ensure(B * P * npix * sizeof(short)));
+    if (o.keepField32) DH_CUDA(o, o.dField32.ensure(B * P * npix * sizeof(float2)));
+    DH_CUDA(o, o.dStats.ensure((size_t)ANALYSIS_COUNT * P * (B + 1) * sizeof(float)));
+    if (o.batchCalEnabled && o.batchCalCount > 0) {
+        const size_t n = o.batchCal.size() * sizeof(float);
+        DH_CUDA(o, o.dBatchCal.ensure(n));
+        DH_CUDA(o, cudaMemcpyAsync(o.dBatchCal.ptr, o.batchCal.data(), n, cudaMemcpyHostToDevice, o.stream));
+    }
+    // reference wave (cached inputs are cheap to recompute on the host)
+    std::vector<short> ref;
+    std::vector<float> refF;
+    referenceWave(c, o.polCount, g, ref, &refF);
+    DH_CUDA(o, o.dRef.ensure(ref.size() * sizeof(short)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dRef.ptr, ref.data(), ref.size() * sizeof(short), cudaMemcpyHostToDevice, o.stream));
+    DH_CUDA(o, o.dRefF.ensure(refF.size() * sizeof(float)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dRefF.ptr, refF.data(), refF.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    // the pageable source must stay alive until the copy completes
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    return ERR_SUCCESS;
+}
+
+// HG basis on the reconstructed-plane axes (digHolo.cpp:10506-10645).
+static int updateBasis(Object& o) {
+    Config& c = o.cfg;
+    const Geometry& g = o.geo;
+    const int G = c.maxMG;
+    const int P = o.polCount;
+    if (G <= 0) { o.modeCount = 0; return ERR_SUCCESS; }
+    float waist[POLMAX] = {c.waist[0], c.waist[1]};
+    for (int p = 0; p < P; p++) if (waist[p] == 0) waist[p] = 400e-6f;
+    if (c.polLockBasisWaist) { waist[1] = waist[0]; c.waist[1] = c.waist[0]; }
+    const std::vector<float>& xa = c.resolutionIdx ? g.x : g.xFull;
+    const std::vector<float>& ya = c.resolutionIdx ? g.y : g.yFull;
+    const float psx = xa[1] - xa[0];
+    const float psy = ya[1] - ya[0];
+    o.modeCount = G * (G + 1) / 2;
+    if (o.basisNx == g.nx && o.basisNy == g.ny && o.basisMG == G && o.basisPolCount == P &&
+        o.basisWaist[0] == waist[0] && o.basisWaist[1] == waist[1] && o.basisPsx == psx && o.basisPsy == psy)
+        return ERR_SUCCESS;
+    const int nx = g.nx, ny = g.ny;
+    DH_CUDA(o, o.dHgX.ensure((size_t)P * G * nx * sizeof(short)));
+    DH_CUDA(o, o.dHgY.ensure((size_t)P * G * ny * sizeof(short)));
+    DH_CUDA(o, o.dHgScaleX.ensure((size_t)P * G * sizeof(float)));
+    DH_CUDA(o, o.dHgScaleY.ensure((size_t)P * G * sizeof(float)));
+    const bool square = (psx == psy);
+    const int L = std::max(nx, ny);
+    DH_CUDA(o, o.dBasisAxis.ensure((size_t)(nx + ny + L) * sizeof(float) + (size_t)G * L * sizeof(short)));
+    float* dAxis = o.dBasisAxis.as<float>();
+    short* dLong = reinterpret_cast<short*>(dAxis + nx + ny + L);
+    for (int p = 0; p < P; p++) {
+        const int src = (P > 1 && waist[1] == waist[0]) ? 0 : p;
+        short* hx = o.dHgX.as<short>() + (size_t)p * G * nx;
+        short* hy = o.dHgY.as<short>() + (size_t)p * G * ny;
+        float* sx = o.dHgScaleX.as<float>() + (size_t)p * G;
+        float* sy = o.dHgScaleY.as<float>() + (size_t)p * G;
+        if (src != p) {
+            DH_CUDA(o, cudaMemcpyAsync(hx, o.dHgX.as<short>(), (size_t)G * nx * sizeof(short), cudaMemcpyDeviceToDevice, o.stream));
+            DH_CUDA(o, cudaMemcpyAsync(hy, o.dHgY.as<short>(), (size_t)G * ny * sizeof(short), cudaMemcpyDeviceToDevice, o.stream));
+            DH_CUDA(o, cudaMemcpyAsync(sx, o.dHgScaleX.as<float>(), (size_t)G * sizeof(float), cudaMemcpyDeviceToDevice, o.stream));
+            DH_CUDA(o, cudaMemcpyAsync(sy, o.dHgScaleY.as<float>(), (size_t)G * sizeof(float), cudaMemcpyDeviceToDevice, o.stream));
+            continue;
+        }
+        if (square) {
+            // one set of modes on the longer axis; the shorter axis reads its centred sub-range
+            const std::vector<float>& la = nx >= ny ? xa : ya;
+            DH_CUDA(o, cudaMemcpyAsync(dAxis, la.data(), L * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+            DhBasisParams bp{dAxis, L, G, (double)waist[p], dLong, sx, nullptr};
+            DH_CUDA(o, dh_launch_basis(bp, o.stream));
+            DH_CUDA(o, cudaMemcpyAsync(sy, sx, (size_t)G * sizeof(float), cudaMemcpyDeviceToDevice, o.stream));
+            const int off = (L - std::min(nx, ny)) / 2;
+            const int offX = nx >= ny ? 0 : off;
+            const int offY = nx >= ny ? off : 0;
+            DH_CUDA(o, cudaMemcpy2DAsync(hx, nx * sizeof(short), dLong + offX, L * sizeof(short), nx * sizeof(short), G,
+                                         cudaMemcpyDeviceToDevice, o.stream));
+            DH_CUDA(o, cudaMemcpy2DAsync(hy, ny * sizeof(short), dLong + offY, L * sizeof(short), ny * sizeof(short), G,
+                                         cudaMemcpyDeviceToDevice, o.stream));
+        } else {
+            DH_CUDA(o, cudaMemcpyAsync(dAxis, xa.data(), nx * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+            DH_CUDA(o, cudaMemcpyAsync(dAxis + nx, ya.data(), ny * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+            DhBasisParams bx{dAxis, nx, G, (double)waist[p], hx, sx, nullptr};
+            DH_CUDA(o, dh_launch_basis(bx, o.stream));
+            DhBasisParams by{dAxis + nx, ny, G, (double)waist[p], hy, sy, nullptr};
+            DH_CUDA(o, dh_launch_basis(by, o.stream));
+        }
+        DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    }
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    o.basisNx = nx; o.basisNy = ny; o.basisMG = G; o.basisPolCount = P;
+    o.basisWaist[0] = waist[0]; o.basisWaist[1] = waist[1];
+    o.basisPsx = psx; o.basisPsy = psy;
+    return ERR_SUCCESS;
+}
+
+static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
+    const Geometry& g = o.geo;
+    memset(&ip, 0, sizeof(ip));
+    ip.window = o.dWindow.as<float2>();
+    ip.frameCount = o.batchCount;
+    ip.polCount = o.polCount;
+    ip.lowres = o.cfg.resolutionIdx;
+    ip.logW = ilog2(g.W); ip.logH = ilog2(g.H);
+    ip.logw = ilog2(g.w); ip.logh = ilog2(g.h);
+    for (int p = 0; p < o.polCount; p++) { ip.sx0[p] = g.SX[p] - g.W / 2; ip.sy[p] = g.SY[p]; }
+    ip.refWave = o.dRef.as<short>();
+    ip.refWaveF = o.dRefF.as<float>();
+    ip.xAxis = o.dX.as<float>();
+    ip.yAxis = o.dY.as<float>();
+    ip.dA = fabsf(g.x[2] - g.x[1]) * fabsf(g.y[2] - g.y[1]);
+    ip.fieldR = o.dFieldR.as<short>();
+    ip.fieldI = o.dFieldI.as<short>();
+    ip.field32 = o.keepField32 ? o.dField32.as<float2>() : nullptr;
+    ip.stats = o.dStats.as<float>();
+    ip.statsStride = o.batchCount + 1;
+    if (withOverlap && o.modeCount > 0) {
+        ip.maxMG = o.cfg.maxMG;
+        ip.modeCount = o.modeCount;
+        ip.hgX = o.dHgX.as<short>();
+        ip.hgY = o.dHgY.as<short>();
+        ip.hgScaleX = o.dHgScaleX.as<float>();
+        ip.hgScaleY = o.dHgScaleY.as<float>();
+        ip.coefs = o.dCoefs.as<float2>();
+    }
+    ip.twiddle = o.dTwiddle.as<float2>();
+}
+
+static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0, int f0, int f1) {
+    const Geometry& g = o.geo;
+    const int P = o.polCount;
+    DhFwdParams fp = fp0;
+    const size_t es = o.framesU16 ? 2 : 4;
+    fp.frames = static_cast<const char*>(fp0.frames) + (size_t)f0 * fp0.frameStride * es;
+    fp.frameCount = f1 - f0;
+    fp.frameOffset = f0;
+    fp.window = fp0.window + (size_t)f0 * P * g.w * g.h;
+    const int timed = o.timing && fp.frameOffset == 0 && f1 == o.batchCount;
+    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[0], o.stream));
+    DH_CUDA(o, dh_launch_forward(fp, o.stream));
+    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[1], o.stream));
+    if (ip0.fieldR) {
+        DhInvParams ip = ip0;
+        const size_t npix = (size_t)g.nx * g.ny;
+        ip.window = ip0.window + (size_t)f0 * P * g.w * g.h;
+        ip.frameCount = f1 - f0;
+        ip.fieldR = ip0.fieldR + (size_t)f0 * P * npix;
+        ip.fieldI = ip0.fieldI + (size_t)f0 * P * npix;
+        if (ip.field32) ip.field32 = ip0.field32 + (size_t)f0 * P * npix;
+        ip.stats = ip0.stats + f0;
+        if (ip.coefs) ip.coefs = ip0.coefs + (size_t)f0 * P * o.modeCount;
+        DH_CUDA(o, dh_launch_inverse(ip, o.stream));
+    }
+    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[2], o.stream));
+    return ERR_SUCCESS;
+}
+
+int objStageTimes(Object& o, float* ms) {
+    if (!o.timing || !o.evStage[0]) return ERR_NULLPOINTER;
+    DH_CUDA(o, cudaEventSynchronize(o.evStage[2]));
+    DH_CUDA(o, cudaEventElapsedTime(&ms[0], o.evStage[0], o.evStage[1]));
+    DH_CUDA(o, cudaEventElapsedTime(&ms[1], o.evStage[1], o.evStage[2]));
+    return ERR_SUCCESS;
+}
+
+// Full pipeline for the batch: stage -> forward -> inverse (+overlap).
+// With host frames the batch is split in chunks whose window copies overlap
+// the previous chunk's kernels.
+int objProcessBatch(Object& o, int syncCoefs) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    int r = prepare(o);
+    if (r) return r;
+    r = updateBasis(o);
+    if (r) return r;
+    const Geometry& g = o.geo;
+    const int B = o.batchCount, P = o.polCount;
+    if (o.modeCount > 0) DH_CUDA(o, o.dCoefs.ensure((size_t)B * P * o.modeCount * sizeof(float2)));
+    DhFwdParams fp;
+    forwardParams(o, fp);
+    DhInvParams ip;
+    inverseParams(o, ip, 1);
+    // the last stats column (aggregate over the batch) is filled on request
+    if (o.framesOnDevice) {
+        r = stageFrames(o, 0, B, fp, 0);
+        if (r) return r;
+        r = launchChunk(o, fp, ip, 0, B);
+        if (r) return r;
+    } else {
+        // copies of this call must not overwrite the staging buffer while an
+        // earlier call's kernels may still read it
+        DH_CUDA(o, cudaEventRecord(o.evStart, o.stream));
+        DH_CUDA(o, cudaStreamWaitEvent(o.copyStream, o.evStart, 0));
+        const int chunk = std::max(1, std::min(B, (B + 7) / 8));
+        int slot = 0;
+        for (int f0 = 0; f0 < B; f0 += chunk) {
+            const int f1 = std::min(B, f0 + chunk);
+            DhFwdParams fpc = fp;
+            r = stageFrames(o, f0, f1, fpc, 1);
+            if (r) return r;
+            DH_CUDA(o, cudaEventRecord(o.evCopy[slot], o.copyStream));
+            DH_CUDA(o, cudaStreamWaitEvent(o.stream, o.evCopy[slot], 0));
+            r = launchChunk(o, fpc, ip, f0, f1);
+            if (r) return r;
+            slot ^= 1;
+        }
+    }
+    o.processedFFT = o.processedIFFT = o.processedTilt = 1;
+    o.processedOverlap = o.modeCount > 0;
+    o.metricsValid = 0;
+    (void)g;
+    if (syncCoefs) return objCoefsToHost(o);
+    return ERR_SUCCESS;
+}
+
+int objCoefsToHost(Object& o) {
+    if (o.modeCount <= 0 || !o.dCoefs.ptr) {
+        DH_CUDA(o, cudaStreamSynchronize(o.stream));
+        return ERR_SUCCESS;
+    }
+    const size_t n = (size_t)o.batchCount * o.polCount * o.modeCount * sizeof(float2);
+    if (!o.hCoefs.ensure(n)) return fail(o, ERR_MEMORYALLOCATION, "host coefficient buffer");
+    DH_CUDA(o, cudaMemcpyAsync(o.hCoefs.ptr, o.dCoefs.ptr, n, cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    return ERR_SUCCESS;
+}
+
+// Individual steps (digHoloProcessFFT/IFFT/RemoveTilt/BasisExtractCoefs).
+// The forward kernel fuses the FFT with the window copy of the IFFT step, and
+// the inverse kernel fuses the IFFT with the tilt removal and the overlap, so
+// each step runs the fused kernels up to and including its own work.
+int objFFT(Object& o) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    int r = prepare(o);
+    if (r) return r;
+    o.processedFFT = 1;
+    o.processedIFFT = o.processedTilt = o.processedOverlap = 0;
+    return ERR_SUCCESS;
+}
+
+static int runStages(Object& o, int withInverse, int withOverlap) {
+    int r = prepare(o);
+    if (r) return r;
+    if (withOverlap) {
+        r = updateBasis(o);
+        if (r) return r;
+        if (o.modeCount > 0)
+            DH_CUDA(o, o.dCoefs.ensure((size_t)o.batchCount * o.polCount * o.modeCount * sizeof(float2)));
+    }
+    DhFwdParams fp;
+    forwardParams(o, fp);
+    r = stageFrames(o, 0, o.batchCount, fp, 0);
+    if (r) return r;
+    DhInvParams ip;
+    inverseParams(o, ip, withOverlap);
+    if (!withInverse) ip.fieldR = nullptr;
+    r = launchChunk(o, fp, ip, 0, o.batchCount);
+    if (r) return r;
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    return ERR_SUCCESS;
+}
+
+int objIFFT(Object& o) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    int r = runStages(o, 0, 0);
+    if (r) return r;
+    o.processedFFT = o.processedIFFT = 1;
+    o.processedTilt = o.processedOverlap = 0;
+    return ERR_SUCCESS;
+}
+
+int objApplyTilt(Object& o) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    int r = runStages(o, 1, 0);
+    if (r) return r;
+    o.processedFFT = o.processedIFFT = o.processedTilt = 1;
+    o.processedOverlap = 0;
+    return ERR_SUCCESS;
+}
+
+int objOverlap(Object& o) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    if (o.cfg.maxMG <= 0) {
+        o.modeCount = 0;
+        return ERR_SUCCESS;
+    }
+    int r = runStages(o, 1, 1);
+    if (r) return r;
+    o.processedFFT = o.processedIFFT = o.processedTilt = o.processedOverlap = 1;
+    return objCoefsToHost(o);
+}
+
+int objStatsToHost(Object& o) {
+    const int B = o.batchCount, P = o.polCount;
+    const Geometry& g = o.geo;
+    const size_t npix = (size_t)g.nx * g.ny;
+    const size_t n = (size_t)ANALYSIS_COUNT * P * (B + 1);
+    if (!o.hStats.ensure(n * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host stats buffer");
+    if (!o.hBatchSum.ensure((size_t)P * npix * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host batch-sum buffer");
+    DH_CUDA(o, o.dFieldsC64.ensure((size_t)P * npix * sizeof(float)));
+    DH_CUDA(o, dh_launch_batchsum(o.dFieldR.as<short>(), o.dFieldI.as<short>(), o.dStats.as<float>(), B + 1, P, B,
+                                  (int)npix, o.dFieldsC64.as<float>(), o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.hStats.ptr, o.dStats.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.hBatchSum.ptr, o.dFieldsC64.ptr, (size_t)P * npix * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    // Aggregate column [B]: the analysis of the summed intensity (digHolo.cpp:2519-2568).
+    float* s = o.hStats.as<float>();
+    const float* sum = o.hBatchSum.as<float>();
+    const int S = B + 1;
+    const float yShift = fabsf((g.y[1] - g.y[0]) * (float)g.ny);
+    const float dA = fabsf(g.x[2] - g.x[1]) * fabsf(g.y[2] - g.y[1]);
+    for (int p = 0; p < P; p++) {
+        double Pw = 0, cx = 0, cy = 0, cyw = 0, e4 = 0, mx = 0;
+        int mxIdx = -1;
+        for (int y = 0; y < g.ny; y++)
+            for (int x = 0; x < g.nx; x++) {
+                const double I = sum[(size_t)p * npix + (size_t)y * g.nx + x];
+                Pw += I;
+                cx += g.x[x] * I;
+                cy += g.y[y] * I;
+                cyw += (g.y[y] + (g.y[y] < 0 ? yShift : 0.f)) * I;
+                e4 += I * I;
+                const int idx = 2 * y * g.nx + x;
+                if (I >= mx) { mx = I; mxIdx = idx; }
+            }
+        const int per = P * S;
+        const int col = p * S + B;
+        s[0 * per + col] = (float)Pw;
+        s[1 * per + col] = (float)(cx / Pw);
+        s[2 * per + col] = (float)(cy / Pw);
+        s[3 * per + col] = (float)(32767.0 / sqrt(mx));
+        memcpy(&s[4 * per + col], &mxIdx, sizeof(int));
+        s[5 * per + col] = (float)(dA * (Pw * Pw / e4));
+        s[6 * per + col] = (float)(cyw / Pw);
+    }
+    return ERR_SUCCESS;
+}
+
+int objFieldsToHost(Object& o, int complexOut) {
+    const Geometry& g = o.geo;
+    const size_t npix = (size_t)g.nx * g.ny;
+    const size_t n = (size_t)o.batchCount * o.polCount * npix;
+    if (complexOut) {
+        if (!o.hFields.ensure(n * sizeof(float2))) return fail(o, ERR_MEMORYALLOCATION, "host field buffer");
+        DH_CUDA(o, o.dFieldsC64.ensure(n * sizeof(float2)));
+        DH_CUDA(o, dh_launch_fields_to_c64(o.dFieldR.as<short>(), o.dFieldI.as<short>(), o.dStats.as<float>(),
+                                           o.batchCount + 1, o.polCount, o.batchCount, (int)npix,
+                                           o.dFieldsC64.as<float2>(), o.stream));
+        DH_CUDA(o, cudaMemcpyAsync(o.hFields.ptr, o.dFieldsC64.ptr, n * sizeof(float2), cudaMemcpyDeviceToHost, o.stream));
+    } else {
+        if (!o.hFieldR.ensure(2 * n * sizeof(short))) return fail(o, ERR_MEMORYALLOCATION, "host int16 field buffer");
+        DH_CUDA(o, cudaMemcpyAsync(o.hFieldR.ptr, o.dFieldR.ptr, n * sizeof(short), cudaMemcpyDeviceToHost, o.stream));
+        DH_CUDA(o, cudaMemcpyAsync(o.hFieldR.as<short>() + n, o.dFieldI.ptr, n * sizeof(short), cudaMemcpyDeviceToHost, o.stream));
+    }
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    return objStatsToHost(o);
+}
+
+int objWindowToHost(Object& o) {
+    const Geometry& g = o.geo;
+    const size_t n = (size_t)o.batchCount * o.polCount * g.w * g.h;
+    if (!o.hWindow.ensure(n * sizeof(float2))) return fail(o, ERR_MEMORYALLOCATION, "host window buffer");
+    DH_CUDA(o, cudaMemcpyAsync(o.hWindow.ptr, o.dWindow.ptr, n * sizeof(float2), cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    return ERR_SUCCESS;
+}
+
+}  // namespace dh

@@ -1,0 +1,165 @@
+// Per-handle state of the digholo_b200 runtime: the user configuration (the
+// fields of digHoloConfig, digHolo.cpp:3323-3372), the derived window
+// geometry, the device buffers and the host mirrors returned to callers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dh_params.h"
+
+namespace dh {
+
+// Error codes and constants of the public interface (digHolo.h:171-182, 1363-1372, 1624-1631).
+enum {
+    ERR_SUCCESS = 0, ERR_ERROR = 1, ERR_INVALIDHANDLE = 2, ERR_NULLPOINTER = 3,
+    ERR_INVALIDDIMENSION = 5, ERR_INVALIDPOLARISATION = 6, ERR_INVALIDAXIS = 7,
+    ERR_INVALIDARGUMENT = 8, ERR_MEMORYALLOCATION = 9
+};
+constexpr int POLMAX = 2;
+constexpr int ANALYSIS_COUNT = 7;
+constexpr int METRIC_COUNT = 9;
+constexpr int METRIC_IL = 0, METRIC_MDL = 1, METRIC_DIAG = 2, METRIC_SNRAVG = 3, METRIC_DIAGBEST = 4,
+              METRIC_DIAGWORST = 5, METRIC_SNRBEST = 6, METRIC_SNRWORST = 7, METRIC_SNRMG = 8;
+constexpr int ZERN_TILTX = 1, ZERN_TILTY = 2, ZERN_DEFOCUS = 4;
+
+struct Config {
+    int frameWidth = 320;
+    int frameHeight = 256;
+    float pixelSize = 20e-6f;
+    float apertureSize = 0.4f;          // Fourier window radius, degrees
+    int resolutionIdx = 0;              // 0 full resolution, 1 window-size IFFT
+    float waist[POLMAX] = {510.f, 510.f};
+    float zern[POLMAX][6] = {{0, -0.75f, 0.75f, 0, 0, 0}, {0, -0.75f, 0.75f, 0, 0, 0}};
+    float beamCentreX[POLMAX] = {0.f, 0.f};
+    float beamCentreY[POLMAX] = {0.f, 0.f};
+    int batchCount = 0;
+    int avgCount = 1;
+    int avgMode = 0;
+    float wavelengthCentre = 1565e-9f;
+    int wavelengthOrdering[2] = {0, 0};
+    int polLockTilt = 0;
+    int polLockBasisWaist = 1;
+    int polLockDefocus = 0;
+    int polCount = 1;
+    int autoAlignTilt = 1, autoAlignDefocus = 1, autoAlignCentre = 1, autoAlignBasisWaist = 1;
+    int autoAlignFourierWindowRadius = 1, autoAlignPolIndependence = 0, autoAlignBasisMulConjTrans = 0;
+    float autoAlignTol = 0.f;
+    int autoAlignMode = 0;
+    int fillFactorCorrection = 1;
+    int autoAlignGoalIdx = 0;
+    int fftWindowSizeX = 0;
+    int fftWindowSizeY = 0;
+    int fftwPlanMode = 0;
+    int maxMG = 0;
+    int basisType = 0;
+    int verbosity = 0;
+    int threadCount = 1;
+};
+
+// Grow-only device allocation.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n);
+    void release();
+    ~DevBuf() { release(); }
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Grow-only pinned host allocation (host mirrors of returned arrays).
+struct HostBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool ensure(size_t n);
+    void release();
+    ~HostBuf() { release(); }
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Geometry of the FFT and IFFT windows, computed with the reference's
+// float32 arithmetic (digHolo.cpp:7267-7378, 7868-8048, 8183-8203).
+struct Geometry {
+    int W = 0, H = 0;                 // FFT window
+    int cx[POLMAX] = {0, 0}, cy[POLMAX] = {0, 0};
+    int w = 0, h = 0;                 // IFFT window
+    int SX[POLMAX] = {0, 0}, SY[POLMAX] = {0, 0};
+    int nx = 0, ny = 0;               // reconstructed field
+    std::vector<float> kx, ky;        // fftshifted Fourier axes (W, H)
+    std::vector<float> x, y;          // reconstructed-plane axes (nx, ny)
+    std::vector<float> xFull, yFull;  // FFT-window camera axes (W, H)
+};
+
+struct Object {
+    Config cfg;
+    std::mutex lock;
+
+    // frame source (digHoloSetBatch* store the pointer, digHolo.cpp:4401-4463)
+    const void* frames = nullptr;
+    int framesU16 = 0;
+    int framesTransposed = 0;
+    int framesOnDevice = 0;
+
+    // batch calibration (digHolo.cpp:4468-4500)
+    std::vector<float> batchCal;  // [pol][count] complex interleaved
+    int batchCalPolCount = 0, batchCalCount = 0, batchCalEnabled = 0;
+
+    // processed state
+    int batchCount = 0, avgCount = 1, polCount = 1;
+    int modeCount = 0;
+    int processedFFT = 0, processedIFFT = 0, processedTilt = 0, processedOverlap = 0;
+    Geometry geo;
+
+    // device state
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evCopy[2] = {nullptr, nullptr};
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    int userStream = 0;                 // stream supplied by digHoloB200SetStream (not owned)
+    int timing = 0;                     // record per-stage events in ProcessBatch
+    cudaEvent_t evStage[3] = {nullptr, nullptr, nullptr};
+    float stageMs[2] = {0.f, 0.f};      // forward, inverse of the last timed batch
+    DevBuf dTwiddle, dFrames, dWindow, dFieldR, dFieldI, dField32, dStats, dCoefs;
+    DevBuf dKx, dKy, dX, dY, dRef, dRefF, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
+    // basis cache key
+    int basisNx = 0, basisNy = 0, basisMG = 0;
+    float basisWaist[POLMAX] = {0.f, 0.f};
+    float basisPsx = 0.f, basisPsy = 0.f;
+    int basisPolCount = 0;
+    int keepField32 = 0;
+
+    // host mirrors
+    HostBuf hCoefs, hFields, hFieldR, hFieldI, hStats, hStatsFFT, hWindow, hBatchSum;
+    std::vector<float> hX, hY;
+    float autoAlignMetrics[METRIC_COUNT][2] = {};
+    int metricsValid = 0;
+    std::string lastError;
+};
+
+// Runtime entry points used by the C ABI layer.
+int objInitDevice(Object& o);
+int objFFT(Object& o);
+int objIFFT(Object& o);
+int objApplyTilt(Object& o);
+int objOverlap(Object& o);
+int objProcessBatch(Object& o, int syncCoefs);
+int objCoefsToHost(Object& o);
+int objFieldsToHost(Object& o, int complexOut);
+int objStatsToHost(Object& o);
+int objWindowToHost(Object& o);
+int objStageTimes(Object& o, float* ms);
+
+// Geometry helpers (host, float32 emulation of the reference).
+void fftWindowGeometry(const Config& c, int polCount, Geometry& g);
+void ifftWindowGeometry(const Config& c, int polCount, Geometry& g);
+void referenceWave(const Config& c, int polCount, const Geometry& g, std::vector<short>& out,
+                   std::vector<float>* outF = nullptr);
+bool isPow2(int v);
+int ilog2(int v);
+
+}  // namespace dh

@@ -1,0 +1,80 @@
+// Launch parameters shared by the host runtime (dh_runtime.cpp) and the
+// kernels (dh_kernels.cu).  Plain structs, passed by value to kernels.
+#pragma once
+#include <stdint.h>
+
+#define DH_MAXPOL 2
+
+// Forward stage: frame window -> pruned R2C FFT -> Fourier window with the
+// reference's window operations (digHolo.cpp:6986-7260 and 1808-2122).
+struct DhFwdParams {
+    const void* frames;     // device pointer to the batch, uint16 or float32
+    int inputU16;           // 1: uint16 pixels, 0: float32 pixels
+    int frameWidth;         // pixels per frame row
+    long long frameStride;  // pixels between frames
+    int frameCount;         // frames to process (batchCount * avgCount)
+    int polCount;
+    int logW, logH;         // FFT window is 2^logW x 2^logH
+    int cx[DH_MAXPOL], cy[DH_MAXPOL];   // FFT window corner in the frame
+    int w, h;               // IFFT window size
+    int colChunk;           // columns of the IFFT window handled per block (divides w)
+    int sx0[DH_MAXPOL];     // first kx column of the IFFT window (SX - W/2)
+    int sy[DH_MAXPOL];      // SY (row origin in fftshifted coordinates)
+    float bcx[DH_MAXPOL], bcy[DH_MAXPOL];   // beam centre relative to FFT window centre (m)
+    float kx0[DH_MAXPOL], ky0[DH_MAXPOL];   // window centre k0*sin(tilt)
+    float r02[DH_MAXPOL];                   // (k0*sin(radius))^2
+    float kyShift;          // |dky * H|, the unwrapped-row offset for the mask
+    float norm;             // 1/sqrt(W*H*ifftLength)
+    float halfPixel;        // pixelSize / 2
+    int fillFactor;         // apply x/sin(x) in kx and ky
+    const float* kxAxis;    // fftshifted kx axis (W)
+    const float* kyAxis;    // fftshifted ky axis (H)
+    const float2* batchCal; // optional per-frame complex factor [pol][batchCalCount]
+    int batchCalCount;
+    int frameOffset;        // index of frame 0 of this launch within the batch
+    float2* window;         // out: [frame][pol][h][w]
+    const float2* twiddle;  // TW_N twiddles
+};
+
+// Inverse stage: Fourier window -> IFFT -> field statistics -> reference wave,
+// -conj, int16 rounding -> separable HG overlap
+// (digHolo.cpp:8558-8760, 8788-9341, 9353-9815).
+struct DhInvParams {
+    const float2* window;   // [frame][pol][h][w]
+    int frameCount, polCount;
+    int lowres;             // 1: field is h x w, 0: field is H x W
+    int logW, logH;         // FFT window (full-res field) sizes
+    int logw, logh;         // IFFT window sizes
+    int sx0[DH_MAXPOL];     // kx column of window column 0 (full-res placement)
+    int sy[DH_MAXPOL];      // row origin for full-res placement
+    const short* refWave;   // [pol][2*(nx+ny)]: Xr, Xi, Yr, Yi (14-bit ints)
+    const float* refWaveF;  // [pol][2*(nx+ny)]: the same wave unquantised, for field32
+    const float* xAxis;     // reconstructed-plane axes (nx, ny)
+    const float* yAxis;
+    float dA;               // pixel area of the reconstructed plane
+    short* fieldR;          // out: [frame][pol][ny][nx]
+    short* fieldI;
+    float2* field32;        // optional out: float field -conj(A.ref) before rounding
+    float* stats;           // out: [param][pol][frameCount+1] (DIGHOLO_ANALYSIS layout)
+    int statsStride;        // frameCount+1 entries per (param, pol)
+    // overlap
+    int maxMG;              // 0: no overlap
+    int modeCount;
+    const short* hgX;       // [pol][maxMG][nx] int16 modes
+    const short* hgY;       // [pol][maxMG][ny]
+    const float* hgScaleX;  // [pol][maxMG]
+    const float* hgScaleY;
+    float2* coefs;          // out: [frame][pol*modeCount + mode]
+    const float2* twiddle;
+};
+
+// FP64 Hermite-Gaussian basis along one axis (digHolo.cpp:1269-1484).
+struct DhBasisParams {
+    const float* axis;   // float axis values
+    int count;           // samples
+    int modes;           // maxMG
+    double w0;
+    short* out16;        // [modes][count]
+    float* scale;        // [modes] float value of one int16 step
+    float* outF;         // optional [modes][count] unquantised float modes
+};
