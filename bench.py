@@ -1,0 +1,461 @@
+#!/usr/bin/env python
+"""Throughput of the digHolo batch path on B200: frames/s through
+FFT -> window -> IFFT -> tilt removal -> HG overlap.
+
+Workload (the batched dual-polarisation benchmark): 1024 frames of 640x512
+uint16 (12-bit), two polarisations (left/right halves, carriers
++-(0.25, 0.2) Nyquist), 120 HG modes (maxMG 15), waist 250 um, 25 dB SNR,
+FFT window 128x128, IFFT resolution mode 1 (window-sized reconstruction,
+the mode the digHolo header recommends).  Frames are synthetic (seeded, the
+hologram model of digholo_b200/synth.py, generated on the GPU).
+
+One step = digHoloProcessBatch over one batch of 1024 frames.
+  value : frames/s with the frames already resident in HBM
+          (digHoloSetBatchUint16 given a device pointer, outputs left on the
+          device); four different batches rotate so the 268 MB of window
+          pixels they hold exceed the 126 MB L2.
+  e2e   : frames/s through the plain C ABI with the frames in pinned host
+          memory: the window copies host->device and the coefficient copy
+          device->host are inside the timed region.
+Timing: CUDA events on the library's stream (set to torch's current
+stream), W untimed warm-up steps, K timed steps, max over ranks.
+With torchrun each rank processes its own batches (frames are independent:
+weak scaling, no collective on the data path).
+
+--impl reference times the reference's own CPU implementation (the
+reference compiled from its sources into oracle/_ref, FFT stage served by
+this project's FFT library, not FFTW) on the host cores.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "batched_640x512_u16_2pol"
+RES_MODE = 1
+FRAMES = 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", type=int, default=RES_MODE, help="IFFT resolution mode (0 full, 1 window)")
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(mode, frames):
+    """Hologram parameters (beam centres, tilts, window radius) and the matching digHolo configuration."""
+    from digholo_b200 import synth
+    kw = dict(synth.WORKLOADS[WORKLOAD])
+    kw["frame_count"] = 1
+    hol = synth.generate(**kw)
+
+    class Cfg:
+        pass
+    c = Cfg()
+    c.frame_width, c.frame_height = hol.frame_width, hol.frame_height
+    c.pixel_size, c.wavelength = hol.pixel_size, hol.wavelength
+    c.pol_count = hol.pol_count
+    c.fft_window = hol.window
+    c.window_radius_deg = hol.radius_deg
+    c.resolution_mode = mode
+    c.max_mg = hol.max_mg
+    c.fill_factor = 1
+    c.pol_lock_tilt = 0
+    c.pol_lock_defocus = 0
+    c.pol_lock_waist = 1
+    c.waist = [hol.waist, hol.waist]
+    c.beam_centre = hol.beam_centres
+    c.tilt_deg = hol.tilts_deg
+    c.defocus = [0.0, 0.0]
+    c.snr_db = synth.WORKLOADS[WORKLOAD]["snr_db"]
+    c.frames = frames
+    return c
+
+
+def torch_frames(cfg, n, seed, device):
+    """The synth.py hologram model evaluated on the GPU (uint16 values stored as int16)."""
+    import torch
+    from digholo_b200 import synth
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    W, H, P, G = cfg.frame_width, cfg.frame_height, cfg.pol_count, cfg.max_mg
+    p = cfg.pixel_size
+    ms, ns = synth.hg_indices(G)
+    M = len(ms)
+    region = W // P
+    xs = (torch.arange(W, device=device, dtype=torch.float64) - W // 2) * p
+    ys = (torch.arange(H, device=device, dtype=torch.float64) - H // 2) * p
+    nyq = math.pi / p
+    clean = torch.empty((n, H, W), device=device, dtype=torch.float32)
+    for pol in range(P):
+        xr = xs[pol * region:(pol + 1) * region]
+        cx, cy = cfg.beam_centre[pol]
+        hx = torch.tensor(synth.hg_modes_1d((xr - cx).cpu().numpy(), cfg.waist[0], G), device=device, dtype=torch.float32)
+        hy = torch.tensor(synth.hg_modes_1d((ys - cy).cpu().numpy(), cfg.waist[0], G), device=device, dtype=torch.float32)
+        sgn = 1.0 if pol == 0 else -1.0
+        kx, ky = sgn * 0.25 * nyq, sgn * 0.2 * nyq
+        ref = (torch.exp(1j * ky * ys)[:, None] * torch.exp(1j * kx * xr)[None, :]).to(torch.complex64)
+        for f0 in range(0, n, 128):
+            f1 = min(n, f0 + 128)
+            c = torch.complex(torch.randn((f1 - f0, M), generator=g, device=device),
+                              torch.randn((f1 - f0, M), generator=g, device=device)) / math.sqrt(2)
+            cm = torch.zeros((f1 - f0, G, G), device=device, dtype=torch.complex64)
+            cm[:, torch.as_tensor(ms, device=device), torch.as_tensor(ns, device=device)] = c
+            s = torch.einsum("fmn,ny,mx->fyx", cm, hy.to(torch.complex64), hx.to(torch.complex64))
+            pw = (s.abs() ** 2).sum(dim=(1, 2), keepdim=True)
+            s = s * torch.sqrt(0.1 * ref.numel() / pw)
+            clean[f0:f1, :, pol * region:(pol + 1) * region] = (ref[None] + s).abs() ** 2
+    sigma = clean.mean() * 10.0 ** (-cfg.snr_db / 20.0)
+    clean += torch.randn(clean.shape, generator=g, device=device) * sigma
+    scale = 4095.0 / clean.max()
+    return torch.clamp(torch.round(clean * scale), 0, 4095).to(torch.int16)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for i, name in enumerate(names):
+                if r[5 + i].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel, mode):
+    """dram bytes per launch of ``kernel`` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_%s_%s_mode%d.md" % (kernel, WORKLOAD, mode))
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def reference_run(cfg, frames_host, seconds, threads):
+    """Time the reference's digHoloProcessBatch on host frames; returns frames/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes as C
+    import ref_lib
+    L = ref_lib.load()
+    # one handle per process: the reference crashes when a handle is created
+    # after another was destroyed (seen in its uint16 conversion), so handles
+    # are never destroyed here
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    L.digHoloConfigSetThreadCount(h, threads)
+    n = frames_host.shape[0]
+    L.digHoloSetBatchUint16(h, n, ref_lib.ptr(frames_host, C.c_ushort), 0)
+    b, m, pc = C.c_int(), C.c_int(), C.c_int()
+    L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+    calls = 0
+    t0 = time.perf_counter()
+    while True:
+        L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+        calls += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return n * calls / el, calls, el
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    from digholo_b200 import synth
+    cfg = workload_config(args.mode, args.frames)
+    sample = 256
+    kw = dict(synth.WORKLOADS[WORKLOAD])
+    kw["frame_count"] = sample
+    frames = np.ascontiguousarray(synth.generate(**kw).frames)
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes as C
+    import ref_lib
+    if not ref_lib.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libdigholo_ref.so missing"}))
+        return 0
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    L.digHoloConfigSetThreadCount(h, threads)
+    L.digHoloSetBatchUint16(h, sample, ref_lib.ptr(frames, C.c_ushort), 0)
+    b, m, pc = C.c_int(), C.c_int(), C.c_int()
+    for _ in range(args.warmup):
+        L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+    el = time.perf_counter() - t0
+    fps = sample * args.steps / el
+    line = {
+        "impl": "reference", "metric": "frames/s (FFT->window->IFFT->tilt->HG overlap)", "value": fps,
+        "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded hologram model, numpy)",
+        "config": {"workload": WORKLOAD + "_mode%d" % args.mode, "frames_per_step": sample,
+                   "frame": "640x512 uint16", "pol": 2, "maxMG": 15, "fft_window": "128x128",
+                   "ifft_resolution_mode": args.mode},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "reference",
+                         "sample": "%d frames per step of the %d-frame workload; reference digHolo.cpp compiled "
+                                   "here with this project's FFT library standing in for FFTW" % (sample, FRAMES)},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import digholo_b200
+    L = digholo_b200.load()
+    cfg = workload_config(args.mode, args.frames)
+    B = args.frames
+    P, W, H = cfg.pol_count, cfg.fft_window[0], cfg.fft_window[1]
+    G = cfg.max_mg
+    M = G * (G + 1) // 2
+
+    # four device-resident batches (rotated: their windows exceed L2)
+    batches = [torch_frames(cfg, B, 1000 + 17 * rank + i, device) for i in range(4)]
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(device)
+
+    h = L.digHoloCreate()
+    from digholo_b200 import api
+    api.configure(L, h, cfg)
+    L.digHoloB200SetStream(h, C.c_void_p(stream.cuda_stream))
+    L.digHoloB200SetTiming(h, 1)
+
+    def step_device(i):
+        t = batches[i % 4]
+        L.digHoloSetBatchUint16(h, B, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_ushort)), 0)
+        rc = L.digHoloB200ProcessBatchDevice(h)
+        if rc != 0:
+            raise RuntimeError("ProcessBatchDevice failed: %s" % L.digHoloB200GetLastError(h))
+
+    for i in range(args.warmup):
+        step_device(i)
+    torch.cuda.synchronize()
+    st = (C.c_float * 3)()
+    L.digHoloB200GetStageTimes(h, st)  # reset
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        step_device(i)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    L.digHoloB200GetStageTimes(h, st)
+    fwd_ms, inv_ms, timed = st[0], st[1], st[2]
+
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * B * args.steps / (elapsed_ms / 1e3)
+
+    # end to end through the C ABI with pinned host frames
+    host = torch.empty((B, H_FRAME(cfg), W_FRAME(cfg)), dtype=torch.int16, pin_memory=True)
+    host.copy_(batches[0].cpu())
+    e2e_steps = max(3, min(args.steps, 10))
+    hp = C.cast(C.c_void_p(host.data_ptr()), C.POINTER(C.c_ushort))
+    b, m, pc = C.c_int(), C.c_int(), C.c_int()
+    L.digHoloB200SetTiming(h, 0)
+    for _ in range(2):
+        L.digHoloSetBatchUint16(h, B, hp, 0)
+        L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        L.digHoloSetBatchUint16(h, B, hp, 0)
+        ptr = L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
+        if not ptr:
+            raise RuntimeError("ProcessBatch failed: %s" % L.digHoloB200GetLastError(h))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * B * e2e_steps / (e2e_ms / 1e3)
+    h2d = B * P * W * H * 2
+    d2h = B * P * M * 8
+
+    if rank != 0:
+        L.digHoloDestroy(h)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel (HBM bytes it must move per launch)
+    peak, peak_kind = measured_peaks()
+    geo = (C.c_int * 10)()
+    L.digHoloB200GetGeometry(h, geo)
+    w, hh, nx, ny = geo[2], geo[3], geo[4], geo[5]
+    fwd_bytes = B * (P * W * H * 2 + P * w * hh * 8)
+    inv_bytes = B * (P * w * hh * 8 + P * nx * ny * 4 + P * M * 8 + 7 * P * 4)
+    if fwd_ms >= inv_ms:
+        kname, kbytes, kms = "k_forward", fwd_bytes, fwd_ms / max(timed, 1)
+    else:
+        kname, kbytes, kms = "k_inverse", inv_bytes, inv_ms / max(timed, 1)
+    achieved = kbytes / (kms / 1e3) / 1e9
+    traffic = profile_traffic(kname, args.mode)
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        sample = host[:256].numpy().view(np.uint16)
+        sample = np.ascontiguousarray(sample)
+        threads = os.cpu_count() or 1
+        try:
+            fps, calls, el = reference_run(cfg, sample, 12.0, threads)
+            cpu = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "reference",
+                   "sample": "256 of the 1024 frames, digHoloProcessBatch repeated for %.1f s (%d calls); "
+                             "reference compiled from its sources, FFT by this project's library (not FFTW)"
+                             % (el, calls)}
+        except Exception as exc:  # the reference build may be absent on a box
+            cpu = {"value": None, "unit": "frames/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: %s" % exc}
+
+    line = {
+        "metric": "frames/s (FFT->window->IFFT->tilt->HG overlap)",
+        "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded hologram model, generated on the GPU)",
+        "config": {"workload": WORKLOAD + "_mode%d" % args.mode, "frames_per_step": B,
+                   "frame": "640x512 uint16", "pol": P, "maxMG": G, "modes": M, "fft_window": "%dx%d" % (W, H),
+                   "ifft_resolution_mode": args.mode, "parallelism": "dp%d (independent frames)" % world,
+                   "l2": "4 rotating device batches; their window pixels (268 MB) exceed the 126 MB L2"},
+        "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": kms,
+                     "stage_ms_per_step": {"k_forward": fwd_ms / max(timed, 1), "k_inverse": inv_ms / max(timed, 1)}},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    L.digHoloDestroy(h)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def H_FRAME(cfg):
+    return cfg.frame_height
+
+
+def W_FRAME(cfg):
+    return cfg.frame_width
+
+
+if __name__ == "__main__":
+    sys.exit(main())

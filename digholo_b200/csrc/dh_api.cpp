@@ -187,9 +187,11 @@ int digHoloConfigSetBatchCalibration(int h, complex64* cal, int polCount, int ba
         o->batchCalPolCount = polCount;
         o->batchCalCount = batchCount;
         o->batchCalEnabled = 1;
+        o->batchCalVersion++;
         return dh::ERR_SUCCESS;
     }
     o->batchCalEnabled = 0;
+    o->batchCalVersion++;
     return cal ? dh::ERR_INVALIDARGUMENT : dh::ERR_NULLPOINTER;
 }
 complex64* digHoloConfigGetBatchCalibration(int h, int* polCount, int* batchCount) {
@@ -202,6 +204,7 @@ complex64* digHoloConfigGetBatchCalibration(int h, int* polCount, int* batchCoun
 int digHoloConfigSetBatchCalibrationEnabled(int h, int enabled) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     o->batchCalEnabled = enabled ? 1 : 0;
+    o->batchCalVersion++;
     return dh::ERR_SUCCESS;
 }
 int digHoloConfigGetBatchCalibrationEnabled(int h) { OBJ_OR(h, 0); return o->batchCalEnabled; }
@@ -566,10 +569,28 @@ int digHoloB200SetTiming(int h, int enable) {
     o->timing = enable ? 1 : 0;
     return dh::ERR_SUCCESS;
 }
-// Milliseconds of the forward and inverse kernels of the last timed batch.
-int digHoloB200GetStageTimes(int h, float* msForwardInverse) {
+// Kernel times of the batches processed with timing on since the last call:
+// out[0] forward-kernel ms (sum), out[1] inverse-kernel ms (sum), out[2] count.
+int digHoloB200GetStageTimes(int h, float* out3) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    return dh::objStageTimes(*o, msForwardInverse);
+    return dh::objStageTimes(*o, out3);
+}
+// Window geometry of the last processed batch: out[0..5] = W, H (FFT window),
+// w, h (IFFT window), nx, ny (reconstructed field); out[6..7] = FFT window
+// corner x, y of polarisation 0; out[8..9] = SX, SY of polarisation 0.
+int digHoloB200GetGeometry(int h, int* out10) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    const dh::Geometry& g = o->geo;
+    const int v[10] = {g.W, g.H, g.w, g.h, g.nx, g.ny, g.cx[0], g.cy[0], g.SX[0], g.SY[0]};
+    for (int i = 0; i < 10; i++) out10[i] = v[i];
+    return dh::ERR_SUCCESS;
+}
+// Selects the forward kernel: 0 = fastest available (default), 1 = always
+// the shared-memory kernel (used by the tests to cover both).
+int digHoloB200SetForwardKernel(int h, int generic) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    o->forceGeneric = generic ? 1 : 0;
+    return dh::ERR_SUCCESS;
 }
 // Last error message of the handle (empty when none).
 const char* digHoloB200GetLastError(int h) {

@@ -12,6 +12,8 @@
 
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_forward_reg_init(const float2* hostTwiddle);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
@@ -243,7 +245,6 @@ int objInitDevice(Object& o) {
     DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy[1], cudaEventDisableTiming));
     DH_CUDA(o, cudaEventCreate(&o.evStart));
     DH_CUDA(o, cudaEventCreate(&o.evStop));
-    for (auto& e : o.evStage) DH_CUDA(o, cudaEventCreate(&e));
     // twiddle(k) = exp(-2 pi i k / 4096), double precision rounded to float
     std::vector<float> tw(2 * 4096);
     for (int k = 0; k < 4096; k++) {
@@ -253,6 +254,7 @@ int objInitDevice(Object& o) {
     }
     DH_CUDA(o, o.dTwiddle.ensure(tw.size() * sizeof(float)));
     DH_CUDA(o, cudaMemcpy(o.dTwiddle.ptr, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice));
+    DH_CUDA(o, dh_forward_reg_init(reinterpret_cast<const float2*>(tw.data())));
     return ERR_SUCCESS;
 }
 
@@ -387,6 +389,10 @@ static int prepare(Object& o) {
         const uintptr_t a = reinterpret_cast<uintptr_t>(o.frames);
         if (a % 16) return fail(o, ERR_INVALIDARGUMENT, "device frame buffer must be 16-byte aligned");
     }
+    if (o.preparedValid && memcmp(&o.preparedCfg, &c, sizeof(Config)) == 0 && o.preparedKeep32 == o.keepField32 &&
+        o.preparedU16 == o.framesU16 && o.preparedBatchCal == o.batchCalVersion)
+        return ERR_SUCCESS;
+    o.preparedValid = 0;
     DH_CUDA(o, o.dKx.ensure(g.W * sizeof(float)));
     DH_CUDA(o, o.dKy.ensure(g.H * sizeof(float)));
     DH_CUDA(o, cudaMemcpyAsync(o.dKx.ptr, g.kx.data(), g.W * sizeof(float), cudaMemcpyHostToDevice, o.stream));
@@ -415,8 +421,13 @@ static int prepare(Object& o) {
     DH_CUDA(o, cudaMemcpyAsync(o.dRef.ptr, ref.data(), ref.size() * sizeof(short), cudaMemcpyHostToDevice, o.stream));
     DH_CUDA(o, o.dRefF.ensure(refF.size() * sizeof(float)));
     DH_CUDA(o, cudaMemcpyAsync(o.dRefF.ptr, refF.data(), refF.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    // the pageable source must stay alive until the copy completes
+    // the pageable sources must stay alive until the copies complete
     DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    o.preparedCfg = c;
+    o.preparedKeep32 = o.keepField32;
+    o.preparedU16 = o.framesU16;
+    o.preparedBatchCal = o.batchCalVersion;
+    o.preparedValid = 1;
     return ERR_SUCCESS;
 }
 
@@ -534,9 +545,26 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
     fp.frameOffset = f0;
     fp.window = fp0.window + (size_t)f0 * P * g.w * g.h;
     const int timed = o.timing && fp.frameOffset == 0 && f1 == o.batchCount;
-    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[0], o.stream));
-    DH_CUDA(o, dh_launch_forward(fp, o.stream));
-    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[1], o.stream));
+    cudaEvent_t* ev = nullptr;
+    if (timed) {
+        if ((int)o.evStage.size() < 3 * (o.evStageUsed + 1)) {
+            for (int i = 0; i < 3; i++) {
+                cudaEvent_t e;
+                DH_CUDA(o, cudaEventCreate(&e));
+                o.evStage.push_back(e);
+            }
+        }
+        ev = &o.evStage[3 * o.evStageUsed];
+        o.evStageUsed++;
+        DH_CUDA(o, cudaEventRecord(ev[0], o.stream));
+    }
+    cudaError_t fe = o.forceGeneric ? cudaErrorNotSupported : dh_launch_forward_reg(fp, o.stream);
+    if (fe == cudaErrorNotSupported) {
+        cudaGetLastError();
+        fe = dh_launch_forward(fp, o.stream);
+    }
+    if (fe != cudaSuccess) return failCuda(o, fe, "forward kernel launch");
+    if (timed) DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
     if (ip0.fieldR) {
         DhInvParams ip = ip0;
         const size_t npix = (size_t)g.nx * g.ny;
@@ -549,15 +577,25 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         if (ip.coefs) ip.coefs = ip0.coefs + (size_t)f0 * P * o.modeCount;
         DH_CUDA(o, dh_launch_inverse(ip, o.stream));
     }
-    if (timed) DH_CUDA(o, cudaEventRecord(o.evStage[2], o.stream));
+    if (timed) DH_CUDA(o, cudaEventRecord(ev[2], o.stream));
     return ERR_SUCCESS;
 }
 
-int objStageTimes(Object& o, float* ms) {
-    if (!o.timing || !o.evStage[0]) return ERR_NULLPOINTER;
-    DH_CUDA(o, cudaEventSynchronize(o.evStage[2]));
-    DH_CUDA(o, cudaEventElapsedTime(&ms[0], o.evStage[0], o.evStage[1]));
-    DH_CUDA(o, cudaEventElapsedTime(&ms[1], o.evStage[1], o.evStage[2]));
+// Sums the forward / inverse kernel times of the batches timed since the
+// last call: out = {forward ms, inverse ms, batch count}; then resets.
+int objStageTimes(Object& o, float* out) {
+    out[0] = out[1] = out[2] = 0.f;
+    if (o.evStageUsed == 0) return ERR_SUCCESS;
+    DH_CUDA(o, cudaEventSynchronize(o.evStage[3 * o.evStageUsed - 1]));
+    for (int i = 0; i < o.evStageUsed; i++) {
+        float a = 0.f, b = 0.f;
+        DH_CUDA(o, cudaEventElapsedTime(&a, o.evStage[3 * i], o.evStage[3 * i + 1]));
+        DH_CUDA(o, cudaEventElapsedTime(&b, o.evStage[3 * i + 1], o.evStage[3 * i + 2]));
+        out[0] += a;
+        out[1] += b;
+    }
+    out[2] = (float)o.evStageUsed;
+    o.evStageUsed = 0;
     return ERR_SUCCESS;
 }
 

@@ -122,8 +122,11 @@ struct Object {
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     int userStream = 0;                 // stream supplied by digHoloB200SetStream (not owned)
     int timing = 0;                     // record per-stage events in ProcessBatch
-    cudaEvent_t evStage[3] = {nullptr, nullptr, nullptr};
-    float stageMs[2] = {0.f, 0.f};      // forward, inverse of the last timed batch
+    std::vector<cudaEvent_t> evStage;   // 3 events per timed batch since the last read
+    int evStageUsed = 0;
+    // inputs of the last prepare(): geometry and uploads are reused while they match
+    Config preparedCfg;
+    int preparedValid = 0, preparedKeep32 = -1, preparedU16 = -1, batchCalVersion = 0, preparedBatchCal = -1;
     DevBuf dTwiddle, dFrames, dWindow, dFieldR, dFieldI, dField32, dStats, dCoefs;
     DevBuf dKx, dKy, dX, dY, dRef, dRefF, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
     // basis cache key
@@ -132,6 +135,7 @@ struct Object {
     float basisPsx = 0.f, basisPsy = 0.f;
     int basisPolCount = 0;
     int keepField32 = 0;
+    int forceGeneric = 0;               // use the shared-memory forward kernel for every shape
 
     // host mirrors
     HostBuf hCoefs, hFields, hFieldR, hFieldI, hStats, hStatsFFT, hWindow, hBatchSum;

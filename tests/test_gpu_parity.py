@@ -38,9 +38,10 @@ def lib():
     return digholo_b200.load()
 
 
-def _run(lib, hol, cfg, keep32=False):
+def _run(lib, hol, cfg, keep32=False, generic=0):
     h = lib.digHoloCreate()
     api.configure(lib, h, cfg)
+    lib.digHoloB200SetForwardKernel(h, generic)
     if keep32:
         lib.digHoloB200SetKeepField32(h, 1)
     out = api.run_batch(lib, h, hol.frames)
@@ -54,11 +55,12 @@ def _run(lib, hol, cfg, keep32=False):
     return out
 
 
+@pytest.mark.parametrize("generic", [0, 1])
 @pytest.mark.parametrize("workload,frames,mode", CASES)
-def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode):
+def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, generic):
     hol = make_case(workload, frames)
     cfg = config_for(hol, mode)
-    g = _run(lib, hol, cfg, keep32=True)
+    g = _run(lib, hol, cfg, keep32=True, generic=generic)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert g["R"].shape == o["R"].shape
     np.testing.assert_array_equal(g["x"], o["x"])
