@@ -1,0 +1,323 @@
+/*
+ * digHolo.h -- C ABI of digholo_b200 (libdigholo_b200.so).
+ *
+ * digholo_b200 runs the digHolo batch path -- camera frames -> FFT of the
+ * window around each beam -> off-axis Fourier window -> IFFT -> reference
+ * tilt/defocus removal -> Hermite-Gaussian modal overlap -- as sm_100a CUDA
+ * kernels on one B200.  The entry points below keep the names, argument
+ * meaning, clamping and error returns of the digHolo C interface; each one
+ * cites the declaration it replaces in the reference's digHolo.h.  Unlike
+ * the reference's Linux build (where EXT_C is empty and the exports are
+ * C++-mangled), every name here is exported with C linkage.
+ *
+ * Ownership follows the reference: frame buffers passed to digHoloSetBatch*
+ * stay owned by the caller and are read during processing (host or device
+ * pointers both work); returned arrays are host buffers owned by the handle
+ * and valid until the next processing or configuration call on it.
+ *
+ * The digHoloB200* functions at the end have no counterpart in the
+ * reference: they serve callers whose frames are already in device memory.
+ */
+#ifndef DIGHOLO_B200_H
+#define DIGHOLO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef float complex64[2];               /* digHolo.h:163 */
+
+/* error codes, digHolo.h:171-182 */
+#define DIGHOLO_ERROR_SUCCESS 0
+#define DIGHOLO_ERROR_ERROR 1
+#define DIGHOLO_ERROR_INVALIDHANDLE 2
+#define DIGHOLO_ERROR_NULLPOINTER 3
+#define DIGHOLO_ERROR_SETFRAMEBUFFERDISABLED 4
+#define DIGHOLO_ERROR_INVALIDDIMENSION 5
+#define DIGHOLO_ERROR_INVALIDPOLARISATION 6
+#define DIGHOLO_ERROR_INVALIDAXIS 7
+#define DIGHOLO_ERROR_INVALIDARGUMENT 8
+#define DIGHOLO_ERROR_MEMORYALLOCATION 9
+#define DIGHOLO_ERROR_FILENOTCREATED 10
+#define DIGHOLO_ERROR_FILENOTFOUND 11
+
+/* averaging modes, digHolo.h:655-658 */
+#define DIGHOLO_AVGMODE_SEQUENTIAL 0
+#define DIGHOLO_AVGMODE_INTERLACED 1
+#define DIGHOLO_AVGMODE_SEQUENTIALSWEEP 2
+#define DIGHOLO_AVGMODE_COUNT 3
+
+/* AutoAlign modes, digHolo.h:925-928 */
+#define DIGHOLO_AUTOALIGNMODE_FULL 0
+#define DIGHOLO_AUTOALIGNMODE_TWEAK 1
+#define DIGHOLO_AUTOALIGNMODE_ESTIMATE 2
+#define DIGHOLO_AUTOALIGNMODE_COUNT 3
+
+/* basis types, digHolo.h:1348-1350 */
+#define DIGHOLO_BASISTYPE_HG 0
+#define DIGHOLO_BASISTYPE_LG 1
+#define DIGHOLO_BASISTYPE_CUSTOM 2
+
+/* metrics, digHolo.h:1363-1372 */
+#define DIGHOLO_METRIC_IL 0
+#define DIGHOLO_METRIC_MDL 1
+#define DIGHOLO_METRIC_DIAG 2
+#define DIGHOLO_METRIC_SNRAVG 3
+#define DIGHOLO_METRIC_DIAGBEST 4
+#define DIGHOLO_METRIC_DIAGWORST 5
+#define DIGHOLO_METRIC_SNRBEST 6
+#define DIGHOLO_METRIC_SNRWORST 7
+#define DIGHOLO_METRIC_SNRMG 8
+#define DIGHOLO_METRIC_COUNT 9
+
+/* batch-summary parameters, digHolo.h:1624-1631 */
+#define DIGHOLO_ANALYSIS_TOTALPOWER 0
+#define DIGHOLO_ANALYSIS_COMX 1
+#define DIGHOLO_ANALYSIS_COMY 2
+#define DIGHOLO_ANALYSIS_MAXABS 3
+#define DIGHOLO_ANALYSIS_MAXABSIDX 4
+#define DIGHOLO_ANALYSIS_AEFF 5
+#define DIGHOLO_ANALYSIS_COMYWRAP 6
+#define DIGHOLO_ANALYSIS_COUNT 7
+
+/* verbosity, digHolo.h:1906-1909 */
+#define DIGHOLO_VERBOSITY_OFF 0
+#define DIGHOLO_VERBOSITY_BASIC 1
+#define DIGHOLO_VERBOSITY_DEBUG 2
+#define DIGHOLO_VERBOSITY_COOKED 3
+
+/* replaces digHolo.h:209 */
+int digHoloCreate();
+/* replaces digHolo.h:216 */
+int digHoloDestroy(int handleIdx);
+/* replaces digHolo.h:245 */
+int digHoloSetFrameBuffer(int handleIdx, float* buffer);
+/* replaces digHolo.h:255 */
+float* digHoloGetFrameBuffer(int handleIdx);
+/* replaces digHolo.h:268 */
+int digHoloSetFrameBufferUint16(int handleIdx, unsigned short* buffer, int transposeMode);
+/* replaces digHolo.h:277 */
+unsigned short* digHoloGetFrameBufferUint16(int handleIdx, int* transposeMode);
+/* replaces digHolo.h:298 */
+int digHoloConfigSetFrameDimensions(int handleIdx, int width, int height);
+/* replaces digHolo.h:308 */
+int digHoloConfigGetFrameDimensions(int handleIdx, int* width, int* height);
+/* replaces digHolo.h:317 */
+int digHoloConfigSetFramePixelSize(int handleIdx, float pixelSize);
+/* replaces digHolo.h:325 */
+float digHoloConfigGetFramePixelSize(int handleIdx);
+/* replaces digHolo.h:334 */
+int digHoloConfigSetPolCount(int handleIdx, int polCount);
+/* replaces digHolo.h:344 */
+int digHoloConfigGetPolCount(int handleIdx);
+/* replaces digHolo.h:449 */
+int digHoloConfigSetFillFactorCorrectionEnabled(int handleIdx, int enabled);
+/* replaces digHolo.h:460 */
+int digHoloConfigGetFillFactorCorrectionEnabled(int handleIdx);
+/* replaces digHolo.h:483 */
+int digHoloSetBatch(int handleIdx, int batchCount, float* frameBuffer);
+/* replaces digHolo.h:502 */
+int digHoloSetBatchAvg(int handleIdx, int batchCount, float* frameBuffer, int avgCount, int avgMode);
+/* replaces digHolo.h:519 */
+int digHoloSetBatchUint16(int handleIdx, int batchCount, unsigned short* frameBuffer, int transpose);
+/* replaces digHolo.h:540 */
+int digHoloSetBatchAvgUint16(int handleIdx, int batchCount, unsigned short* frameBuffer, int avgCount, int avgMode, int transpose);
+/* replaces digHolo.h:551 */
+int digHoloConfigSetBatchCount(int handleIdx, int batchCount);
+/* replaces digHolo.h:559 */
+int digHoloConfigGetBatchCount(int handleIdx);
+/* replaces digHolo.h:570 */
+int digHoloConfigSetBatchAvgCount(int handleIdx, int avgCount);
+/* replaces digHolo.h:580 */
+int digHoloConfigGetBatchAvgCount(int handleIdx);
+/* replaces digHolo.h:599 */
+int digHoloConfigSetBatchCalibration(int handleIdx, complex64* cal, int polCount, int batchCount);
+/* replaces digHolo.h:611 */
+complex64* digHoloConfigGetBatchCalibration(int handleIdx, int *polCount, int *batchCount);
+/* replaces digHolo.h:635 */
+int digHoloConfigSetBatchCalibrationEnabled(int handleIdx, int enabled);
+/* replaces digHolo.h:645 */
+int digHoloConfigGetBatchCalibrationEnabled(int handleIdx);
+/* replaces digHolo.h:670 */
+int digHoloConfigSetBatchAvgMode(int handleIdx, int avgMode);
+/* replaces digHolo.h:680 */
+int digHoloConfigGetBatchAvgMode(int handleIdx);
+/* replaces digHolo.h:701 */
+int digHoloConfigSetfftWindowSize(int handleIdx, int width, int height);
+/* replaces digHolo.h:712 */
+int digHoloConfigGetfftWindowSize(int handleIdx, int *width, int *height);
+/* replaces digHolo.h:722 */
+int digHoloConfigSetfftWindowSizeX(int handleIdx, int width);
+/* replaces digHolo.h:730 */
+int digHoloConfigGetfftWindowSizeX(int handleIdx);
+/* replaces digHolo.h:739 */
+int digHoloConfigGetfftWindowSizeY(int handleIdx);
+/* replaces digHolo.h:749 */
+int digHoloConfigSetfftWindowSizeY(int handleIdx, int height);
+/* replaces digHolo.h:766 */
+int digHoloConfigSetFourierWindowRadius(int handleIdx, float windowRadius);
+/* replaces digHolo.h:774 */
+float digHoloConfigGetFourierWindowRadius(int handleIdx);
+/* replaces digHolo.h:786 */
+int digHoloConfigSetIFFTResolutionMode(int handleIdx, int resolutionModeIdx);
+/* replaces digHolo.h:797 */
+int digHoloConfigGetIFFTResolutionMode(int handleIdx);
+/* replaces digHolo.h:814 */
+int digHoloConfigSetWavelengthCentre(int handleIdx, float lambda0);
+/* replaces digHolo.h:822 */
+float digHoloConfigGetWavelengthCentre(int handleIdx);
+/* replaces digHolo.h:938 */
+int digHoloConfigSetAutoAlignBeamCentre(int handleIdx, int enable);
+/* replaces digHolo.h:946 */
+int digHoloConfigGetAutoAlignBeamCentre(int handleIdx);
+/* replaces digHolo.h:955 */
+int digHoloConfigSetAutoAlignDefocus(int handleIdx, int enable);
+/* replaces digHolo.h:963 */
+int digHoloConfigGetAutoAlignDefocus(int handleIdx);
+/* replaces digHolo.h:972 */
+int digHoloConfigSetAutoAlignTilt(int handleIdx, int enable);
+/* replaces digHolo.h:980 */
+int digHoloConfigGetAutoAlignTilt(int handleIdx);
+/* replaces digHolo.h:989 */
+int digHoloConfigSetAutoAlignBasisWaist(int handleIdx, int enable);
+/* replaces digHolo.h:997 */
+int digHoloConfigGetAutoAlignBasisWaist(int handleIdx);
+/* replaces digHolo.h:1008 */
+int digHoloConfigSetAutoAlignFourierWindowRadius(int handleIdx, int enable);
+/* replaces digHolo.h:1016 */
+int digHoloConfigGetAutoAlignFourierWindowRadius(int handleIdx);
+/* replaces digHolo.h:1025 */
+int digHoloConfigSetAutoAlignTol(int handleIdx, float tolerance);
+/* replaces digHolo.h:1033 */
+float digHoloConfigGetAutoAlignTol(int handleIdx);
+/* replaces digHolo.h:1046 */
+int digHoloConfigSetAutoAlignPolIndependence(int handleIdx, int polIndependence);
+/* replaces digHolo.h:1058 */
+int digHoloConfigGetAutoAlignPolIndependence(int handleIdx);
+/* replaces digHolo.h:1071 */
+int digHoloConfigSetAutoAlignBasisMulConjTrans(int handleIdx, int mulConjTranspose);
+/* replaces digHolo.h:1083 */
+int digHoloConfigGetAutoAlignBasisMulConjTrans(int handleIdx);
+/* replaces digHolo.h:1101 */
+int digHoloConfigSetAutoAlignMode(int handleIdx, int alignMode);
+/* replaces digHolo.h:1109 */
+int digHoloConfigGetAutoAlignMode(int handleIdx);
+/* replaces digHolo.h:1128 */
+int digHoloConfigSetAutoAlignGoalIdx(int handleIdx, int goalIdx);
+/* replaces digHolo.h:1136 */
+int digHoloConfigGetAutoAlignGoalIdx(int handleIdx);
+/* replaces digHolo.h:1205 */
+int digHoloConfigSetBeamCentre(int handleIdx, int axisIdx, int polIdx, float centre);
+/* replaces digHolo.h:1215 */
+float digHoloConfigGetBeamCentre(int handleIdx, int axisIdx, int polIdx);
+/* replaces digHolo.h:1226 */
+int digHoloConfigSetTilt(int handleIdx, int axisIdx, int polIdx, float tilt);
+/* replaces digHolo.h:1236 */
+float digHoloConfigGetTilt(int handleIdx, int axisIdx, int polIdx);
+/* replaces digHolo.h:1246 */
+int digHoloConfigSetDefocus(int handleIdx, int polIdx, float defocus);
+/* replaces digHolo.h:1255 */
+float digHoloConfigGetDefocus(int handleIdx, int polIdx);
+/* replaces digHolo.h:1270 */
+int digHoloConfigSetPolLockTilt(int handleIdx, int polLock);
+/* replaces digHolo.h:1282 */
+int digHoloConfigGetPolLockTilt(int handleIdx);
+/* replaces digHolo.h:1297 */
+int digHoloConfigSetPolLockDefocus(int handleIdx, int polLock);
+/* replaces digHolo.h:1309 */
+int digHoloConfigGetPolLockDefocus(int handleIdx);
+/* replaces digHolo.h:1318 */
+int digHoloConfigSetPolLockBasisWaist(int handleIdx, int polLock);
+/* replaces digHolo.h:1326 */
+int digHoloConfigGetPolLockBasisWaist(int handleIdx);
+/* replaces digHolo.h:1384 */
+int digHoloConfigSetBasisGroupCount(int handleIdx, int groupCount);
+/* replaces digHolo.h:1393 */
+int digHoloConfigGetBasisGroupCount(int handleIdx);
+/* replaces digHolo.h:1404 */
+int digHoloConfigSetBasisWaist(int handleIdx, int polIdx, float waist);
+/* replaces digHolo.h:1416 */
+float digHoloConfigGetBasisWaist(int handleIdx, int polIdx);
+/* replaces digHolo.h:1424 */
+int digHoloConfigSetBasisTypeHG(int handleIdx);
+/* replaces digHolo.h:1464 */
+int digHoloConfigSetBasisType(int handleIdx, int basisType);
+/* replaces digHolo.h:1472 */
+int digHoloConfigGetBasisType(int handleIdx);
+/* replaces digHolo.h:1494 */
+complex64* digHoloProcessBatch(int handleIdx, int* batchCount, int* modeCount, int* polCount);
+/* replaces digHolo.h:1549 */
+complex64* digHoloGetFields(int handleIdx, int* batchCount, int* polCount, float** x, float** y, int* width, int* height);
+/* replaces digHolo.h:1568 */
+int digHoloGetFields16(int handleIdx, int* batchCount, int* polCount, short** fieldR, short** fieldI, float** fieldScale, float** x, float** y, int* width, int* height);
+/* replaces digHolo.h:1603 */
+complex64* digHoloBasisGetCoefs(int handleIdx, int* batchCount, int* modeCount, int* polCount);
+/* replaces digHolo.h:1659 */
+int digHoloBatchGetSummary(int handleIdx, int planeIdx, int* parameterCount, int* totalCount, int* polCount, float** parameters, int* pixelCountX, int* pixelCountY, float** xAxis, float** yAxis, float** totalIntensity);
+/* replaces digHolo.h:1670 */
+int digHoloProcessFFT(int handleIdx);
+/* replaces digHolo.h:1682 */
+int digHoloProcessIFFT(int handleIdx);
+/* replaces digHolo.h:1694 */
+int digHoloProcessRemoveTilt(int handleIdx);
+/* replaces digHolo.h:1706 */
+int digHoloProcessBasisExtractCoefs(int handleIdx);
+/* replaces digHolo.h:1732 */
+complex64* digHoloGetFourierPlaneWindow(int handleIdx, int* batchCount, int* polCount, int* width, int* height);
+/* replaces digHolo.h:1749 */
+int digHoloConfigSetThreadCount(int handleIdx, int threadCount);
+/* replaces digHolo.h:1757 */
+int digHoloConfigGetThreadCount(int handleIdx);
+/* replaces digHolo.h:1808 */
+int digHoloConfigSetFFTWPlanMode(int handleIdx, int planningMode);
+/* replaces digHolo.h:1818 */
+int digHoloConfigGetFFTWPlanMode(int handleIdx);
+/* replaces digHolo.h:1924 */
+int digHoloConfigSetVerbosity(int handleIdx, int verbosity);
+/* replaces digHolo.h:1937 */
+int digHoloConfigGetVerbosity(int handleIdx);
+
+/* ------------------------------------------------------------------------
+ * Extensions with no counterpart in the reference.
+ * ---------------------------------------------------------------------- */
+
+/* Runs the batch path on frames already in device memory (digHoloSetBatch*
+ * given a device pointer) and leaves every output on the device; returns
+ * without waiting for the GPU. */
+int digHoloB200ProcessBatchDevice(int handleIdx);
+
+/* Device pointer to the coefficients [batch][pol * mode] of the last batch. */
+complex64* digHoloB200GetCoefsDevice(int handleIdx, int* batchCount, int* modeCount, int* polCount);
+
+/* Waits for the handle's GPU work (DIGHOLO_ERROR_ERROR on a CUDA error). */
+int digHoloB200Synchronize(int handleIdx);
+
+/* Runs the handle's GPU work on a caller-owned cudaStream_t (nullptr: a
+ * private stream).  Call before the first processing. */
+int digHoloB200SetStream(int handleIdx, void* stream);
+
+/* Keep the float field -conj(A.ref) computed with the unquantised reference
+ * wave, next to the int16 field; read it with digHoloB200GetFields32. */
+int digHoloB200SetKeepField32(int handleIdx, int enable);
+complex64* digHoloB200GetFields32(int handleIdx, int* batchCount, int* polCount, int* width, int* height);
+
+/* CUDA-event timing of the forward and inverse kernels: out3 = {forward ms
+ * summed, inverse ms summed, batches} since the previous call. */
+int digHoloB200SetTiming(int handleIdx, int enable);
+int digHoloB200GetStageTimes(int handleIdx, float* out3);
+
+/* Window geometry of the last batch: W, H, w, h, nx, ny, FFT-window corner
+ * (x, y) and IFFT-window origin (SX, SY) of polarisation 0. */
+int digHoloB200GetGeometry(int handleIdx, int* out10);
+
+/* 1: always use the shared-memory forward kernel (testing aid). */
+int digHoloB200SetForwardKernel(int handleIdx, int generic);
+
+/* Message of the handle's last error ("" when none). */
+const char* digHoloB200GetLastError(int handleIdx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIGHOLO_B200_H */
