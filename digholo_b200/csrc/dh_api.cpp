@@ -32,6 +32,8 @@ Object* get(int h) {
 
 #define OBJ_OR(h, ret) Object* o = get(h); if (!o) return ret
 
+dh::Object* dhObjectForHandle(int h) { return get(h); }
+
 extern "C" {
 
 // ------------------------------------------------------------ handles

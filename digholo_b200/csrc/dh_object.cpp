@@ -648,6 +648,65 @@ int objProcessBatch(Object& o, int syncCoefs) {
     return ERR_SUCCESS;
 }
 
+// The batch path with caller-owned outputs and an external window scratch
+// (digHoloB200ProcessBatchNoAlloc).  Allocates nothing: the handle's tables
+// must already match the configuration.
+int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* window, size_t windowBytes,
+                      float2* coefs, short* fieldR, short* fieldI, float* stats) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    if (o.device < 0 || !o.preparedValid)
+        return fail(o, ERR_ERROR, "no-alloc path: process one batch with this configuration first (that call allocates)");
+    cudaSetDevice(o.device);
+    Config a = o.cfg, b = o.preparedCfg;
+    a.batchCount = b.batchCount = 0;
+    if (a.fftWindowSizeX <= 0) a.fftWindowSizeX = a.frameWidth / a.polCount;
+    if (a.fftWindowSizeY <= 0) a.fftWindowSizeY = a.frameHeight;
+    if (memcmp(&a, &b, sizeof(Config)) != 0)
+        return fail(o, ERR_ERROR, "no-alloc path: configuration changed since the handle was prepared");
+    const Geometry& g = o.geo;
+    const int P = o.polCount;
+    if ((size_t)B * P * g.w * g.h * sizeof(float2) > windowBytes)
+        return fail(o, ERR_INVALIDDIMENSION, "no-alloc path: frameCount * polCount * w * h * 8 bytes exceeds the 8 MiB window scratch");
+    if (o.cfg.maxMG > 0) {
+        if (!coefs) return fail(o, ERR_NULLPOINTER, "no-alloc path: coefficient buffer is null");
+        if (o.basisMG != o.cfg.maxMG || o.basisNx != g.nx || o.basisNy != g.ny || o.basisPolCount != P)
+            return fail(o, ERR_ERROR, "no-alloc path: basis not prepared for this configuration");
+    }
+    if (!isDevicePointer(frames) || (reinterpret_cast<uintptr_t>(frames) % 16))
+        return fail(o, ERR_INVALIDARGUMENT, "no-alloc path: frames must be a 16-byte aligned device pointer");
+    const int saveU16 = o.framesU16;
+    o.framesU16 = u16;
+    DhFwdParams fp;
+    forwardParams(o, fp);
+    o.framesU16 = saveU16;
+    fp.frames = frames;
+    fp.frameWidth = o.cfg.frameWidth;
+    fp.frameStride = (long long)o.cfg.frameWidth * o.cfg.frameHeight;
+    for (int p = 0; p < P; p++) { fp.cx[p] = g.cx[p]; fp.cy[p] = g.cy[p]; }
+    fp.frameCount = B;
+    fp.frameOffset = 0;
+    fp.window = window;
+    DhInvParams ip;
+    inverseParams(o, ip, o.cfg.maxMG > 0);
+    ip.window = window;
+    ip.frameCount = B;
+    ip.fieldR = fieldR;
+    ip.fieldI = fieldI;
+    ip.field32 = nullptr;
+    ip.stats = stats;
+    ip.statsStride = B + 1;
+    ip.coefs = o.cfg.maxMG > 0 ? coefs : nullptr;
+    if (!ip.coefs) ip.maxMG = 0;
+    cudaError_t fe = o.forceGeneric ? cudaErrorNotSupported : dh_launch_forward_reg(fp, o.stream);
+    if (fe == cudaErrorNotSupported) {
+        cudaGetLastError();
+        fe = dh_launch_forward(fp, o.stream);
+    }
+    if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
+    DH_CUDA(o, dh_launch_inverse(ip, o.stream));
+    return ERR_SUCCESS;
+}
+
 int objCoefsToHost(Object& o) {
     if (o.modeCount <= 0 || !o.dCoefs.ptr) {
         DH_CUDA(o, cudaStreamSynchronize(o.stream));

@@ -316,6 +316,25 @@ int digHoloB200SetForwardKernel(int handleIdx, int generic);
 /* Message of the handle's last error ("" when none). */
 const char* digHoloB200GetLastError(int handleIdx);
 
+/* No counterpart in the reference.  The batch path for callers that cannot
+ * allocate device memory while they process frames (a real-time acquisition
+ * callback must not block in cudaMalloc/cudaFree, which can synchronise the
+ * device; some applications fix their memory pool at start-up).  Nothing is
+ * allocated: the scratch carrying the Fourier windows between the two
+ * kernels is a static 8 MiB device array, and the caller passes the device
+ * frames and device outputs -- coefs [frame][pol*mode] complex64, fieldR and
+ * fieldI [frame][pol][ny][nx] int16, stats [7][pol][frameCount+1] float (the
+ * aggregate column is not written).  The handle must already hold the tables
+ * for its configuration (process one batch with digHoloProcessBatch or
+ * digHoloB200ProcessBatchDevice first; that call allocates).  Sizes with
+ * frameCount*polCount*w*h*8 bytes above 8 MiB are refused with
+ * DIGHOLO_ERROR_INVALIDDIMENSION.  The first call on a device looks up the
+ * scratch address (cudaGetSymbolAddress): make it before any stream capture.
+ * Calls share the scratch; calls whose GPU work overlaps race on it.
+ * Returns without waiting for the GPU (see digHoloB200Synchronize). */
+int digHoloB200ProcessBatchNoAlloc(int handleIdx, const void* frames, int frameCount, int framesAreUint16,
+                                   complex64* coefs, short* fieldR, short* fieldI, float* stats);
+
 #ifdef __cplusplus
 }
 #endif
