@@ -183,6 +183,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def max_over_ranks(ms, device=None):
+    """Slowest rank's elapsed time (ms); the identity without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_seed(rank, batch_index):
+    """Seed of a rank's synthetic batch: every rank processes its own frames (weak scaling)."""
+    return 1000 + 17 * rank + batch_index
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -307,7 +323,7 @@ def main():
     M = G * (G + 1) // 2
 
     # four device-resident batches (rotated: their windows exceed L2)
-    batches = [torch_frames(cfg, B, 1000 + 17 * rank + i, device) for i in range(4)]
+    batches = [torch_frames(cfg, B, shard_seed(rank, i), device) for i in range(4)]
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream(device)
 
@@ -350,10 +366,7 @@ def main():
     L.digHoloB200GetStageTimes(h, st)
     fwd_ms, inv_ms, timed = st[0], st[1], st[2]
 
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=device, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, device)
     value = world * B * args.steps / (elapsed_ms / 1e3)
 
     # end to end through the C ABI with pinned host frames
@@ -380,10 +393,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, device)
     e2e = world * B * e2e_steps / (e2e_ms / 1e3)
     h2d = B * P * W * H * 2
     d2h = B * P * M * 8

@@ -1,0 +1,88 @@
+"""The oracle (FP64 restatement) pinned against the reference.
+
+* against the committed golden fixtures (outputs of the unmodified reference,
+  tests/golden/make_golden.py), which need no reference build;
+* against the live reference build (oracle/_ref) where it exists.
+
+Tolerances: int16 fields within 2 LSB and field relative L2 <= 5e-5; coefficient
+relative L2 <= 2e-5 (for 16-row fields after removing the scale the
+reference omits, digHolo.cpp:2318-2331); field scales relative <= 1e-5.
+"""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+import digholo_oracle as O
+import ref_lib
+from helpers import config_for, make_case, rel_l2
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _check(o, cfg, coefs, R, I, scale, x, y):
+    np.testing.assert_array_equal(x, o["x"])
+    np.testing.assert_array_equal(y, o["y"])
+    dR = np.abs(R.astype(int) - o["R"])
+    dI = np.abs(I.astype(int) - o["I"])
+    assert max(dR.max(), dI.max()) <= 2
+    assert np.max(np.abs(scale.T - o["scale"]) / o["scale"]) <= 1e-5
+    # one 14-bit reference-wave entry rounded the other way shifts a whole row
+    # or column by 1 LSB, so compare the fields, not the count of differing values
+    f = (R + 1j * I.astype(np.float64)) / scale.T[:, :, None, None]
+    fo = (o["R"] + 1j * o["I"].astype(np.float64)) / o["scale"][:, :, None, None]
+    assert rel_l2(f, fo) <= 5e-5
+    co = o["coefs"]
+    if o["h"] == 16 and cfg.resolution_mode == 1:
+        co = O.reference_unscaled_16(co, cfg, o)
+    assert rel_l2(coefs, co) <= 2e-5
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_oracle_matches_golden(path):
+    d = np.load(path)
+    meta = json.loads(str(d["meta"]))
+    hol = make_case(meta["workload"], meta["frames"])
+    cfg = config_for(hol, meta["mode"])
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    _check(o, cfg, d["coefs"], d["R"], d["I"], d["scale"], d["x"], d["y"])
+
+
+def test_golden_fixtures_present():
+    assert len(GOLDEN) == 4
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_oracle_matches_live_reference(mode):
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    hol = make_case("plain_320x256_f32_1pol", 4)
+    cfg = config_for(hol, mode)
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    r = ref_lib.run_batch(L, h, hol.frames)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
+
+
+def test_exact_and_quantised_flavours_agree():
+    hol = make_case("plain_320x256_f32_1pol", 2)
+    cfg = config_for(hol, 0)
+    q = O.process_batch(hol.frames, cfg, quantised=True)
+    e = O.process_batch(hol.frames, cfg, quantised=False)
+    # the quantisation of the reference (int16 field, 14-bit wave, int16 modes) costs ~5e-5
+    assert rel_l2(q["field"], e["field"]) < 2e-4
+    assert rel_l2(q["coefs"], e["coefs"]) < 1e-4
+
+
+def test_metrics_on_unitary_batch():
+    # a batch whose coefficient matrix is unitary has IL = MDL = 0 dB on both paths
+    rng = np.random.default_rng(7)
+    z = rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))
+    q, _ = np.linalg.qr(z)
+    m = O.power_meter(q.T.reshape(6, 1, 6))
+    assert abs(m["il_db"]) < 1e-9 and abs(m["mdl_db"]) < 1e-9
+    assert abs(m["il_frob_db"]) < 1e-9
