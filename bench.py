@@ -325,7 +325,10 @@ def main():
     # four device-resident batches (rotated: their windows exceed L2)
     batches = [torch_frames(cfg, B, shard_seed(rank, i), device) for i in range(4)]
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream(device)
+    # a dedicated (non-default) stream shared by the library and the timing events
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
 
     h = L.digHoloCreate()
     from digholo_b200 import api

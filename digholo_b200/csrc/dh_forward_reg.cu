@@ -1,30 +1,31 @@
 // Forward stage, register-resident variant for FFT windows up to 128 pixels
-// wide: one thread transforms one window row entirely in registers (packed
-// half-length complex FFT, compile-time twiddles from constant memory, no
-// barriers inside the transform), and the column transform is evaluated only
-// for the IFFT window's rows, as h-point FFTs of the H/h decimated column
-// sequences followed by an H/h-term twiddled sum.
+// wide (same results as k_forward in dh_kernels.cu, and as the reference's
+// FFTW r2c + digHoloCopyWindow, digHolo.cpp:7184-7260 and 1808-2122).
 //
-// Same results as k_forward (dh_kernels.cu) and the reference's
-// FFTW r2c + digHoloCopyWindow (digHolo.cpp:7184-7260, 1808-2122).
+//   1. the window is staged into shared memory with coalesced 16-byte loads;
+//   2. two threads share a row: after the first decimation-in-frequency
+//      stage of the packed half-length complex FFT, each transforms one half
+//      (even or odd outputs) in registers, with literal twiddles;
+//   3. the R2C split is evaluated for the IFFT window's kx columns only;
+//   4. the column transform is evaluated for the IFFT window's h rows only:
+//      h-point register FFTs of the H/h decimated column sequences, then an
+//      H/h-term twiddled sum;
+//   5. the frame-independent window factors (mask, normalisation, inverse
+//      pixel sinc, beam-centre phase) come from a per-configuration table.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
 #include "dh_common.cuh"
 #include "dh_params.h"
+#include "dh_twiddle64.h"
 
 using namespace dh;
 
-// exp(-2 pi i k / 4096), k < 4096, set once by dh_forward_reg_init.
-__constant__ float2 c_tw[TW_N];
-
 namespace {
 
-// In-place radix-2 decimation-in-frequency FFT of N values held in
-// registers: natural-order input, bit-reversed output.  Every index is a
-// compile-time constant, so the twiddles are constant-bank operands and the
-// trivial ones (1, -i) cost nothing.
+// In-place radix-2 decimation-in-frequency FFT of N <= 64 values in
+// registers: natural-order input, bit-reversed output.
 template <int N>
 __device__ __forceinline__ void fftRegDIF(float2 (&v)[N]) {
 #pragma unroll
@@ -37,14 +38,12 @@ __device__ __forceinline__ void fftRegDIF(float2 (&v)[N]) {
                 const float2 b = v[blk + j + m];
                 v[blk + j] = cadd(a, b);
                 const float2 d = csub(a, b);
-                // twiddle exp(-2 pi i j / (2m))
                 if (j == 0) {
                     v[blk + j + m] = d;
                 } else if (2 * j == m) {
                     v[blk + j + m] = make_float2(d.y, -d.x);  // multiply by -i
                 } else {
-                    const float2 w = c_tw[j * (TW_N / (2 * m))];
-                    v[blk + j + m] = cmul(d, w);
+                    v[blk + j + m] = cmul(d, tw64(j * (64 / (2 * m))));
                 }
             }
         }
@@ -60,153 +59,179 @@ __host__ __device__ constexpr int brevC(int i) {
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
 
-__device__ __forceinline__ int wrapModF(int a, int n) {
-    int r = a % n;
-    return r < 0 ? r + n : r;
+// uint16 -> float without the conversion unit: 2^23 + u has the integer u in
+// its mantissa, so subtracting 2^23 is exact.
+__device__ __forceinline__ float u16lo(unsigned int u) { return __int_as_float(0x4B000000u | (u & 0xFFFFu)) - 8388608.0f; }
+__device__ __forceinline__ float u16hi(unsigned int u) { return __int_as_float(0x4B000000u | (u >> 16)) - 8388608.0f; }
+
+// Pixel pairs 4q .. 4q+3 (pixels 8q .. 8q+7 for uint16, 4q .. 4q+3 pairs for
+// float) of a staged row, read with one or two 16-byte shared loads.
+template <bool U16>
+__device__ __forceinline__ void pixelQuad(const unsigned char* row, int q, float2 (&out)[4]) {
+    if (U16) {
+        const uint4 u = *reinterpret_cast<const uint4*>(row + 16 * q);
+        out[0] = make_float2(u16lo(u.x), u16hi(u.x));
+        out[1] = make_float2(u16lo(u.y), u16hi(u.y));
+        out[2] = make_float2(u16lo(u.z), u16hi(u.z));
+        out[3] = make_float2(u16lo(u.w), u16hi(u.w));
+    } else {
+        const float4 a = *reinterpret_cast<const float4*>(row + 32 * q);
+        const float4 b = *reinterpret_cast<const float4*>(row + 32 * q + 16);
+        out[0] = make_float2(a.x, a.y);
+        out[1] = make_float2(a.z, a.w);
+        out[2] = make_float2(b.x, b.y);
+        out[3] = make_float2(b.z, b.w);
+    }
 }
 
 }  // namespace
 
-// Template N: half the FFT-window width (complex samples per row).
-// Template HW: IFFT-window height h (rows kept; also the inner FFT length).
-// blockDim.x = max(H, w * H / HW); one block per (frame, polarisation).
-template <int N, int HW>
-__global__ void __launch_bounds__(256) k_forward_reg(DhFwdParams p) {
-    constexpr int LOGN = ilog2c(N);
+// N: complex samples per packed row (W/2).  HW: IFFT-window height h.
+// blockDim.x = 2H; one block per (frame, polarisation).
+template <int N, int HW, bool U16>
+__global__ void __launch_bounds__(256, 2) k_forward_reg(DhFwdParams p) {
+    constexpr int HALF = N / 2;
+    constexpr int LOGHALF = ilog2c(HALF);
     constexpr int LOGHW = ilog2c(HW);
-    constexpr int ZLD = N + 1;  // padded row stride of the Z buffer (complex)
-    extern __shared__ float2 sm[];
+    constexpr int ZLD = N + 2;                  // Z row stride (complex), padded: conflict-free pair stores
+    constexpr int ES = U16 ? 2 : 4;
+    constexpr int ROWBYTES = 2 * N * ES;
+    constexpr int SLD = ROWBYTES + 16;          // staging row stride (bytes), padded
+    extern __shared__ float4 smRaw[];
     const int H = 1 << p.logH;
-    const int W = 2 * N;
-    const int w = p.w;
-    const int Q = H / HW;  // decimation of the column transform
+    const int w = p.w, h = p.h;
+    const int Q = H / HW;
     const int unit = blockIdx.x;
     const int pol = unit % p.polCount;
     const int frame = unit / p.polCount;
-    float2* zbuf = sm;                       // H x ZLD
-    float2* colbuf = sm + (size_t)H * ZLD;   // H x w
-    float2* exch = sm;                       // w x Q x HW (reuses zbuf after the row pass)
-
-    // ---- rows: each thread loads one row and transforms it in registers
     const int tid = threadIdx.x;
-    if (tid < H) {
-        const long long base = (long long)frame * p.frameStride + (long long)(p.cy[pol] + tid) * p.frameWidth + p.cx[pol];
-        float2 v[N];
-        if (p.inputU16) {
-            const uint4* src = reinterpret_cast<const uint4*>(static_cast<const uint16_t*>(p.frames) + base);
-#pragma unroll
-            for (int q = 0; q < W / 8; q++) {
-                const uint4 u = __ldg(src + q);
-                v[4 * q + 0] = make_float2((float)(u.x & 0xFFFFu), (float)(u.x >> 16));
-                v[4 * q + 1] = make_float2((float)(u.y & 0xFFFFu), (float)(u.y >> 16));
-                v[4 * q + 2] = make_float2((float)(u.z & 0xFFFFu), (float)(u.z >> 16));
-                v[4 * q + 3] = make_float2((float)(u.w & 0xFFFFu), (float)(u.w >> 16));
-            }
-        } else {
-            const float4* src = reinterpret_cast<const float4*>(static_cast<const float*>(p.frames) + base);
-#pragma unroll
-            for (int q = 0; q < W / 4; q++) {
-                const float4 f = __ldg(src + q);
-                v[2 * q + 0] = make_float2(f.x, f.y);
-                v[2 * q + 1] = make_float2(f.z, f.w);
-            }
+
+    unsigned char* region = reinterpret_cast<unsigned char*>(smRaw);
+    const size_t regionBytes = max((size_t)H * SLD, (size_t)H * ZLD * sizeof(float2));
+    float2* colbuf = reinterpret_cast<float2*>(region + regionBytes);   // H x w
+    float2* tSplit = colbuf + (size_t)H * w;                            // w
+    float2* tCol = tSplit + w;                                          // h x Q
+    float2* tAdj = tCol + (size_t)h * Q;                                // h x w
+
+    // per-configuration tables
+    for (int e = tid; e < w; e += blockDim.x) tSplit[e] = p.tabSplit[pol * w + e];
+    for (int e = tid; e < h * Q; e += blockDim.x) tCol[e] = p.tabCol[(size_t)pol * h * Q + e];
+    for (int e = tid; e < h * w; e += blockDim.x) tAdj[e] = p.tabAdj[(size_t)pol * h * w + e];
+
+    // 1. coalesced staging of the H x W window
+    {
+        const unsigned char* src = static_cast<const unsigned char*>(p.frames) +
+            ((size_t)frame * p.frameStride + (size_t)p.cy[pol] * p.frameWidth + p.cx[pol]) * ES;
+        const size_t srcPitch = (size_t)p.frameWidth * ES;
+        constexpr int VPR = ROWBYTES / 16;
+        for (int e = tid; e < H * VPR; e += blockDim.x) {
+            const int r = e / VPR, q = e - r * VPR;
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + r * srcPitch) + q);
+            *reinterpret_cast<uint4*>(region + (size_t)r * SLD + 16 * q) = v;
         }
-        fftRegDIF<N>(v);
-        float2* zr = zbuf + (size_t)tid * ZLD;
-#pragma unroll
-        for (int i = 0; i < N; i++) zr[brevC<LOGN>(i)] = v[i];
     }
     __syncthreads();
 
-    // ---- R2C split: X[k] for the w kept columns k = sx0 + c
+    // 2. row transforms: thread pair (row r, half hf)
+    const int r = tid >> 1, hf = tid & 1;
+    float2 u[HALF];
+    if (r < H) {
+        const unsigned char* row = region + (size_t)r * SLD;
+#pragma unroll
+        for (int q = 0; q < HALF / 4; q++) {
+            float2 a[4], b[4];
+            pixelQuad<U16>(row, q, a);
+            pixelQuad<U16>(row, q + HALF / 4, b);
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int j = 4 * q + t;
+                u[j] = hf ? cmul(csub(a[t], b[t]), tw64(j * (64 / N))) : cadd(a[t], b[t]);
+            }
+        }
+        fftRegDIF<HALF>(u);
+    }
+    __syncthreads();  // staging is dead; Z overwrites it
+    float2* zbuf = reinterpret_cast<float2*>(region);
+    if (r < H) {
+        float2* zr = zbuf + (size_t)r * ZLD;
+#pragma unroll
+        for (int i = 0; i < HALF; i++) zr[2 * brevC<LOGHALF>(i) + hf] = u[i];
+    }
+    __syncthreads();
+
+    // 3. R2C split for the kept columns k = sx0 + c
     const int sx0 = p.sx0[pol];
     for (int e = tid; e < H * w; e += blockDim.x) {
-        const int r = e / w, c = e - r * w;
+        const int rr = e / w, c = e - rr * w;
         const int k = sx0 + c;
-        const float2* zr = zbuf + (size_t)r * ZLD;
+        const float2* zr = zbuf + (size_t)rr * ZLD;
         const float2 zk = zr[k & (N - 1)];
         const float2 zc = cconj(zr[(N - k) & (N - 1)]);
         const float2 even = cscale(cadd(zk, zc), 0.5f);
         const float2 d = csub(zk, zc);
         const float2 odd = make_float2(0.5f * d.y, -0.5f * d.x);
-        const float2 wk = c_tw[k << (TW_LOG - LOGN - 1)];
-        colbuf[e] = cadd(even, cmul(wk, odd));
+        colbuf[e] = cadd(even, cmul(tSplit[c], odd));
     }
     __syncthreads();
 
-    // ---- columns: HW-point FFT of each decimated sequence X[Q a + b][c], a < HW
+    // 4. column transforms of the decimated sequences X[Q a + b][c], a < HW
+    float2* exch = zbuf;  // [HW][Q][w], after the split Z is dead
     for (int e = tid; e < w * Q; e += blockDim.x) {
         const int c = e % w, b = e / w;
         float2 v[HW];
 #pragma unroll
         for (int a = 0; a < HW; a++) v[a] = colbuf[(size_t)(Q * a + b) * w + c];
         fftRegDIF<HW>(v);
-        float2* dst = exch + ((size_t)c * Q + b) * HW;
 #pragma unroll
-        for (int i = 0; i < HW; i++) dst[brevC<LOGHW>(i)] = v[i];
+        for (int i = 0; i < HW; i++) exch[((size_t)brevC<LOGHW>(i) * Q + b) * w + c] = v[i];
     }
     __syncthreads();
 
-    // ---- kept rows: Y[k] = sum_b exp(-2 pi i k b / H) Z_b[k mod HW], then the window operations
+    // 5. kept rows: Y = sum_b tCol[j][b] Z_b[row mod HW], then the window factors
     float2 bc = make_float2(1.0f, 0.0f);
     if (p.batchCal && p.batchCalCount > 0)
         bc = p.batchCal[pol * p.batchCalCount + ((p.frameOffset + frame) % p.batchCalCount)];
-    const float kx0 = p.kx0[pol], ky0 = p.ky0[pol], r02 = p.r02[pol];
-    const float bcx = p.bcx[pol], bcy = p.bcy[pol];
-    const int twShiftH = TW_LOG - p.logH;
-    for (int e = tid; e < p.h * w; e += blockDim.x) {
+    const int sy = p.sy[pol];
+    float2* out = p.window + (size_t)(frame * p.polCount + pol) * h * w;
+    for (int e = tid; e < h * w; e += blockDim.x) {
         const int j = e / w, c = e - j * w;
-        const int jSY = j + p.sy[pol];
-        const int row = wrapModF(jSY + H / 2, H);
-        const float2* zb = exch + (size_t)c * Q * HW + (row & (HW - 1));
+        int row = (j + sy + H / 2) % H;
+        if (row < 0) row += H;
+        const float2* zb = exch + (size_t)(row & (HW - 1)) * Q * w + c;
+        const float2* tc = tCol + (size_t)j * Q;
         float2 Y = zb[0];
-        for (int b = 1; b < Q; b++) {
-            const float2 t = c_tw[((row * b) & (H - 1)) << twShiftH];
-            Y = cadd(Y, cmul(zb[(size_t)b * HW], t));
-        }
-        Y = cmul(Y, bc);
-        const float kx = p.kxAxis[sx0 + c];
-        const float ky = p.kyAxis[row];
-        const float shift = jSY < 0 ? p.kyShift : (jSY > H ? -p.kyShift : 0.0f);
-        const float dky = __fsub_rn(ky, __fadd_rn(ky0, shift));
-        const float dkx = __fsub_rn(kx, kx0);
-        const float dr2 = __fadd_rn(__fmul_rn(dkx, dkx), __fmul_rn(dky, dky));
-        float env = 1.0f;
-        if (p.fillFactor) env = xcsc(kx * p.halfPixel) * xcsc(ky * p.halfPixel);
-        const float normF = (dr2 <= r02) ? env * p.norm : 0.0f;
-        const float arg = __fadd_rn(__fmul_rn(bcx, kx), __fmul_rn(ky, bcy));
-        float sn, cs;
-        sincosf(arg, &sn, &cs);
-        const float2 adj = make_float2(cs * normF, sn * normF);
-        const size_t o = ((size_t)(frame * p.polCount + pol) * p.h + j) * p.w + c;
-        p.window[o] = cmul(Y, adj);
+        for (int b = 1; b < Q; b++) Y = cadd(Y, cmul(zb[(size_t)b * w], tc[b]));
+        out[e] = cmul(cmul(Y, bc), tAdj[e]);
     }
-}
-
-cudaError_t dh_forward_reg_init(const float2* hostTwiddle) {
-    return cudaMemcpyToSymbol(c_tw, hostTwiddle, sizeof(float2) * TW_N);
 }
 
 template <int N, int HW>
 static cudaError_t launchReg(const DhFwdParams& p, cudaStream_t s) {
     const int H = 1 << p.logH;
-    const int threads = max(H, p.w * (H / HW));
-    const size_t smem = sizeof(float2) * ((size_t)H * (N + 1) + (size_t)H * p.w);
-    const size_t exch = sizeof(float2) * (size_t)p.w * (H / HW) * HW;
-    if (exch > sizeof(float2) * (size_t)H * (N + 1)) return cudaErrorNotSupported;
-    cudaError_t e = cudaFuncSetAttribute(k_forward_reg<N, HW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_forward_reg<N, HW><<<(unsigned)(p.frameCount * p.polCount), threads, smem, s>>>(p);
+    const int es = p.inputU16 ? 2 : 4;
+    const size_t region = max((size_t)H * (2 * N * es + 16), (size_t)H * (N + 2) * sizeof(float2));
+    const size_t smem = region + sizeof(float2) * ((size_t)H * p.w + p.w + (size_t)p.h * (H / HW) + (size_t)p.h * p.w);
+    if ((size_t)p.w * H * sizeof(float2) > region) return cudaErrorNotSupported;
+    const unsigned blocks = (unsigned)(p.frameCount * p.polCount);
+    cudaError_t e;
+    if (p.inputU16) {
+        e = cudaFuncSetAttribute(k_forward_reg<N, HW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_forward_reg<N, HW, true><<<blocks, 2 * H, smem, s>>>(p);
+    } else {
+        e = cudaFuncSetAttribute(k_forward_reg<N, HW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_forward_reg<N, HW, false><<<blocks, 2 * H, smem, s>>>(p);
+    }
     return cudaGetLastError();
 }
 
 // Returns cudaErrorNotSupported when the shape needs the generic kernel.
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s) {
     const int W = 1 << p.logW, H = 1 << p.logH;
-    if (p.h != p.w || H > 256 || H < p.h || p.w > 32) return cudaErrorNotSupported;
-    if (p.w * (H / p.h) > 256) return cudaErrorNotSupported;
-    const size_t smem = sizeof(float2) * ((size_t)H * (W / 2 + 1) + (size_t)H * p.w);
-    if (smem > 200 * 1024) return cudaErrorNotSupported;
+    if (!p.tabSplit || !p.tabCol || !p.tabAdj) return cudaErrorNotSupported;
+    if (p.h != p.w || H > 128 || H < p.h || p.w > 32) return cudaErrorNotSupported;
+    if (p.w * (H / p.h) > 2 * H) return cudaErrorNotSupported;
     if (p.h == 16) {
         if (W == 32) return launchReg<16, 16>(p, s);
         if (W == 64) return launchReg<32, 16>(p, s);

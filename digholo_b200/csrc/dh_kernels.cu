@@ -455,7 +455,15 @@ cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
     const size_t smem = dh_inverse_smem_bytes(p);
     cudaError_t e = cudaFuncSetAttribute(k_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_inverse<<<(unsigned)(p.frameCount * p.polCount), INV_THREADS, smem, s>>>(p);
+    // small (low-resolution) fields: one thread per pair of pixels, at least two warps
+    int threads = INV_THREADS;
+    if (p.lowres) {
+        const int npix = (1 << p.logw) * (1 << p.logh);
+        threads = npix / 2;
+        if (threads < 64) threads = 64;
+        if (threads > INV_THREADS) threads = INV_THREADS;
+    }
+    k_inverse<<<(unsigned)(p.frameCount * p.polCount), threads, smem, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -13,7 +13,6 @@
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
-cudaError_t dh_forward_reg_init(const float2* hostTwiddle);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
@@ -254,7 +253,6 @@ int objInitDevice(Object& o) {
     }
     DH_CUDA(o, o.dTwiddle.ensure(tw.size() * sizeof(float)));
     DH_CUDA(o, cudaMemcpy(o.dTwiddle.ptr, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice));
-    DH_CUDA(o, dh_forward_reg_init(reinterpret_cast<const float2*>(tw.data())));
     return ERR_SUCCESS;
 }
 
@@ -320,6 +318,73 @@ static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
     return ERR_SUCCESS;
 }
 
+// Frame-independent factors of the forward stage for the register kernel,
+// evaluated with the float32 arithmetic of digHoloCopyWindow
+// (digHolo.cpp:1955-2035): per polarisation, the R2C split twiddles
+// [w], the column-sum twiddles [h][H/h] and the window factors [h][w].
+static void forwardTables(const Object& o, std::vector<float>& split, std::vector<float>& col,
+                          std::vector<float>& adj) {
+    const Config& c = o.cfg;
+    const Geometry& g = o.geo;
+    const int P = o.polCount, w = g.w, h = g.h, W = g.W, H = g.H;
+    const int Q = H / h;
+    split.assign((size_t)P * w * 2, 0.f);
+    col.assign((size_t)P * h * Q * 2, 0.f);
+    adj.assign((size_t)P * h * w * 2, 0.f);
+    const float lam = c.wavelengthCentre;
+    const float k0 = 2 * PI_F / lam;
+    const float kr = k0 * sinf(c.apertureSize * UNIT_ANGLE);
+    const float r02 = kr * kr;
+    const double fftLength = 1.0 * W * H;
+    const double ifftLength = c.resolutionIdx ? 1.0 * w * h : fftLength;
+    const float norm = (float)(1.0 / sqrt(fftLength * ifftLength));
+    const float halfPixel = 0.5f * c.pixelSize;
+    const float kyShift = fabsf((g.ky[1] - g.ky[0]) * H);
+    auto xcscD = [](float x) { return x == 0.f ? 1.0f : (float)((double)x / sin((double)x)); };
+    for (int p = 0; p < P; p++) {
+        const int sx0 = g.SX[p] - W / 2;
+        for (int cc = 0; cc < w; cc++) {
+            const double a = -2.0 * PI_D * (double)(sx0 + cc) / (double)W;
+            split[((size_t)p * w + cc) * 2] = (float)cos(a);
+            split[((size_t)p * w + cc) * 2 + 1] = (float)sin(a);
+        }
+        const int cx0 = (g.cx[p] + W / 2) - c.frameWidth / 2;
+        const int cy0 = (g.cy[p] + H / 2) - c.frameHeight / 2;
+        const float bcx = c.beamCentreX[p] - (cx0) * c.pixelSize;
+        const float bcy = c.beamCentreY[p] - (cy0) * c.pixelSize;
+        const float kx0 = k0 * sinf(c.zern[p][ZERN_TILTX] * UNIT_ANGLE);
+        const float ky0 = k0 * sinf(c.zern[p][ZERN_TILTY] * UNIT_ANGLE);
+        for (int j = 0; j < h; j++) {
+            const int jSY = j + g.SY[p];
+            int row = (jSY + H / 2) % H;
+            if (row < 0) row += H;
+            for (int b = 0; b < Q; b++) {
+                const double a = -2.0 * PI_D * (double)((row * b) % H) / (double)H;
+                col[(((size_t)p * h + j) * Q + b) * 2] = (float)cos(a);
+                col[(((size_t)p * h + j) * Q + b) * 2 + 1] = (float)sin(a);
+            }
+            const float ky = g.ky[row];
+            const float shift = jSY < 0 ? kyShift : (jSY > H ? -kyShift : 0.0f);
+            for (int cc = 0; cc < w; cc++) {
+                const float kx = g.kx[sx0 + cc];
+                volatile float dky = ky - (ky0 + shift);
+                volatile float dkx = kx - kx0;
+                volatile float dkx2 = dkx * dkx;
+                volatile float dky2 = dky * dky;
+                const float dr2 = dkx2 + dky2;
+                const float env = c.fillFactorCorrection ? xcscD(kx * halfPixel) * xcscD(ky * halfPixel) : 1.0f;
+                const float normF = (dr2 <= r02) ? env * norm : 0.0f;
+                volatile float ax = bcx * kx;
+                volatile float ay = ky * bcy;
+                const float arg = ax + ay;
+                const size_t o2 = (((size_t)p * h + j) * w + cc) * 2;
+                adj[o2] = (float)cos((double)arg) * normF;
+                adj[o2 + 1] = (float)sin((double)arg) * normF;
+            }
+        }
+    }
+}
+
 static void forwardParams(Object& o, DhFwdParams& fp) {
     const Config& c = o.cfg;
     const Geometry& g = o.geo;
@@ -362,6 +427,14 @@ static void forwardParams(Object& o, DhFwdParams& fp) {
     }
     fp.window = o.dWindow.as<float2>();
     fp.twiddle = o.dTwiddle.as<float2>();
+    if (o.dTables.ptr) {
+        const Geometry& gg = o.geo;
+        const size_t P = o.polCount;
+        float2* t = o.dTables.as<float2>();
+        fp.tabSplit = t;
+        fp.tabCol = t + P * gg.w;
+        fp.tabAdj = t + P * gg.w + P * gg.h * (gg.H / gg.h);
+    }
 }
 
 // digHoloFFT_SetWindow + digHoloIFFT_SetWindow: geometry, axes, buffers.
@@ -412,6 +485,18 @@ static int prepare(Object& o) {
         const size_t n = o.batchCal.size() * sizeof(float);
         DH_CUDA(o, o.dBatchCal.ensure(n));
         DH_CUDA(o, cudaMemcpyAsync(o.dBatchCal.ptr, o.batchCal.data(), n, cudaMemcpyHostToDevice, o.stream));
+    }
+    {
+        std::vector<float> split, col, adj;
+        forwardTables(o, split, col, adj);
+        const size_t n = split.size() + col.size() + adj.size();
+        DH_CUDA(o, o.dTables.ensure(n * sizeof(float)));
+        float* t = o.dTables.as<float>();
+        DH_CUDA(o, cudaMemcpyAsync(t, split.data(), split.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+        DH_CUDA(o, cudaMemcpyAsync(t + split.size(), col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+        DH_CUDA(o, cudaMemcpyAsync(t + split.size() + col.size(), adj.data(), adj.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, o.stream));
+        DH_CUDA(o, cudaStreamSynchronize(o.stream));
     }
     // reference wave (cached inputs are cheap to recompute on the host)
     std::vector<short> ref;

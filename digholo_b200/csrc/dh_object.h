@@ -128,7 +128,7 @@ struct Object {
     Config preparedCfg;
     int preparedValid = 0, preparedKeep32 = -1, preparedU16 = -1, batchCalVersion = 0, preparedBatchCal = -1;
     DevBuf dTwiddle, dFrames, dWindow, dFieldR, dFieldI, dField32, dStats, dCoefs;
-    DevBuf dKx, dKy, dX, dY, dRef, dRefF, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
+    DevBuf dKx, dKy, dX, dY, dRef, dRefF, dTables, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
     // basis cache key
     int basisNx = 0, basisNy = 0, basisMG = 0;
     float basisWaist[POLMAX] = {0.f, 0.f};

@@ -34,6 +34,11 @@ struct DhFwdParams {
     int frameOffset;        // index of frame 0 of this launch within the batch
     float2* window;         // out: [frame][pol][h][w]
     const float2* twiddle;  // TW_N twiddles
+    // Frame-independent factors, precomputed per configuration for the
+    // register kernel (the generic kernel evaluates them itself):
+    const float2* tabSplit; // [pol][w]    exp(-2 pi i (sx0 + c) / W), the R2C split twiddles
+    const float2* tabCol;   // [pol][h][Q] exp(-2 pi i row_j b / H), Q = H / h
+    const float2* tabAdj;   // [pol][h][w] mask x norm x 1/sinc x exp(i (kx bcx + ky bcy))
 };
 
 // Inverse stage: Fourier window -> IFFT -> field statistics -> reference wave,
