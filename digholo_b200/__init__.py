@@ -46,6 +46,7 @@ def _bind_extensions(lib, out):
         "digHoloB200GetStageTimes": (_C.c_int, [_C.c_int, P(_C.c_float)]),
         "digHoloB200GetGeometry": (_C.c_int, [_C.c_int, P(_C.c_int)]),
         "digHoloB200SetForwardKernel": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200GetAutoAlignEvaluations": (_C.c_int, [_C.c_int]),
         "digHoloB200ProcessBatchNoAlloc": (_C.c_int, [_C.c_int, _C.c_void_p, _C.c_int, _C.c_int, _C.c_void_p,
                                                      _C.c_void_p, _C.c_void_p, _C.c_void_p]),
     }

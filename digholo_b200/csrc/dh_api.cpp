@@ -15,6 +15,8 @@
 
 using dh::Object;
 
+void dh_eigen_destroy(DhEigen* e);
+
 typedef float complex64[2];
 
 namespace {
@@ -65,6 +67,7 @@ int digHoloDestroy(int h) {
             for (auto e : o->evCopy) if (e) cudaEventDestroy(e);
             if (o->evStart) cudaEventDestroy(o->evStart);
             if (o->evStop) cudaEventDestroy(o->evStop);
+            dh_eigen_destroy(o->eigen);
         }
         delete o;
     }
@@ -505,6 +508,31 @@ complex64* digHoloGetFourierPlaneWindow(int h, int* batchCount, int* polCount, i
     return (complex64*)o->hWindow.ptr;
 }
 
+// ------------------------------------------------------------ metrics and AutoAlign
+// digHolo.h:1152 / digHolo.cpp:14989 and 13012-13016
+float digHoloAutoAlign(int h) {
+    OBJ_OR(h, 0.0f);
+    return dh::objAutoAlign(*o);
+}
+// digHolo.h:1163 / digHolo.cpp:15014: the metric averaged over wavelengths
+float digHoloAutoAlignGetMetric(int h, int metricIdx) {
+    OBJ_OR(h, 0.0f);
+    if (metricIdx < 0 || metricIdx >= dh::METRIC_COUNT) return 0.0f;
+    return o->autoAlignMetrics[metricIdx][1];
+}
+// digHolo.h:1174 / digHolo.cpp:15001: [wavelength 0, average]
+float* digHoloAutoAlignGetMetrics(int h, int metricIdx) {
+    OBJ_OR(h, nullptr);
+    if (metricIdx < 0 || metricIdx >= dh::METRIC_COUNT) return nullptr;
+    return o->autoAlignMetrics[metricIdx];
+}
+// digHolo.h:1185 / digHolo.cpp:15043 and 12214-12230
+int digHoloAutoAlignCalcMetrics(int h) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    std::lock_guard<std::mutex> g(o->lock);
+    return dh::objCalcMetrics(*o);
+}
+
 // ------------------------------------------------------------ extensions
 // No counterpart in the reference: device-resident use without host copies.
 
@@ -593,6 +621,11 @@ int digHoloB200SetForwardKernel(int h, int generic) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     o->forceGeneric = generic ? 1 : 0;
     return dh::ERR_SUCCESS;
+}
+// Number of batch evaluations the last digHoloAutoAlign ran.
+int digHoloB200GetAutoAlignEvaluations(int h) {
+    OBJ_OR(h, 0);
+    return o->alignEvaluations;
 }
 // Last error message of the handle (empty when none).
 const char* digHoloB200GetLastError(int h) {

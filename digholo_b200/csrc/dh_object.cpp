@@ -324,7 +324,7 @@ static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
 // [w], the column-sum twiddles [h][H/h] and the window factors [h][w].
 static void forwardTables(const Object& o, std::vector<float>& split, std::vector<float>& col,
                           std::vector<float>& adj) {
-    const Config& c = o.cfg;
+    const Config& c = o.useSnaps ? o.ifftSnap : o.cfg;
     const Geometry& g = o.geo;
     const int P = o.polCount, w = g.w, h = g.h, W = g.W, H = g.H;
     const int Q = H / h;
@@ -386,7 +386,7 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
 }
 
 static void forwardParams(Object& o, DhFwdParams& fp) {
-    const Config& c = o.cfg;
+    const Config& c = o.useSnaps ? o.ifftSnap : o.cfg;
     const Geometry& g = o.geo;
     memset(&fp, 0, sizeof(fp));
     fp.inputU16 = o.framesU16;
@@ -450,8 +450,10 @@ static int prepare(Object& o) {
     // the reference stores the default window size back into the config (digHolo.cpp:7283-7290)
     if (c.fftWindowSizeX <= 0) c.fftWindowSizeX = c.frameWidth / c.polCount;
     if (c.fftWindowSizeY <= 0) c.fftWindowSizeY = c.frameHeight;
-    fftWindowGeometry(c, o.polCount, o.geo);
-    ifftWindowGeometry(c, o.polCount, o.geo);
+    // AutoAlign evaluations place the FFT and IFFT windows with the settings of
+    // the last evaluation that reran those stages (stage snapshots)
+    fftWindowGeometry(o.useSnaps ? o.fftSnap : c, o.polCount, o.geo);
+    ifftWindowGeometry(o.useSnaps ? o.ifftSnap : c, o.polCount, o.geo);
     r = checkSupported(o);
     if (r) return r;
     const Geometry& g = o.geo;
@@ -462,7 +464,7 @@ static int prepare(Object& o) {
         const uintptr_t a = reinterpret_cast<uintptr_t>(o.frames);
         if (a % 16) return fail(o, ERR_INVALIDARGUMENT, "device frame buffer must be 16-byte aligned");
     }
-    if (o.preparedValid && memcmp(&o.preparedCfg, &c, sizeof(Config)) == 0 && o.preparedKeep32 == o.keepField32 &&
+    if (!o.useSnaps && o.preparedValid && memcmp(&o.preparedCfg, &c, sizeof(Config)) == 0 && o.preparedKeep32 == o.keepField32 &&
         o.preparedU16 == o.framesU16 && o.preparedBatchCal == o.batchCalVersion)
         return ERR_SUCCESS;
     o.preparedValid = 0;
@@ -512,7 +514,7 @@ static int prepare(Object& o) {
     o.preparedKeep32 = o.keepField32;
     o.preparedU16 = o.framesU16;
     o.preparedBatchCal = o.batchCalVersion;
-    o.preparedValid = 1;
+    o.preparedValid = o.useSnaps ? 0 : 1;
     return ERR_SUCCESS;
 }
 
@@ -789,6 +791,13 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     }
     if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
     DH_CUDA(o, dh_launch_inverse(ip, o.stream));
+    return ERR_SUCCESS;
+}
+
+// The batch path for one AutoAlign evaluation: outputs stay on the device.
+int objProcessForAlign(Object& o) {
+    int r = objProcessBatch(o, 0);
+    if (r) return r;
     return ERR_SUCCESS;
 }
 

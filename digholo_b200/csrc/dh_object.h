@@ -12,6 +12,8 @@
 
 #include "dh_params.h"
 
+struct DhEigen;
+
 namespace dh {
 
 // Error codes and constants of the public interface (digHolo.h:171-182, 1363-1372, 1624-1631).
@@ -135,6 +137,14 @@ struct Object {
     float basisPsx = 0.f, basisPsy = 0.f;
     int basisPolCount = 0;
     int keepField32 = 0;
+    // power meter / AutoAlign
+    DevBuf dMetricA, dMetricG, dCoefsBackup, dAlignFrames;
+    DhEigen* eigen = nullptr;
+    int alignEvaluations = 0;
+    // stage snapshots used while AutoAlign runs: the FFT window comes from
+    // fftSnap and the Fourier-window selection from ifftSnap
+    int useSnaps = 0;
+    Config fftSnap, ifftSnap;
     int forceGeneric = 0;               // use the shared-memory forward kernel for every shape
 
     // host mirrors
@@ -157,6 +167,9 @@ int objFieldsToHost(Object& o, int complexOut);
 int objStatsToHost(Object& o);
 int objWindowToHost(Object& o);
 int objStageTimes(Object& o, float* ms);
+int objProcessForAlign(Object& o);
+int objCalcMetrics(Object& o);
+float objAutoAlign(Object& o);
 
 // Geometry helpers (host, float32 emulation of the reference).
 void fftWindowGeometry(const Config& c, int polCount, Geometry& g);

@@ -88,10 +88,28 @@ class Hologram:
         self.wavelength = wavelength
 
 
+def transfer_coefs(frame_count, pol_count, max_mg, seed, loss_db=1.0):
+    """Coefficients of frames that each excite one column of a Haar-random
+    unitary times a per-mode loss uniform in [0, loss_db] dB: frame f of
+    polarisation p carries column (f mod M) of diag(d_p) U_p."""
+    rng = np.random.default_rng(seed)
+    M = len(hg_indices(max_mg)[0])
+    out = np.zeros((frame_count, pol_count, M), dtype=np.complex128)
+    for p in range(pol_count):
+        z = (rng.standard_normal((M, M)) + 1j * rng.standard_normal((M, M))) / math.sqrt(2.0)
+        q, r = np.linalg.qr(z)
+        q = q * (np.diag(r) / np.abs(np.diag(r)))[None, :]   # Haar: fix the phases of R's diagonal
+        d = 10.0 ** (-rng.uniform(0.0, loss_db, size=M) / 20.0)
+        T = d[:, None] * q
+        for f in range(frame_count):
+            out[f, p] = T[:, f % M]
+    return out
+
+
 def generate(frame_count, frame_width, frame_height, pol_count, max_mg, waist, snr_db,
              carrier=(0.25, 0.2), window=(64, 64), dtype="float32", seed=1000,
              centre_jitter=40e-6, signal_fraction=0.1, taper=False, coefs=None,
-             pixel_size=PIXEL_SIZE, wavelength=WAVELENGTH):
+             pixel_size=PIXEL_SIZE, wavelength=WAVELENGTH, defocus=0.0, normalise_frames=True):
     """Generate ``frame_count`` frames (frame_count, frame_height, frame_width).
 
     ``coefs`` may be given as (frame_count, pol_count, modeCount) complex; by
@@ -138,8 +156,18 @@ def generate(frame_count, frame_width, frame_height, pol_count, max_mg, waist, s
             cmat[:, ms, ns] = coefs[f0:f1, pol, :]
             # S[f, y, x] = sum_mn c_mn hy[n, y] hx[m, x]
             s = np.einsum("fmn,ny,mx->fyx", cmat, hy, hx, optimize=True)
-            p = np.sum(np.abs(s) ** 2, axis=(1, 2), keepdims=True)
-            s = s * np.sqrt(signal_fraction * npix / np.maximum(p, 1e-300))
+            if defocus:
+                # quadratic phase of a defocus of `defocus` dioptres about the beam centre
+                r2 = ((ys - cy) ** 2)[:, None] + ((xr - cx) ** 2)[None, :]
+                s = s * np.exp(1j * math.pi * defocus * r2 / wavelength)[None]
+            if normalise_frames:
+                p = np.sum(np.abs(s) ** 2, axis=(1, 2), keepdims=True)
+                s = s * np.sqrt(signal_fraction * npix / np.maximum(p, 1e-300))
+            else:
+                # one scale for the whole batch, so relative frame powers (mode-dependent loss)
+                # survive: sum over pixels of |S|^2 ~ sum |c|^2 / pixel^2 for unit-power HG modes
+                mean_c2 = float(np.mean(np.sum(np.abs(coefs[:, pol, :]) ** 2, axis=1)))
+                s = s * math.sqrt(signal_fraction * npix * pixel_size ** 2 / max(mean_c2, 1e-300))
             clean[f0:f1, :, x0:x0 + region_w] = np.abs(ref[None] + s) ** 2
 
     sigma = clean.mean() * 10.0 ** (-snr_db / 20.0)
@@ -168,6 +196,11 @@ WORKLOADS = {
     "batched_640x512_u16_2pol": dict(frame_count=1024, frame_width=640, frame_height=512, pol_count=2,
                                      max_mg=15, waist=250e-6, snr_db=25, window=(128, 128),
                                      dtype="uint16", seed=1002),
+    # frames excite columns of a Haar-random 120x120 transfer matrix with per-mode loss
+    # (coefficients from transfer_coefs); frames are not normalised individually
+    "align_640x512_f32_2pol": dict(frame_count=512, frame_width=640, frame_height=512, pol_count=2,
+                                   max_mg=15, waist=250e-6, snr_db=30, window=(128, 128),
+                                   dtype="float32", seed=1004, normalise_frames=False),
     "largefield_2048_u16_2pol": dict(frame_count=256, frame_width=2048, frame_height=2048, pol_count=2,
                                      max_mg=30, waist=600e-6, snr_db=20, window=(512, 512),
                                      dtype="uint16", seed=1005, taper=True),

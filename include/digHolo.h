@@ -206,6 +206,19 @@ int digHoloConfigGetAutoAlignMode(int handleIdx);
 int digHoloConfigSetAutoAlignGoalIdx(int handleIdx, int goalIdx);
 /* replaces digHolo.h:1136 */
 int digHoloConfigGetAutoAlignGoalIdx(int handleIdx);
+/* replaces digHolo.h:1152.  Runs the reference's TWEAK coordinate search
+ * (tilt, beam centre, defocus, waist; optional Fourier-window radius rule)
+ * with every evaluation on the GPU and returns the final value of the goal
+ * metric in dB.  FULL and ESTIMATE start the same search from the current
+ * settings: the snap estimate from the full Fourier plane is not built. */
+float digHoloAutoAlign(int handleIdx);
+/* replaces digHolo.h:1163 */
+float digHoloAutoAlignGetMetric(int handleIdx, int metricIdx);
+/* replaces digHolo.h:1174 */
+float* digHoloAutoAlignGetMetrics(int handleIdx, int metricIdx);
+/* replaces digHolo.h:1185.  IL, MDL (FP64 Gram eigenvalues on the GPU),
+ * SNR, diagonal/crosstalk metrics of the last processed batch. */
+int digHoloAutoAlignCalcMetrics(int handleIdx);
 /* replaces digHolo.h:1205 */
 int digHoloConfigSetBeamCentre(int handleIdx, int axisIdx, int polIdx, float centre);
 /* replaces digHolo.h:1215 */
@@ -315,6 +328,10 @@ int digHoloB200SetForwardKernel(int handleIdx, int generic);
 
 /* Message of the handle's last error ("" when none). */
 const char* digHoloB200GetLastError(int handleIdx);
+
+/* Number of batch evaluations (window selection, tilt removal, overlap and
+ * power meter) the last digHoloAutoAlign call made. */
+int digHoloB200GetAutoAlignEvaluations(int handleIdx);
 
 /* No counterpart in the reference.  The batch path for callers that cannot
  * allocate device memory while they process frames (a real-time acquisition

@@ -1,0 +1,95 @@
+"""Power meter and AutoAlign on the GPU against the reference build.
+
+Workload: frames exciting the columns of a Haar-random transfer matrix with
+per-mode loss (synth.transfer_coefs), dual polarisation, 120 modes.
+Tolerances: every metric of digHoloAutoAlignCalcMetrics within 0.01 dB of
+the reference's; AutoAlign (TWEAK mode, goal IL, from a perturbed start)
+ends within 0.01 dB of the reference's final IL and MDL.
+"""
+import ctypes as C
+import time
+
+import numpy as np
+import pytest
+
+import ref_lib
+from digholo_b200 import api, synth
+from helpers import config_for
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(frames, seed=77):
+    kw = dict(synth.WORKLOADS["align_640x512_f32_2pol"])
+    kw["frame_count"] = frames
+    kw["coefs"] = synth.transfer_coefs(frames, 2, kw["max_mg"], seed)
+    return synth.generate(**kw)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import digholo_b200
+    return digholo_b200.load()
+
+
+def test_calc_metrics_match_reference(lib):
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    hol = _case(32)
+    cfg = config_for(hol, 0)
+    L = ref_lib.load()
+    hr = L.digHoloCreate()
+    ref_lib.configure(L, hr, cfg)
+    ref_lib.run_batch(L, hr, hol.frames, want_fields=False)
+    assert L.digHoloAutoAlignCalcMetrics(hr) == 0
+    ref = np.array([L.digHoloAutoAlignGetMetric(hr, i) for i in range(9)])
+    h = lib.digHoloCreate()
+    api.configure(lib, h, cfg)
+    api.run_batch(lib, h, hol.frames, want_fields=False)
+    assert lib.digHoloAutoAlignCalcMetrics(h) == 0
+    ours = np.array([lib.digHoloAutoAlignGetMetric(h, i) for i in range(9)])
+    lib.digHoloDestroy(h)
+    finite = np.isfinite(ref) & (np.abs(ref) < 1e30)
+    assert np.all(np.abs(ours[finite] - ref[finite]) <= 0.01), (ours, ref)
+
+
+def _align(L, cfg, frames, tol=0.01):
+    h = L.digHoloCreate()
+    api.configure(L, h, cfg)
+    L.digHoloConfigSetAutoAlignMode(h, 1)          # TWEAK
+    L.digHoloConfigSetAutoAlignGoalIdx(h, 0)       # IL
+    L.digHoloConfigSetAutoAlignTol(h, tol)
+    L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
+    fr = np.ascontiguousarray(frames)
+    api.set_batch(L, h, fr)
+    # process once first: the reference's TWEAK search takes its limits from
+    # working variables that only an FFT sets (on a fresh handle it clamps the
+    # beam centre and the waist to zero)
+    b, m, p = C.c_int(), C.c_int(), C.c_int()
+    L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+    t = time.time()
+    val = L.digHoloAutoAlign(h)
+    dt = time.time() - t
+    metrics = np.array([L.digHoloAutoAlignGetMetric(h, i) for i in range(9)])
+    params = [L.digHoloConfigGetBeamCentre(h, 0, 0), L.digHoloConfigGetBeamCentre(h, 1, 0),
+              L.digHoloConfigGetTilt(h, 0, 0), L.digHoloConfigGetTilt(h, 1, 0), L.digHoloConfigGetBasisWaist(h, 0)]
+    evaluations = L.digHoloB200GetAutoAlignEvaluations(h) if hasattr(L, "digHoloB200GetAutoAlignEvaluations") else -1
+    return val, metrics, params, dt, evaluations
+
+
+def test_autoalign_tweak_matches_reference(lib):
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    hol = _case(32)
+    cfg = config_for(hol, 0)
+    # perturbed start: centre +30 um, tilt +2 %, waist +10 %
+    cfg.beam_centre = [[bc[0] + 30e-6, bc[1] - 20e-6] for bc in cfg.beam_centre]
+    cfg.tilt_deg = [[t[0] * 1.02, t[1] * 0.98] for t in cfg.tilt_deg]
+    cfg.waist = [w * 1.1 for w in cfg.waist]
+    vr, mr, pr, tr, _ = _align(ref_lib.load(), cfg, hol.frames)
+    vg, mg, pg, tg, ng = _align(lib, cfg, hol.frames)
+    print("reference IL %.4f MDL %.4f in %.2f s; this build IL %.4f MDL %.4f in %.2f s (%d evaluations)"
+          % (mr[0], mr[1], tr, mg[0], mg[1], tg, ng))
+    print("reference params", np.array(pr), "this build", np.array(pg))
+    assert abs(mg[0] - mr[0]) <= 0.01
+    assert abs(mg[1] - mr[1]) <= 0.01
