@@ -47,6 +47,9 @@ def _bind_extensions(lib, out):
         "digHoloB200GetGeometry": (_C.c_int, [_C.c_int, P(_C.c_int)]),
         "digHoloB200SetForwardKernel": (_C.c_int, [_C.c_int, _C.c_int]),
         "digHoloB200GetAutoAlignEvaluations": (_C.c_int, [_C.c_int]),
+        "digHoloB200GetForwardKernel": (_C.c_int, [_C.c_int]),
+        "digHoloB200SetInverseKernel": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200GetInverseKernel": (_C.c_int, [_C.c_int]),
         "digHoloB200ProcessBatchNoAlloc": (_C.c_int, [_C.c_int, _C.c_void_p, _C.c_int, _C.c_int, _C.c_void_p,
                                                      _C.c_void_p, _C.c_void_p, _C.c_void_p]),
     }

@@ -67,6 +67,7 @@ int digHoloDestroy(int h) {
             for (auto e : o->evCopy) if (e) cudaEventDestroy(e);
             if (o->evStart) cudaEventDestroy(o->evStart);
             if (o->evStop) cudaEventDestroy(o->evStop);
+            if (o->hStatus) cudaFreeHost(o->hStatus);
             dh_eigen_destroy(o->eigen);
         }
         delete o;
@@ -556,7 +557,8 @@ complex64* digHoloB200GetCoefsDevice(int h, int* batchCount, int* modeCount, int
 int digHoloB200Synchronize(int h) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     if (!o->stream) return dh::ERR_SUCCESS;
-    return cudaStreamSynchronize(o->stream) == cudaSuccess ? dh::ERR_SUCCESS : dh::ERR_ERROR;
+    if (cudaStreamSynchronize(o->stream) != cudaSuccess) return dh::ERR_ERROR;
+    return dh::objCheckStatus(*o);
 }
 // Keep the float field -conj(A.ref) before int16 rounding (off by default).
 int digHoloB200SetKeepField32(int h, int enable) {
@@ -617,10 +619,27 @@ int digHoloB200GetGeometry(int h, int* out10) {
 }
 // Selects the forward kernel: 0 = fastest available (default), 1 = always
 // the shared-memory kernel (used by the tests to cover both).
-int digHoloB200SetForwardKernel(int h, int generic) {
+int digHoloB200SetForwardKernel(int h, int kernel) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    o->forceGeneric = generic ? 1 : 0;
+    if (kernel < 0 || kernel > 3) return dh::ERR_INVALIDARGUMENT;
+    o->forwardKernel = kernel;
     return dh::ERR_SUCCESS;
+}
+int digHoloB200SetInverseKernel(int h, int kernel) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    if (kernel < 0 || kernel > 1) return dh::ERR_INVALIDARGUMENT;
+    o->inverseKernel = kernel;
+    return dh::ERR_SUCCESS;
+}
+// Inverse kernel used by the last batch: 1 block per unit, 2 warp per unit.
+int digHoloB200GetInverseKernel(int h) {
+    OBJ_OR(h, 0);
+    return o->lastInverseKernel;
+}
+// Forward kernel used by the last batch: 1 generic, 2 register, 3 TMA-fed.
+int digHoloB200GetForwardKernel(int h) {
+    OBJ_OR(h, 0);
+    return o->lastForwardKernel;
 }
 // Number of batch evaluations the last digHoloAutoAlign ran.
 int digHoloB200GetAutoAlignEvaluations(int h) {

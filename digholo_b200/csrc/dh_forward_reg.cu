@@ -18,7 +18,7 @@
 
 #include "dh_common.cuh"
 #include "dh_params.h"
-#include "dh_twiddle64.h"
+#include "dh_twiddle128.h"
 
 using namespace dh;
 

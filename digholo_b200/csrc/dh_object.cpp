@@ -13,6 +13,8 @@
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
@@ -253,6 +255,9 @@ int objInitDevice(Object& o) {
     }
     DH_CUDA(o, o.dTwiddle.ensure(tw.size() * sizeof(float)));
     DH_CUDA(o, cudaMemcpy(o.dTwiddle.ptr, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice));
+    DH_CUDA(o, cudaHostAlloc(reinterpret_cast<void**>(&o.hStatus), sizeof(int), cudaHostAllocMapped));
+    *o.hStatus = 0;
+    DH_CUDA(o, cudaHostGetDevicePointer(reinterpret_cast<void**>(&o.dStatus), o.hStatus, 0));
     return ERR_SUCCESS;
 }
 
@@ -427,6 +432,7 @@ static void forwardParams(Object& o, DhFwdParams& fp) {
     }
     fp.window = o.dWindow.as<float2>();
     fp.twiddle = o.dTwiddle.as<float2>();
+    fp.status = o.dStatus;
     if (o.dTables.ptr) {
         const Geometry& gg = o.geo;
         const size_t P = o.polCount;
@@ -622,6 +628,51 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
     ip.twiddle = o.dTwiddle.as<float2>();
 }
 
+// Forward stage: the TMA-fed persistent kernel where the shape and the
+// alignment allow it, else the register kernel, else the generic one.
+static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
+    const int mode = o.forwardKernel;
+    cudaError_t fe = cudaErrorNotSupported;
+    if (mode == 0 || mode == 3) {
+        fe = dh_launch_forward_tma(fp, o.stream);
+        if (fe == cudaSuccess) { o.lastForwardKernel = 3; return fe; }
+        if (fe != cudaErrorNotSupported || mode == 3) return fe;
+        cudaGetLastError();
+    }
+    if (mode == 0 || mode == 2) {
+        fe = dh_launch_forward_reg(fp, o.stream);
+        if (fe == cudaSuccess) { o.lastForwardKernel = 2; return fe; }
+        if (fe != cudaErrorNotSupported || mode == 2) return fe;
+        cudaGetLastError();
+    }
+    fe = dh_launch_forward(fp, o.stream);
+    if (fe == cudaSuccess) o.lastForwardKernel = 1;
+    return fe;
+}
+
+// Inverse stage: the warp-per-unit kernel for 16/32-pixel low-resolution
+// fields, else the block-per-unit kernel.
+static cudaError_t launchInverse(Object& o, const DhInvParams& ip) {
+    if (o.inverseKernel == 0) {
+        cudaError_t e = dh_launch_inverse_lo(ip, o.stream);
+        if (e == cudaSuccess) { o.lastInverseKernel = 2; return e; }
+        if (e != cudaErrorNotSupported) return e;
+        cudaGetLastError();
+    }
+    cudaError_t e = dh_launch_inverse(ip, o.stream);
+    if (e == cudaSuccess) o.lastInverseKernel = 1;
+    return e;
+}
+
+// Reads the kernels' failure flag after the stream has been synchronised.
+int objCheckStatus(Object& o) {
+    if (o.hStatus && *(volatile int*)o.hStatus) {
+        *(volatile int*)o.hStatus = 0;
+        return fail(o, ERR_ERROR, "forward kernel: a TMA completion wait expired");
+    }
+    return ERR_SUCCESS;
+}
+
 static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0, int f0, int f1) {
     const Geometry& g = o.geo;
     const int P = o.polCount;
@@ -645,11 +696,7 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         o.evStageUsed++;
         DH_CUDA(o, cudaEventRecord(ev[0], o.stream));
     }
-    cudaError_t fe = o.forceGeneric ? cudaErrorNotSupported : dh_launch_forward_reg(fp, o.stream);
-    if (fe == cudaErrorNotSupported) {
-        cudaGetLastError();
-        fe = dh_launch_forward(fp, o.stream);
-    }
+    cudaError_t fe = launchForward(o, fp);
     if (fe != cudaSuccess) return failCuda(o, fe, "forward kernel launch");
     if (timed) DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
     if (ip0.fieldR) {
@@ -662,7 +709,7 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         if (ip.field32) ip.field32 = ip0.field32 + (size_t)f0 * P * npix;
         ip.stats = ip0.stats + f0;
         if (ip.coefs) ip.coefs = ip0.coefs + (size_t)f0 * P * o.modeCount;
-        DH_CUDA(o, dh_launch_inverse(ip, o.stream));
+        DH_CUDA(o, launchInverse(o, ip));
     }
     if (timed) DH_CUDA(o, cudaEventRecord(ev[2], o.stream));
     return ERR_SUCCESS;
@@ -784,13 +831,9 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     ip.statsStride = B + 1;
     ip.coefs = o.cfg.maxMG > 0 ? coefs : nullptr;
     if (!ip.coefs) ip.maxMG = 0;
-    cudaError_t fe = o.forceGeneric ? cudaErrorNotSupported : dh_launch_forward_reg(fp, o.stream);
-    if (fe == cudaErrorNotSupported) {
-        cudaGetLastError();
-        fe = dh_launch_forward(fp, o.stream);
-    }
+    cudaError_t fe = launchForward(o, fp);
     if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
-    DH_CUDA(o, dh_launch_inverse(ip, o.stream));
+    DH_CUDA(o, launchInverse(o, ip));
     return ERR_SUCCESS;
 }
 
@@ -804,13 +847,13 @@ int objProcessForAlign(Object& o) {
 int objCoefsToHost(Object& o) {
     if (o.modeCount <= 0 || !o.dCoefs.ptr) {
         DH_CUDA(o, cudaStreamSynchronize(o.stream));
-        return ERR_SUCCESS;
+        return objCheckStatus(o);
     }
     const size_t n = (size_t)o.batchCount * o.polCount * o.modeCount * sizeof(float2);
     if (!o.hCoefs.ensure(n)) return fail(o, ERR_MEMORYALLOCATION, "host coefficient buffer");
     DH_CUDA(o, cudaMemcpyAsync(o.hCoefs.ptr, o.dCoefs.ptr, n, cudaMemcpyDeviceToHost, o.stream));
     DH_CUDA(o, cudaStreamSynchronize(o.stream));
-    return ERR_SUCCESS;
+    return objCheckStatus(o);
 }
 
 // Individual steps (digHoloProcessFFT/IFFT/RemoveTilt/BasisExtractCoefs).

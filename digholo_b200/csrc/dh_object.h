@@ -145,7 +145,16 @@ struct Object {
     // fftSnap and the Fourier-window selection from ifftSnap
     int useSnaps = 0;
     Config fftSnap, ifftSnap;
-    int forceGeneric = 0;               // use the shared-memory forward kernel for every shape
+    // forward kernel choice: 0 automatic (TMA-fed, then register, then
+    // generic), 1 generic, 2 register, 3 TMA-fed only; and the one that ran last
+    int forwardKernel = 0;
+    int lastForwardKernel = 0;
+    // inverse kernel choice: 0 automatic (warp-per-unit kernel for 16/32-pixel
+    // low-resolution fields, else the block kernel), 1 block kernel
+    int inverseKernel = 0;
+    int lastInverseKernel = 0;
+    int* hStatus = nullptr;             // host-mapped failure flag written by the kernels
+    int* dStatus = nullptr;             // its device address
 
     // host mirrors
     HostBuf hCoefs, hFields, hFieldR, hFieldI, hStats, hStatsFFT, hWindow, hBatchSum;
@@ -168,6 +177,7 @@ int objStatsToHost(Object& o);
 int objWindowToHost(Object& o);
 int objStageTimes(Object& o, float* ms);
 int objProcessForAlign(Object& o);
+int objCheckStatus(Object& o);
 int objCalcMetrics(Object& o);
 float objAutoAlign(Object& o);
 

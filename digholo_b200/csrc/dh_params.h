@@ -39,6 +39,7 @@ struct DhFwdParams {
     const float2* tabSplit; // [pol][w]    exp(-2 pi i (sx0 + c) / W), the R2C split twiddles
     const float2* tabCol;   // [pol][h][Q] exp(-2 pi i row_j b / H), Q = H / h
     const float2* tabAdj;   // [pol][h][w] mask x norm x 1/sinc x exp(i (kx bcx + ky bcy))
+    int* status;            // set to 1 by a kernel whose bounded wait expired (host-mapped)
 };
 
 // Inverse stage: Fourier window -> IFFT -> field statistics -> reference wave,

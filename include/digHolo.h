@@ -323,8 +323,19 @@ int digHoloB200GetStageTimes(int handleIdx, float* out3);
  * (x, y) and IFFT-window origin (SX, SY) of polarisation 0. */
 int digHoloB200GetGeometry(int handleIdx, int* out10);
 
-/* 1: always use the shared-memory forward kernel (testing aid). */
-int digHoloB200SetForwardKernel(int handleIdx, int generic);
+/* Forward kernel choice (testing aid): 0 automatic (the TMA-fed persistent
+ * kernel where shape and alignment allow, else the register kernel, else the
+ * generic one), 1 generic shared-memory kernel, 2 register kernel, 3 TMA-fed
+ * kernel only (the batch fails where it does not apply). */
+int digHoloB200SetForwardKernel(int handleIdx, int kernel);
+/* Forward kernel the last batch ran: 1 generic, 2 register, 3 TMA-fed. */
+int digHoloB200GetForwardKernel(int handleIdx);
+/* Inverse kernel choice (testing aid): 0 automatic (one warp per frame and
+ * polarisation for 16- and 32-pixel low-resolution fields, else one block),
+ * 1 one block per frame and polarisation. */
+int digHoloB200SetInverseKernel(int handleIdx, int kernel);
+/* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit. */
+int digHoloB200GetInverseKernel(int handleIdx);
 
 /* Message of the handle's last error ("" when none). */
 const char* digHoloB200GetLastError(int handleIdx);

@@ -38,13 +38,22 @@ def lib():
     return digholo_b200.load()
 
 
-def _run(lib, hol, cfg, keep32=False, generic=0):
+# (forward, inverse) kernel choices: forward 0 automatic (the TMA-fed
+# persistent kernel wherever it applies), 1 generic shared-memory kernel,
+# 2 register kernel; inverse 0 automatic (one warp per unit for 16/32-pixel
+# low-resolution fields), 1 one block per unit
+KERNELS = [(0, 0), (1, 1), (2, 0), (0, 1)]
+
+
+def _run(lib, hol, cfg, keep32=False, kernel=(0, 0)):
     h = lib.digHoloCreate()
     api.configure(lib, h, cfg)
-    lib.digHoloB200SetForwardKernel(h, generic)
+    assert lib.digHoloB200SetForwardKernel(h, kernel[0]) == 0
+    assert lib.digHoloB200SetInverseKernel(h, kernel[1]) == 0
     if keep32:
         lib.digHoloB200SetKeepField32(h, 1)
     out = api.run_batch(lib, h, hol.frames)
+    out["kernel"] = (lib.digHoloB200GetForwardKernel(h), lib.digHoloB200GetInverseKernel(h))
     if keep32:
         b, p, w, hh = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         fp = lib.digHoloB200GetFields32(h, C.byref(b), C.byref(p), C.byref(w), C.byref(hh))
@@ -55,12 +64,16 @@ def _run(lib, hol, cfg, keep32=False, generic=0):
     return out
 
 
-@pytest.mark.parametrize("generic", [0, 1])
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("workload,frames,mode", CASES)
-def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, generic):
+def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, kernel):
     hol = make_case(workload, frames)
     cfg = config_for(hol, mode)
-    g = _run(lib, hol, cfg, keep32=True, generic=generic)
+    g = _run(lib, hol, cfg, keep32=True, kernel=kernel)
+    # every workload here fits the TMA-fed forward kernel, and in mode 1 the
+    # warp-per-unit inverse kernel; otherwise the kernels asked for run
+    assert g["kernel"][0] == (3 if kernel[0] == 0 else kernel[0])
+    assert g["kernel"][1] == (2 if (kernel[1] == 0 and mode == 1) else 1)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert g["R"].shape == o["R"].shape
     np.testing.assert_array_equal(g["x"], o["x"])
