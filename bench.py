@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--mode", type=int, default=RES_MODE, help="IFFT resolution mode (0 full, 1 window)")
     ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--overlap", default="tc", choices=["tc", "f32"],
+                    help="overlap of full-resolution fields: split-BF16 tensor cores or FP32 CUDA cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -335,6 +337,7 @@ def main():
     api.configure(L, h, cfg)
     L.digHoloB200SetStream(h, C.c_void_p(stream.cuda_stream))
     L.digHoloB200SetTiming(h, 1)
+    L.digHoloB200SetOverlapKernel(h, 0 if args.overlap == "tc" else 1)
 
     def step_device(i):
         t = batches[i % 4]
@@ -407,6 +410,11 @@ def main():
             torch.distributed.destroy_process_group()
         return 0
 
+    # kernels per step: forward + inverse, plus the separate FP32 overlap
+    # kernel for full-resolution fields when that path is chosen
+    per_step = 2 + (1 if (L.digHoloB200GetInverseKernel(h) == 3 and L.digHoloB200GetOverlapKernel(h) == 1) else 0)
+    overlap_name = {1: "fp32 cuda cores", 2: "split-bf16 tensor cores"}.get(L.digHoloB200GetOverlapKernel(h), "?")
+
     # roofline of the dominant kernel (HBM bytes it must move per launch)
     peak, peak_kind = measured_peaks()
     geo = (C.c_int * 10)()
@@ -443,7 +451,8 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded hologram model, generated on the GPU)",
         "config": {"workload": WORKLOAD + "_mode%d" % args.mode, "frames_per_step": B,
                    "frame": "640x512 uint16", "pol": P, "maxMG": G, "modes": M, "fft_window": "%dx%d" % (W, H),
-                   "ifft_resolution_mode": args.mode, "parallelism": "dp%d (independent frames)" % world,
+                   "ifft_resolution_mode": args.mode, "overlap": overlap_name,
+                   "parallelism": "dp%d (independent frames)" % world,
                    "l2": "4 rotating device batches; their window pixels (268 MB) exceed the 126 MB L2"},
         "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps},
@@ -451,7 +460,7 @@ def main():
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": kbytes, "avg_launch_ms": kms,
                      "stage_ms_per_step": {"k_forward": fwd_ms / max(timed, 1), "k_inverse": inv_ms / max(timed, 1)}},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": per_step * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

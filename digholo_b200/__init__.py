@@ -50,6 +50,8 @@ def _bind_extensions(lib, out):
         "digHoloB200GetForwardKernel": (_C.c_int, [_C.c_int]),
         "digHoloB200SetInverseKernel": (_C.c_int, [_C.c_int, _C.c_int]),
         "digHoloB200GetInverseKernel": (_C.c_int, [_C.c_int]),
+        "digHoloB200SetOverlapKernel": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200GetOverlapKernel": (_C.c_int, [_C.c_int]),
         "digHoloB200ProcessBatchNoAlloc": (_C.c_int, [_C.c_int, _C.c_void_p, _C.c_int, _C.c_int, _C.c_void_p,
                                                      _C.c_void_p, _C.c_void_p, _C.c_void_p]),
     }

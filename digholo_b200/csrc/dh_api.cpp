@@ -631,10 +631,22 @@ int digHoloB200SetInverseKernel(int h, int kernel) {
     o->inverseKernel = kernel;
     return dh::ERR_SUCCESS;
 }
-// Inverse kernel used by the last batch: 1 block per unit, 2 warp per unit.
+// Inverse kernel used by the last batch: 1 block per unit, 2 warp per unit,
+// 3 full-resolution field kernel + overlap kernel.
 int digHoloB200GetInverseKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastInverseKernel;
+}
+int digHoloB200SetOverlapKernel(int h, int kernel) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    if (kernel < 0 || kernel > 1) return dh::ERR_INVALIDARGUMENT;
+    o->overlapKernel = kernel;
+    return dh::ERR_SUCCESS;
+}
+// Overlap used by the last batch: 1 FP32 CUDA cores, 2 split-BF16 tensor cores.
+int digHoloB200GetOverlapKernel(int h) {
+    OBJ_OR(h, 0);
+    return o->lastOverlapKernel;
 }
 // Forward kernel used by the last batch: 1 generic, 2 register, 3 TMA-fed.
 int digHoloB200GetForwardKernel(int h) {

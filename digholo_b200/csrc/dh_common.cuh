@@ -62,6 +62,17 @@ __device__ __forceinline__ void fft_dit(float2* base, int count, int seqStride, 
     }
 }
 
+// Round half to even and saturate to int16, as the reference's
+// _mm256_cvtps_epi32 + _mm256_packs_epi32 do (digHolo.cpp:2822-2829): NaN
+// gives INT_MIN there and so -32768 here (fmaxf returns the non-NaN operand).
+// Inputs are scale * v with |scale * v| <= 32767 (1 + 2^-13) for finite
+// fields, so the int32 overflow cases of the conversion never arise.  The
+// clamped value plus 1.5 * 2^23 carries the rounded integer in its low bits.
+__device__ __forceinline__ short roundSat16(float v) {
+    const float c = fminf(fmaxf(v, -32768.0f), 32767.0f);
+    return (short)__float_as_int(c + 12582912.0f);
+}
+
 // x / sin(x) with value 1 at x = 0: the inverse pixel sinc used for the
 // fill-factor correction.
 __device__ __forceinline__ float xcsc(float x) {

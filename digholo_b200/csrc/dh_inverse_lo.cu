@@ -214,13 +214,8 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
             const float2 w = cmul(a, cmul(ry, rx));
             p.field32[o] = make_float2(-w.x, w.y);
         }
-        const float fr = rintf(scale * vr), fi = rintf(scale * vi);
-        // float -> int32 with the x86 convention (NaN / overflow -> INT_MIN),
-        // then saturate to int16 (digHolo.cpp:2822-2829)
-        const int ir = (fr >= -2147483648.0f && fr < 2147483648.0f) ? (int)fr : INT32_MIN;
-        const int ii = (fi >= -2147483648.0f && fi < 2147483648.0f) ? (int)fi : INT32_MIN;
-        const short sr = (short)max(-32768, min(32767, ir));
-        const short si = (short)max(-32768, min(32767, ii));
+        const short sr = roundSat16(scale * vr);
+        const short si = roundSat16(scale * vi);
         p.fieldR[o] = sr;
         p.fieldI[o] = si;
         V[i] = make_float2((float)sr, (float)si);

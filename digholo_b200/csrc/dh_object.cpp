@@ -15,6 +15,8 @@ cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
+cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
+cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStream_t s);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
@@ -608,6 +610,7 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
     for (int p = 0; p < o.polCount; p++) { ip.sx0[p] = g.SX[p] - g.W / 2; ip.sy[p] = g.SY[p]; }
     ip.refWave = o.dRef.as<short>();
     ip.refWaveF = o.dRefF.as<float>();
+    ip.status = o.dStatus;
     ip.xAxis = o.dX.as<float>();
     ip.yAxis = o.dY.as<float>();
     ip.dA = fabsf(g.x[2] - g.x[1]) * fabsf(g.y[2] - g.y[1]);
@@ -658,9 +661,29 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip) {
         if (e == cudaSuccess) { o.lastInverseKernel = 2; return e; }
         if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
+        // full resolution: field kernel, then the overlap kernel
+        int fused = 0;
+        e = dh_launch_field_full(ip, o.overlapKernel == 0, &fused, o.stream);
+        if (e == cudaSuccess && fused) { o.lastInverseKernel = 3; o.lastOverlapKernel = 2; return e; }
+        if (e == cudaErrorNotSupported && fused) {
+            cudaGetLastError();
+            e = dh_launch_field_full(ip, 0, &fused, o.stream);
+        }
+        if (e == cudaSuccess) {
+            const int nx = 1 << ip.logW, ny = 1 << ip.logH;
+            e = dh_launch_overlap_f32(ip, nx, ny, o.stream);
+            if (e == cudaSuccess) { o.lastInverseKernel = 3; o.lastOverlapKernel = 1; return e; }
+            if (e != cudaErrorNotSupported) return e;
+            cudaGetLastError();
+            // overlap shape not covered: rerun the whole stage with the block kernel
+        } else if (e != cudaErrorNotSupported) {
+            return e;
+        } else {
+            cudaGetLastError();
+        }
     }
     cudaError_t e = dh_launch_inverse(ip, o.stream);
-    if (e == cudaSuccess) o.lastInverseKernel = 1;
+    if (e == cudaSuccess) { o.lastInverseKernel = 1; o.lastOverlapKernel = 1; }
     return e;
 }
 
@@ -668,7 +691,7 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip) {
 int objCheckStatus(Object& o) {
     if (o.hStatus && *(volatile int*)o.hStatus) {
         *(volatile int*)o.hStatus = 0;
-        return fail(o, ERR_ERROR, "forward kernel: a TMA completion wait expired");
+        return fail(o, ERR_ERROR, "kernel: a completion wait (TMA or tensor-core commit) expired");
     }
     return ERR_SUCCESS;
 }

@@ -153,6 +153,10 @@ struct Object {
     // low-resolution fields, else the block kernel), 1 block kernel
     int inverseKernel = 0;
     int lastInverseKernel = 0;
+    // overlap of full-resolution fields: 0 tensor cores (split-BF16) where the
+    // shape allows, 1 FP32 CUDA cores; and the one that ran last (1 FP32, 2 tensor)
+    int overlapKernel = 0;
+    int lastOverlapKernel = 0;
     int* hStatus = nullptr;             // host-mapped failure flag written by the kernels
     int* dStatus = nullptr;             // its device address
 

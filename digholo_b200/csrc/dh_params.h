@@ -72,6 +72,7 @@ struct DhInvParams {
     const float* hgScaleY;
     float2* coefs;          // out: [frame][pol*modeCount + mode]
     const float2* twiddle;
+    int* status;            // set by a kernel whose bounded wait expired (host-mapped)
 };
 
 // FP64 Hermite-Gaussian basis along one axis (digHolo.cpp:1269-1484).

@@ -331,11 +331,20 @@ int digHoloB200SetForwardKernel(int handleIdx, int kernel);
 /* Forward kernel the last batch ran: 1 generic, 2 register, 3 TMA-fed. */
 int digHoloB200GetForwardKernel(int handleIdx);
 /* Inverse kernel choice (testing aid): 0 automatic (one warp per frame and
- * polarisation for 16- and 32-pixel low-resolution fields, else one block),
- * 1 one block per frame and polarisation. */
+ * polarisation for 16- and 32-pixel low-resolution fields; the pruned
+ * full-resolution field kernel followed by the overlap kernel for
+ * full-resolution fields; else one block), 1 one block per frame and
+ * polarisation. */
 int digHoloB200SetInverseKernel(int handleIdx, int kernel);
-/* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit. */
+/* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit,
+ * 3 full-resolution field kernel + overlap kernel. */
 int digHoloB200GetInverseKernel(int handleIdx);
+/* Overlap of full-resolution fields: 0 (default) on the tensor cores in
+ * split-BF16 precision (bf16 hi + lo of both int16 operands, three products,
+ * FP32 accumulation) where the field shape allows, 1 FP32 on the CUDA cores. */
+int digHoloB200SetOverlapKernel(int handleIdx, int kernel);
+/* Overlap the last batch ran: 1 FP32 CUDA cores, 2 split-BF16 tensor cores. */
+int digHoloB200GetOverlapKernel(int handleIdx);
 
 /* Message of the handle's last error ("" when none). */
 const char* digHoloB200GetLastError(int handleIdx);
