@@ -1,0 +1,351 @@
+// Gradient-driven AutoAlign.  objAlignGradient evaluates the batch path and
+// its adjoint on the GPU (dh_align_grad.cu): the gradient of
+// IL = 10 log10(sum |c|^2) + const with respect to each polarisation's tilt,
+// defocus, beam centre and basis waist, the Fourier-window selection held
+// fixed.  objAutoAlignAdjoint maximises the same IL with a quasi-Newton
+// (BFGS) iteration in step-normalised coordinates and a backtracking line
+// search, in place of the reference's coordinate search (AutoAlign,
+// digHolo.cpp:12237-12982), and leaves the metrics of the final
+// configuration like digHoloAutoAlign does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dh_grad.h"
+#include "dh_object.h"
+
+namespace dh {
+
+static const double PI_DA = 3.14159265358979323846;
+static const float UNIT_ANGLE_A = (float)(PI_DA / 180.0);
+enum { G_TX = 0, G_TY = 1, G_DEF = 2, G_CX = 3, G_CY = 4, G_WAIST = 5 };
+
+// Captured power S = sum |c|^2 of the last batch (host copy of the coefficients).
+static int capturedPower(Object& o, double& S) {
+    const size_t n = (size_t)o.batchCount * o.polCount * o.modeCount;
+    std::vector<float> hc(2 * n);
+    if (cudaMemcpyAsync(hc.data(), o.dCoefs.ptr, hc.size() * sizeof(float), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess)
+        return ERR_ERROR;
+    if (cudaStreamSynchronize(o.stream) != cudaSuccess) return ERR_ERROR;
+    S = 0.0;
+    for (size_t i = 0; i < hc.size(); i++) S += (double)hc[i] * hc[i];
+    return ERR_SUCCESS;
+}
+
+// grad12[pol * 6 + k], k in {tiltX, tiltY, defocus, beamCentreX, beamCentreY,
+// waist} (config units: degrees, dioptre, m, m); parameters tied by the
+// polarisation locks carry the sum on polarisation 0 and zero on 1.
+// ilOut = 10 log10(S).
+int objAlignGradient(Object& o, float* grad12, float* ilOut) {
+    Config& c = o.cfg;
+    if (c.maxMG <= 0) return fail(o, ERR_ERROR, "adjoint AutoAlign needs a modal basis (maxMG > 0)");
+    const int keep = o.keepField32;
+    o.keepField32 = 1;
+    int r = objProcessForAlign(o);
+    o.keepField32 = keep;
+    if (r) return r;
+    const Geometry& g = o.geo;
+    const int P = o.polCount, B = o.batchCount, G = c.maxMG, M = o.modeCount;
+    const int units = B * P;
+    const int w = g.w, h = g.h, W = g.W, H = g.H;
+    const size_t npix = (size_t)g.nx * g.ny;
+
+    // beam-centre phase derivatives of the window: i kx per column, i ky per row
+    std::vector<float> tab((size_t)P * (w + h));
+    for (int p = 0; p < P; p++) {
+        const int sx0 = g.SX[p] - W / 2;
+        for (int cc = 0; cc < w; cc++) tab[(size_t)p * w + cc] = g.kx[sx0 + cc];
+        for (int j = 0; j < h; j++) {
+            int row = (j + g.SY[p] + H / 2) % H;
+            if (row < 0) row += H;
+            tab[(size_t)P * w + (size_t)p * h + j] = g.ky[row];
+        }
+    }
+    DH_CUDA(o, o.dGradTab.ensure(tab.size() * sizeof(float)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dGradTab.ptr, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    const size_t winElems = (size_t)units * w * h;
+    DH_CUDA(o, o.dGradW.ensure(2 * winElems * sizeof(float2)));
+    float2* Wx = o.dGradW.as<float2>();
+    float2* Wy = Wx + winElems;
+    DH_CUDA(o, dh_launch_window_deriv(o.dWindow.as<float2>(), o.dGradTab.as<float>(), o.dGradTab.as<float>() + (size_t)P * w,
+                                      w, h, P, units, Wx, Wy, o.stream));
+    // fields of the derivative windows
+    DH_CUDA(o, o.dGradV.ensure(2 * (size_t)units * npix * sizeof(float2)));
+    float2* Vx = o.dGradV.as<float2>();
+    float2* Vy = Vx + (size_t)units * npix;
+    DH_CUDA(o, o.dGradScratch.ensure(2 * (size_t)units * npix * sizeof(short) + (size_t)7 * P * (B + 1) * sizeof(float)));
+    short* sR = o.dGradScratch.as<short>();
+    short* sI = sR + (size_t)units * npix;
+    float* sStats = reinterpret_cast<float*>(sI + (size_t)units * npix);
+    r = objInverseAux(o, Wx, Vx, sR, sI, sStats);
+    if (r) return r;
+    r = objInverseAux(o, Wy, Vy, sR, sI, sStats);
+    if (r) return r;
+    // float modes up to order G + 1 (the waist derivative reaches m + 2)
+    const int GE = G + 2;
+    const int L = std::max(g.nx, g.ny);
+    DH_CUDA(o, o.dGradBasis.ensure((size_t)P * GE * (g.nx + g.ny) * sizeof(float) + (size_t)GE * L * sizeof(short) +
+                                   (size_t)GE * sizeof(float)));
+    float* hx = o.dGradBasis.as<float>();
+    float* hy = hx + (size_t)P * GE * g.nx;
+    float* scale = hy + (size_t)P * GE * g.ny;
+    short* s16 = reinterpret_cast<short*>(scale + GE);
+    r = objBasisFloat(o, GE, hx, hy, s16, scale);
+    if (r) return r;
+
+    DhGradParams gp;
+    memset(&gp, 0, sizeof(gp));
+    gp.V = o.dField32.as<float2>();
+    gp.Vx = Vx;
+    gp.Vy = Vy;
+    gp.coefs = o.dCoefs.as<float2>();
+    gp.hx = hx;
+    gp.hy = hy;
+    gp.xAxis = o.dX.as<float>();
+    gp.yAxis = o.dY.as<float>();
+    gp.nx = g.nx;
+    gp.ny = g.ny;
+    gp.frameCount = B;
+    gp.polCount = P;
+    gp.G = G;
+    gp.M = M;
+    const float k0 = (float)(2.0 * PI_DA / c.wavelengthCentre);
+    for (int p = 0; p < P; p++) {
+        const int st = c.polLockTilt ? 0 : p;
+        gp.k0u[p] = k0 * UNIT_ANGLE_A;
+        gp.tiltX[p] = c.zern[st][ZERN_TILTX];
+        gp.tiltY[p] = c.zern[st][ZERN_TILTY];
+        gp.bcx[p] = c.beamCentreX[p];
+        gp.bcy[p] = c.beamCentreY[p];
+        float wv = c.waist[c.polLockBasisWaist ? 0 : p];
+        gp.waist[p] = wv == 0 ? 400e-6f : wv;
+    }
+    gp.piOverLambda = (float)(PI_DA / c.wavelengthCentre);
+    DH_CUDA(o, o.dGradOut.ensure((size_t)units * 6 * sizeof(float)));
+    gp.out = o.dGradOut.as<float>();
+    DH_CUDA(o, dh_launch_align_grad(gp, o.stream));
+    std::vector<float> part((size_t)units * 6);
+    DH_CUDA(o, cudaMemcpyAsync(part.data(), gp.out, part.size() * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    double S = 0.0;
+    r = capturedPower(o, S);   // synchronises the stream
+    if (r) return r;
+    r = objCheckStatus(o);
+    if (r) return r;
+    double acc[2][6] = {};
+    for (int u = 0; u < units; u++)
+        for (int k = 0; k < 6; k++) acc[u % P][k] += part[(size_t)u * 6 + k];
+    // d IL / d theta = 10 / ln 10 * dS / S, dS = 2 Re sum conj(c) dc
+    const double f = (S > 0) ? 20.0 / std::log(10.0) / S : 0.0;
+    for (int p = 0; p < 2; p++)
+        for (int k = 0; k < 6; k++) grad12[p * 6 + k] = p < P ? (float)(f * acc[p][k]) : 0.f;
+    if (P > 1) {
+        auto tie = [&](int k) { grad12[k] += grad12[6 + k]; grad12[6 + k] = 0.f; };
+        if (c.polLockTilt) { tie(G_TX); tie(G_TY); }
+        if (c.polLockDefocus) tie(G_DEF);
+        if (c.polLockBasisWaist) tie(G_WAIST);
+    }
+    if (ilOut) *ilOut = (float)(10.0 * std::log10(S > 0 ? S : 1e-300));
+    return ERR_SUCCESS;
+}
+
+namespace {
+
+struct Param {
+    int pol, kind;
+    double scale;
+};
+
+double getParam(const Config& c, const Param& q) {
+    switch (q.kind) {
+        case G_TX: return c.zern[q.pol][ZERN_TILTX];
+        case G_TY: return c.zern[q.pol][ZERN_TILTY];
+        case G_DEF: return c.zern[q.pol][ZERN_DEFOCUS];
+        case G_CX: return c.beamCentreX[q.pol];
+        case G_CY: return c.beamCentreY[q.pol];
+        default: return c.waist[q.pol];
+    }
+}
+
+void setParam(Config& c, const Param& q, double v) {
+    switch (q.kind) {
+        case G_TX: c.zern[q.pol][ZERN_TILTX] = (float)v; break;
+        case G_TY: c.zern[q.pol][ZERN_TILTY] = (float)v; break;
+        case G_DEF: c.zern[q.pol][ZERN_DEFOCUS] = (float)v; break;
+        case G_CX: c.beamCentreX[q.pol] = (float)v; break;
+        case G_CY: c.beamCentreY[q.pol] = (float)v; break;
+        default: c.waist[q.pol] = (float)v; break;
+    }
+}
+
+}  // namespace
+
+// Maximises IL over the enabled alignment parameters (tilt, beam centre,
+// defocus, waist; tied polarisations share one parameter).  Each evaluation
+// is one GPU batch pass plus its adjoint; the step coordinates are the
+// parameters divided by the reference's search step sizes (tilt 0.1 x the
+// window radius, centre and waist 0.1 x the waist, defocus 0.4,
+// digHolo.cpp:12298-12313).
+float objAutoAlignAdjoint(Object& o) {
+    Config& c = o.cfg;
+    const int P = o.polCount;
+    if (c.maxMG <= 0) return -FLT_MAX;
+    // frames from host memory go to the device once for the whole search
+    const void* userFrames = o.frames;
+    const int userOnDevice = o.framesOnDevice;
+    struct Restore {
+        Object& o; const void* f; int d; int k;
+        ~Restore() { o.frames = f; o.framesOnDevice = d; o.keepField32 = k; o.useSnaps = 0; o.preparedValid = 0; }
+    } restore{o, userFrames, userOnDevice, o.keepField32};
+    o.keepField32 = 1;   // every evaluation needs the float field for the adjoint
+    {
+        int r0 = objProcessForAlign(o);
+        if (r0) return -FLT_MAX;
+        if (!o.framesOnDevice) {
+            const size_t bytes = (size_t)o.batchCount * c.frameWidth * c.frameHeight * (o.framesU16 ? 2 : 4);
+            if (o.dAlignFrames.ensure(bytes) != cudaSuccess) return -FLT_MAX;
+            if (cudaMemcpy(o.dAlignFrames.ptr, o.frames, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return -FLT_MAX;
+            o.frames = o.dAlignFrames.ptr;
+            o.framesOnDevice = 1;
+        }
+    }
+    float w0 = c.waist[0] == 0 ? 400e-6f : c.waist[0];
+    const double tiltStep = c.apertureSize * 0.1;
+    const double centreStep = w0 * 0.1;
+    double defocusStep = 0.4;
+    for (int p = 0; p < P; p++) defocusStep = std::max(defocusStep, (double)std::fabs(c.zern[p][ZERN_DEFOCUS]) * 0.1);
+    const double waistStep = w0 * 0.1;
+    std::vector<Param> prm;
+    for (int p = 0; p < P; p++) {
+        if (c.autoAlignTilt && (p == 0 || !c.polLockTilt)) {
+            prm.push_back({p, G_TX, tiltStep});
+            prm.push_back({p, G_TY, tiltStep});
+        }
+        if (c.autoAlignCentre) {
+            prm.push_back({p, G_CX, centreStep});
+            prm.push_back({p, G_CY, centreStep});
+        }
+        if (c.autoAlignDefocus && (p == 0 || !c.polLockDefocus)) prm.push_back({p, G_DEF, defocusStep});
+        if (c.autoAlignBasisWaist && (p == 0 || !c.polLockBasisWaist)) prm.push_back({p, G_WAIST, waistStep});
+    }
+    const int n = (int)prm.size();
+    o.alignEvaluations = 0;
+    std::vector<double> z(n), gz(n), zt(n), gt(n);
+    for (int i = 0; i < n; i++) z[i] = getParam(c, prm[i]) / prm[i].scale;
+    auto apply = [&](const std::vector<double>& zz) {
+        for (int i = 0; i < n; i++) setParam(c, prm[i], zz[i] * prm[i].scale);
+        if (c.polLockBasisWaist && P > 1) c.waist[1] = c.waist[0];
+    };
+    // f = -IL (minimised) and its gradient in step coordinates
+    auto evalF = [&](const std::vector<double>& zz, double& f, std::vector<double>& gg) -> int {
+        apply(zz);
+        float g12[12], il = 0.f;
+        const int r = objAlignGradient(o, g12, &il);
+        o.alignEvaluations++;
+        if (r) return r;
+        f = -(double)il;
+        for (int i = 0; i < n; i++) gg[i] = -(double)g12[prm[i].pol * 6 + prm[i].kind] * prm[i].scale;
+        return ERR_SUCCESS;
+    };
+    // The FFT window stays where the first evaluation put it; the Fourier
+    // window selection and mask are held during a round (the gradient
+    // assumes them fixed) and re-selected at the reached point between rounds.
+    o.useSnaps = 1;
+    o.fftSnap = o.ifftSnap = c;
+    double f = 0.0;
+    if (n == 0 || evalF(z, f, gz)) {
+        objCalcMetrics(o);
+        return o.autoAlignMetrics[METRIC_IL][0];
+    }
+    // inverse Hessian estimate, initially a scaled identity (first step of unit length)
+    std::vector<double> Hi((size_t)n * n, 0.0);
+    double gn = 0.0;
+    for (double v : gz) gn += v * v;
+    gn = std::sqrt(gn);
+    for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
+    const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.1);   // dB
+    const int maxIter = 40, maxRounds = 3;
+    int quiet = 0, round = 0;
+    double roundStart = f;
+    std::vector<double> d(n), s(n), y(n), Hy(n);
+    for (int it = 0; it < maxIter; it++) {
+        double slope = 0.0;
+        for (int i = 0; i < n; i++) {
+            double v = 0.0;
+            for (int j = 0; j < n; j++) v -= Hi[(size_t)i * n + j] * gz[j];
+            d[i] = v;
+            slope += v * gz[i];
+        }
+        if (slope >= 0) {   // not a descent direction: restart from the gradient
+            for (int i = 0; i < n; i++) {
+                for (int j = 0; j < n; j++) Hi[(size_t)i * n + j] = (i == j) ? 1.0 / std::max(gn, 1e-12) : 0.0;
+                d[i] = -gz[i] / std::max(gn, 1e-12);
+            }
+            slope = 0.0;
+            for (int i = 0; i < n; i++) slope += d[i] * gz[i];
+        }
+        double t = 1.0, ft = 0.0;
+        bool accepted = false;
+        for (int ls = 0; ls < 6; ls++) {
+            for (int i = 0; i < n; i++) zt[i] = z[i] + t * d[i];
+            if (evalF(zt, ft, gt)) return -FLT_MAX;
+            if (ft <= f + 1e-4 * t * slope) { accepted = true; break; }
+            // minimiser of the quadratic through f, slope and ft, kept in [0.1 t, 0.5 t]
+            const double tq = -slope * t * t / (2.0 * (ft - f - slope * t));
+            t = std::min(0.5 * t, std::max(0.1 * t, tq));
+        }
+        if (!accepted) { apply(z); break; }
+        double sy = 0.0;
+        for (int i = 0; i < n; i++) {
+            s[i] = zt[i] - z[i];
+            y[i] = gt[i] - gz[i];
+            sy += s[i] * y[i];
+        }
+        const double df = f - ft;
+        z = zt;
+        gz = gt;
+        f = ft;
+        gn = 0.0;
+        for (double v : gz) gn += v * v;
+        gn = std::sqrt(gn);
+        if (sy > 1e-12) {
+            // BFGS update of the inverse Hessian
+            double yHy = 0.0;
+            for (int i = 0; i < n; i++) {
+                double v = 0.0;
+                for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * y[j];
+                Hy[i] = v;
+                yHy += y[i] * v;
+            }
+            const double rho = 1.0 / sy;
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++)
+                    Hi[(size_t)i * n + j] += (1.0 + yHy * rho) * rho * s[i] * s[j] - rho * (Hy[i] * s[j] + s[i] * Hy[j]);
+        }
+        quiet = (df < tol) ? quiet + 1 : 0;
+        if (quiet >= 2) {
+            // converged with these windows: re-select them at the reached point
+            const double gain = roundStart - f;
+            if (++round >= maxRounds || (round > 1 && gain < tol)) break;
+            const float ap = o.ifftSnap.apertureSize;
+            o.ifftSnap = c;
+            o.ifftSnap.apertureSize = ap;
+            if (evalF(z, f, gz)) return -FLT_MAX;
+            roundStart = f;
+            quiet = 0;
+        }
+    }
+    apply(z);
+    o.useSnaps = 0;
+    // final pass and the metrics of the reached configuration
+    if (objProcessForAlign(o)) return -FLT_MAX;
+    o.alignEvaluations++;
+    objCalcMetrics(o);
+    objCoefsToHost(o);
+    return o.autoAlignMetrics[c.autoAlignGoalIdx][0];
+}
+
+}  // namespace dh

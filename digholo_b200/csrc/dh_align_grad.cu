@@ -1,0 +1,162 @@
+// Adjoint of the batch path for gradient-driven AutoAlign: the gradient of
+// the captured power S = sum |c_mn|^2 (IL = 10 log10 S + const, the power
+// meter's insertion loss, digHolo.cpp:3105-3143 and 11012-11062) with
+// respect to each polarisation's beam centre, tilt, defocus and basis waist,
+// with the Fourier-window selection held fixed.
+//
+// With V = -conj(A R) the tilt-removed field (A the reconstructed field, R
+// the reference wave of digHolo.cpp:10386-10504, phase
+//   phi(x, y) = (-k0 tx + offx) x + bcx (-k0 tx) + focal x^2 + (same in y),
+//   focal = -pi D / lambda),
+// and c_mn = sum_xy Hx_m(x) Hy_n(y) V(x, y) (the separable overlap,
+// digHolo.cpp:2149-2341, in float), dS = 2 Re sum_mn conj(c_mn) dc_mn
+//   = 2 Re sum_xy Abar dV + 2 Re sum_xy Abar_w dw V,
+// Abar = sum_mn conj(c_mn) Hx_m Hy_n (the adjoint field) and
+// Abar_w = sum_mn conj(c_mn) d(Hx_m Hy_n)/dw.  The tangents of V are
+//   dV/dtx = V i k0 u (x + bcx),   dV/dty = V i k0 u (y + bcy)   (u = pi/180),
+//   dV/dD  = V i (pi / lambda) (x^2 + y^2),
+//   dV/dbcx = -conj(A_x R) + V i k0 u tx,  A_x the field of the window times
+//             i kx (the beam-centre phase of digHoloCopyWindow, digHolo.cpp:1955-2035),
+// and for the waist the Hermite-Gaussian ladder relation
+//   dpsi_m/dw = -(1 / 2w) (sqrt(m (m-1)) psi_{m-2} - sqrt((m+1)(m+2)) psi_{m+2}).
+// One block per (frame, polarisation) field; per-field partial sums of
+// Re sum conj(c) dc for the six parameters.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "dh_common.cuh"
+#include "dh_grad.h"
+
+using namespace dh;
+
+
+// Window of the beam-centre derivatives: Wx = i kx W, Wy = i ky W.
+__global__ void k_window_deriv(const float2* __restrict__ W, const float* __restrict__ kxw, const float* __restrict__ kyw,
+                               int w, int h, int polCount, int units, float2* __restrict__ Wx, float2* __restrict__ Wy) {
+    const size_t total = (size_t)units * w * h;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t unit = e / ((size_t)w * h);
+        const int rem = (int)(e - unit * w * h);
+        const int j = rem / w, c = rem - j * w;
+        const int pol = (int)(unit % polCount);
+        const float2 v = W[e];
+        const float kx = kxw[pol * w + c], ky = kyw[pol * h + j];
+        Wx[e] = make_float2(-kx * v.y, kx * v.x);
+        Wy[e] = make_float2(-ky * v.y, ky * v.x);
+    }
+}
+
+// blockDim.x = 256; shared: U, Uw [G][ny] complex, hx/hy derivative rows.
+__global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
+    extern __shared__ float2 sg[];
+    const int unit = blockIdx.x;
+    const int P = p.polCount, G = p.G, M = p.M, nx = p.nx, ny = p.ny;
+    const int pol = unit % P, frame = unit / P;
+    const int GE = G + 2;
+    float2* cc = sg;                                   // [M] conj(c)
+    float2* U = cc + M;                                // [G][ny]  sum_n conj(c_mn) Hy_n(y)
+    float2* Uw = U + (size_t)G * ny;                   // [G][ny]  sum_n conj(c_mn) Hy'_n(y)
+    float* dhx = reinterpret_cast<float*>(Uw + (size_t)G * ny);   // [G][nx] Hx'_m
+    float* dhy = dhx + (size_t)G * nx;                              // [G][ny] Hy'_n
+    float* red = dhy + (size_t)G * ny;                              // [8 warps][6]
+    const float* hxp = p.hx + (size_t)pol * GE * nx;
+    const float* hyp = p.hy + (size_t)pol * GE * ny;
+    const float w0 = p.waist[pol];
+    const int tid = threadIdx.x;
+
+    for (int mode = tid; mode < M; mode += blockDim.x) {
+        const float2 c = p.coefs[(size_t)frame * P * M + (size_t)pol * M + mode];
+        cc[mode] = make_float2(c.x, -c.y);
+    }
+    // ladder derivatives of the modes with respect to the waist
+    for (int e = tid; e < G * nx; e += blockDim.x) {
+        const int m = e / nx, x = e - m * nx;
+        float v = 0.f;
+        if (m >= 2) v += sqrtf((float)(m * (m - 1))) * hxp[(m - 2) * nx + x];
+        v -= sqrtf((float)((m + 1) * (m + 2))) * hxp[(m + 2) * nx + x];
+        dhx[e] = -v / (2.0f * w0);
+    }
+    for (int e = tid; e < G * ny; e += blockDim.x) {
+        const int n = e / ny, y = e - n * ny;
+        float v = 0.f;
+        if (n >= 2) v += sqrtf((float)(n * (n - 1))) * hyp[(n - 2) * ny + y];
+        v -= sqrtf((float)((n + 1) * (n + 2))) * hyp[(n + 2) * ny + y];
+        dhy[e] = -v / (2.0f * w0);
+    }
+    __syncthreads();
+    // U[m][y] = sum_n conj(c_mn) Hy_n(y) over the modes m + n < G (digHolo.cpp:1245-1265 order)
+    for (int e = tid; e < G * ny; e += blockDim.x) {
+        const int m = e / ny, y = e - m * ny;
+        float2 u = make_float2(0.f, 0.f), uw = make_float2(0.f, 0.f);
+        for (int n = 0; m + n < G; n++) {
+            const int g = m + n;
+            const float2 c = cc[g * (g + 1) / 2 + n];
+            const float hv = hyp[n * ny + y], dv = dhy[n * ny + y];
+            u.x = fmaf(c.x, hv, u.x); u.y = fmaf(c.y, hv, u.y);
+            uw.x = fmaf(c.x, dv, uw.x); uw.y = fmaf(c.y, dv, uw.y);
+        }
+        U[e] = u;
+        Uw[e] = uw;
+    }
+    __syncthreads();
+
+    const float2* Vp = p.V + (size_t)unit * nx * ny;
+    const float2* Vxp = p.Vx + (size_t)unit * nx * ny;
+    const float2* Vyp = p.Vy + (size_t)unit * nx * ny;
+    const float k0u = p.k0u[pol];
+    const float txr = p.tiltX[pol], tyr = p.tiltY[pol];
+    const float bx = p.bcx[pol], by = p.bcy[pol];
+    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int e = tid; e < nx * ny; e += blockDim.x) {
+        const int y = e / nx, x = e - y * nx;
+        float2 a = make_float2(0.f, 0.f), aw = make_float2(0.f, 0.f);
+        for (int m = 0; m < G; m++) {
+            const float hv = hxp[m * nx + x], dv = dhx[m * nx + x];
+            const float2 u = U[m * ny + y], uw = Uw[m * ny + y];
+            a.x = fmaf(hv, u.x, a.x); a.y = fmaf(hv, u.y, a.y);
+            aw.x = fmaf(dv, u.x, fmaf(hv, uw.x, aw.x));
+            aw.y = fmaf(dv, u.y, fmaf(hv, uw.y, aw.y));
+        }
+        const float2 v = Vp[e], vx = Vxp[e], vy = Vyp[e];
+        // Re(Abar V i) = -Im(Abar V)
+        const float imAV = a.x * v.y + a.y * v.x;
+        const float xv = p.xAxis[x], yv = p.yAxis[y];
+        s[0] += -imAV * k0u * (xv + bx);
+        s[1] += -imAV * k0u * (yv + by);
+        s[2] += -imAV * p.piOverLambda * (xv * xv + yv * yv);
+        s[3] += (a.x * vx.x - a.y * vx.y) - imAV * k0u * txr;
+        s[4] += (a.x * vy.x - a.y * vy.y) - imAV * k0u * tyr;
+        s[5] += aw.x * v.x - aw.y * v.y;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+    if ((tid & 31) == 0)
+        for (int k = 0; k < 6; k++) red[(tid >> 5) * 6 + k] = s[k];
+    __syncthreads();
+    if (tid < 6) {
+        float t = 0.f;
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 6 + tid];
+        p.out[(size_t)unit * 6 + tid] = t;
+    }
+}
+
+cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const float* kyw, int w, int h, int polCount, int units,
+                                   float2* Wx, float2* Wy, cudaStream_t s) {
+    const size_t total = (size_t)units * w * h;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    k_window_deriv<<<blocks, 256, 0, s>>>(W, kxw, kyw, w, h, polCount, units, Wx, Wy);
+    return cudaGetLastError();
+}
+
+cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s) {
+    const size_t smem = sizeof(float2) * ((size_t)p.M + 2 * (size_t)p.G * p.ny) + sizeof(float) * ((size_t)p.G * (p.nx + p.ny) + 8 * 6);
+    if (smem > 200 * 1024) return cudaErrorNotSupported;
+    cudaError_t e = cudaFuncSetAttribute(k_align_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_align_grad<<<(unsigned)(p.frameCount * p.polCount), 256, smem, s>>>(p);
+    return cudaGetLastError();
+}

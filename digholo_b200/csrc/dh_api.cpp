@@ -653,6 +653,32 @@ int digHoloB200GetForwardKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastForwardKernel;
 }
+// Gradient of IL = 10 log10(sum |c|^2) + const with respect to
+// [pol][tiltX, tiltY, defocus, beamCentreX, beamCentreY, waist] at the current
+// configuration (Fourier-window selection held fixed), from one batch pass
+// and its adjoint on the GPU; il = 10 log10(sum |c|^2).
+int digHoloB200AutoAlignGradient(int h, float* grad12, float* il) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    if (!grad12) return dh::ERR_NULLPOINTER;
+    return dh::objAlignGradient(*o, grad12, il);
+}
+// Holds the FFT window and the Fourier-window selection and mask at the
+// current settings (enable = 1) while the beam-centre phase, the reference
+// wave and the basis keep following the configuration; 0 releases them.
+int digHoloB200FreezeWindow(int h, int enable) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    o->useSnaps = enable ? 1 : 0;
+    if (enable) o->fftSnap = o->ifftSnap = o->cfg;
+    o->preparedValid = 0;
+    return dh::ERR_SUCCESS;
+}
+// Gradient-driven AutoAlign (goal IL): quasi-Newton on the adjoint gradient.
+// Returns the goal metric of the final configuration; the metrics are read
+// with digHoloAutoAlignGetMetric(s) as after digHoloAutoAlign.
+float digHoloB200AutoAlignAdjoint(int h) {
+    OBJ_OR(h, 0.0f);
+    return dh::objAutoAlignAdjoint(*o);
+}
 // Number of batch evaluations the last digHoloAutoAlign ran.
 int digHoloB200GetAutoAlignEvaluations(int h) {
     OBJ_OR(h, 0);

@@ -63,20 +63,6 @@ void HostBuf::release() {
 bool isPow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 int ilog2(int v) { int l = 0; while ((1 << l) < v) l++; return l; }
 
-static int fail(Object& o, int code, const char* what) {
-    o.lastError = what;
-    if (o.cfg.verbosity >= 1) { fprintf(stderr, "digholo_b200: %s\n", what); fflush(stderr); }
-    return code;
-}
-static int failCuda(Object& o, cudaError_t e, const char* where) {
-    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
-    o.lastError = m;
-    fprintf(stderr, "digholo_b200: %s\n", m.c_str());
-    fflush(stderr);
-    return ERR_ERROR;
-}
-#define DH_CUDA(o, call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return failCuda(o, e_, #call); } while (0)
-
 // ------------------------------------------------------------------ geometry
 
 static void axisShifted(int n, float step, std::vector<float>& a) {
@@ -357,8 +343,10 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
         }
         const int cx0 = (g.cx[p] + W / 2) - c.frameWidth / 2;
         const int cy0 = (g.cy[p] + H / 2) - c.frameHeight / 2;
-        const float bcx = c.beamCentreX[p] - (cx0) * c.pixelSize;
-        const float bcy = c.beamCentreY[p] - (cy0) * c.pixelSize;
+        // the beam-centre phase follows the live configuration; the window
+        // selection and the mask may come from a snapshot
+        const float bcx = o.cfg.beamCentreX[p] - (cx0) * c.pixelSize;
+        const float bcy = o.cfg.beamCentreY[p] - (cy0) * c.pixelSize;
         const float kx0 = k0 * sinf(c.zern[p][ZERN_TILTX] * UNIT_ANGLE);
         const float ky0 = k0 * sinf(c.zern[p][ZERN_TILTY] * UNIT_ANGLE);
         for (int j = 0; j < h; j++) {
@@ -412,8 +400,8 @@ static void forwardParams(Object& o, DhFwdParams& fp) {
         fp.sy[p] = g.SY[p];
         const int cx0 = (g.cx[p] + g.W / 2) - c.frameWidth / 2;   // digHolo.cpp:8580-8584
         const int cy0 = (g.cy[p] + g.H / 2) - c.frameHeight / 2;
-        fp.bcx[p] = c.beamCentreX[p] - (cx0) * c.pixelSize;
-        fp.bcy[p] = c.beamCentreY[p] - (cy0) * c.pixelSize;
+        fp.bcx[p] = o.cfg.beamCentreX[p] - (cx0) * c.pixelSize;
+        fp.bcy[p] = o.cfg.beamCentreY[p] - (cy0) * c.pixelSize;
         const float tx = c.zern[p][ZERN_TILTX] * UNIT_ANGLE;       // digHolo.cpp:8588-8589
         const float ty = c.zern[p][ZERN_TILTY] * UNIT_ANGLE;
         fp.kx0[p] = k0 * sinf(tx);
@@ -857,6 +845,41 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     cudaError_t fe = launchForward(o, fp);
     if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
     DH_CUDA(o, launchInverse(o, ip));
+    return ERR_SUCCESS;
+}
+
+// Inverse stage on another window buffer of the current geometry: the float
+// field -conj(A R) to field32, the int16 field and statistics to scratch, no
+// overlap.  The beam-centre derivative fields of the adjoint use it.
+int objInverseAux(Object& o, const float2* window, float2* field32, short* scratchR, short* scratchI, float* scratchStats) {
+    DhInvParams ip;
+    inverseParams(o, ip, 0);
+    ip.window = window;
+    ip.field32 = field32;
+    ip.fieldR = scratchR;
+    ip.fieldI = scratchI;
+    ip.stats = scratchStats;
+    const int k = o.lastInverseKernel, ov = o.lastOverlapKernel;
+    DH_CUDA(o, launchInverse(o, ip));
+    o.lastInverseKernel = k;
+    o.lastOverlapKernel = ov;
+    return ERR_SUCCESS;
+}
+
+// Unquantised float HG modes [pol][modes][n] on the reconstructed-plane axes
+// for the current waists (the FP64 recurrence of digHolo.cpp:1269-1484).
+int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale) {
+    const Config& c = o.cfg;
+    const Geometry& g = o.geo;
+    const int P = o.polCount;
+    for (int p = 0; p < P; p++) {
+        float w = c.waist[c.polLockBasisWaist ? 0 : p];
+        if (w == 0) w = 400e-6f;
+        DhBasisParams bx{o.dX.as<float>(), g.nx, modes, (double)w, scratch16, scratchScale, outX + (size_t)p * modes * g.nx};
+        DH_CUDA(o, dh_launch_basis(bx, o.stream));
+        DhBasisParams by{o.dY.as<float>(), g.ny, modes, (double)w, scratch16, scratchScale, outY + (size_t)p * modes * g.ny};
+        DH_CUDA(o, dh_launch_basis(by, o.stream));
+    }
     return ERR_SUCCESS;
 }
 

@@ -2,6 +2,7 @@
 // fields of digHoloConfig, digHolo.cpp:3323-3372), the derived window
 // geometry, the device buffers and the host mirrors returned to callers.
 #pragma once
+#include <cstdio>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -139,6 +140,8 @@ struct Object {
     int keepField32 = 0;
     // power meter / AutoAlign
     DevBuf dMetricA, dMetricG, dCoefsBackup, dAlignFrames;
+    // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums
+    DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab;
     DhEigen* eigen = nullptr;
     int alignEvaluations = 0;
     // stage snapshots used while AutoAlign runs: the FFT window comes from
@@ -168,6 +171,22 @@ struct Object {
     std::string lastError;
 };
 
+// Error reporting shared by the runtime files: the message is kept for
+// digHoloB200GetLastError and printed at verbosity >= 1 (CUDA errors always).
+inline int fail(Object& o, int code, const char* what) {
+    o.lastError = what;
+    if (o.cfg.verbosity >= 1) { fprintf(stderr, "digholo_b200: %s\n", what); fflush(stderr); }
+    return code;
+}
+inline int failCuda(Object& o, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    o.lastError = m;
+    fprintf(stderr, "digholo_b200: %s\n", m.c_str());
+    fflush(stderr);
+    return ERR_ERROR;
+}
+#define DH_CUDA(o, call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return failCuda(o, e_, #call); } while (0)
+
 // Runtime entry points used by the C ABI layer.
 int objInitDevice(Object& o);
 int objFFT(Object& o);
@@ -182,6 +201,10 @@ int objWindowToHost(Object& o);
 int objStageTimes(Object& o, float* ms);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
+int objInverseAux(Object& o, const float2* window, float2* field32, short* scratchR, short* scratchI, float* scratchStats);
+int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);
+int objAlignGradient(Object& o, float* grad12, float* ilOut);
+float objAutoAlignAdjoint(Object& o);
 int objCalcMetrics(Object& o);
 float objAutoAlign(Object& o);
 

@@ -349,6 +349,22 @@ int digHoloB200GetOverlapKernel(int handleIdx);
 /* Message of the handle's last error ("" when none). */
 const char* digHoloB200GetLastError(int handleIdx);
 
+/* Gradient of IL = 10 log10(sum |c|^2) + const with respect to
+ * grad12[pol * 6 + k], k = tiltX (deg), tiltY (deg), defocus, beamCentreX (m),
+ * beamCentreY (m), waist (m), at the current configuration with the
+ * Fourier-window selection held fixed: one batch pass and its adjoint on the
+ * GPU.  Parameters tied by the polarisation locks carry the sum on
+ * polarisation 0.  *il (optional) = 10 log10(sum |c|^2). */
+int digHoloB200AutoAlignGradient(int handleIdx, float* grad12, float* il);
+/* 1: hold the FFT window and the Fourier-window selection and mask at the
+ * current settings (the beam-centre phase, reference wave and basis keep
+ * following the configuration), as the gradient assumes; 0: release. */
+int digHoloB200FreezeWindow(int handleIdx, int enable);
+/* Gradient-driven AutoAlign (goal IL): quasi-Newton (BFGS) on the adjoint
+ * gradient over the enabled alignment parameters.  Returns the goal metric
+ * of the final configuration; digHoloAutoAlignGetMetric(s) read the metrics. */
+float digHoloB200AutoAlignAdjoint(int handleIdx);
+
 /* Number of batch evaluations (window selection, tilt removal, overlap and
  * power meter) the last digHoloAutoAlign call made. */
 int digHoloB200GetAutoAlignEvaluations(int handleIdx);
