@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--overlap", default="tc", choices=["tc", "f32"],
                     help="overlap of full-resolution fields: split-BF16 tensor cores or FP32 CUDA cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autoalign", action="store_true", help="skip the AutoAlign (plain vs adjoint) measurement")
     return ap.parse_args()
 
 
@@ -444,6 +445,13 @@ def main():
             cpu = {"value": None, "unit": "frames/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % exc}
 
+    align = None
+    if not args.no_autoalign:
+        try:
+            align = autoalign_leg(L, torch, device)
+        except Exception as exc:
+            align = {"unavailable": str(exc)}
+
     line = {
         "metric": "frames/s (FFT->window->IFFT->tilt->HG overlap)",
         "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -463,12 +471,71 @@ def main():
         "gpu_launches": per_step * args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "autoalign": align,
     }
     print(json.dumps(line))
     L.digHoloDestroy(h)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def autoalign_leg(L, torch, device):
+    """ms per AutoAlign, plain coordinate search (digHoloAutoAlign, TWEAK) vs
+    the adjoint-driven search (digHoloB200AutoAlignAdjoint), goal IL, on 512
+    frames of 640x512 float32, two polarisations, each frame one column of a
+    Haar-random 120x120 transfer matrix with 0-1 dB per-mode loss, full
+    resolution (IFFT mode 0); the start is off by +60/-60 um in beam centre,
+    +5/-5 % in tilt, +0.2 in defocus and +15 % in waist.  Frames are device
+    resident; each search runs twice on its handle and the second is timed."""
+    import ctypes as C
+    import numpy as np
+    from digholo_b200 import api, synth
+    kw = dict(synth.WORKLOADS["align_640x512_f32_2pol"])
+    B = kw["frame_count"]
+    kw["coefs"] = synth.transfer_coefs(B, 2, kw["max_mg"], 1004)
+    hol = synth.generate(**kw)
+    frames = torch.from_numpy(np.ascontiguousarray(hol.frames)).to(device)
+
+    class Cfg:
+        pass
+    cfg = Cfg()
+    cfg.frame_width, cfg.frame_height = hol.frame_width, hol.frame_height
+    cfg.pixel_size, cfg.wavelength = hol.pixel_size, hol.wavelength
+    cfg.pol_count, cfg.fft_window, cfg.window_radius_deg = 2, hol.window, hol.radius_deg
+    cfg.resolution_mode, cfg.max_mg, cfg.fill_factor = 0, hol.max_mg, 1
+    cfg.pol_lock_tilt, cfg.pol_lock_defocus, cfg.pol_lock_waist = 0, 0, 1
+    cfg.beam_centre = [[bc[0] + 60e-6, bc[1] - 60e-6] for bc in hol.beam_centres]
+    cfg.tilt_deg = [[t[0] * 1.05, t[1] * 0.95] for t in hol.tilts_deg]
+    cfg.waist = [hol.waist * 1.15] * 2
+    cfg.defocus = [0.2, 0.2]
+    out = {}
+    for name in ("plain", "adjoint"):
+        h = L.digHoloCreate()
+        ms = None
+        for run in range(2):
+            api.configure(L, h, cfg)
+            L.digHoloSetBatch(h, B, C.cast(C.c_void_p(frames.data_ptr()), C.POINTER(C.c_float)))
+            b, m, p = C.c_int(), C.c_int(), C.c_int()
+            L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+            L.digHoloConfigSetAutoAlignMode(h, 1)
+            L.digHoloConfigSetAutoAlignGoalIdx(h, 0)
+            L.digHoloConfigSetAutoAlignTol(h, 0.01)
+            L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
+            L.digHoloB200Synchronize(h)
+            t = time.perf_counter()
+            if name == "plain":
+                L.digHoloAutoAlign(h)
+            else:
+                L.digHoloB200AutoAlignAdjoint(h)
+            L.digHoloB200Synchronize(h)
+            ms = (time.perf_counter() - t) * 1e3
+        out[name] = {"ms": ms, "il_db": L.digHoloAutoAlignGetMetric(h, 0), "mdl_db": L.digHoloAutoAlignGetMetric(h, 1),
+                     "evaluations": L.digHoloB200GetAutoAlignEvaluations(h)}
+        L.digHoloDestroy(h)
+    return {"metric": "ms per AutoAlign (goal IL), host wall clock around the call", "workload":
+            "align_640x512_f32_2pol_mode0: 512 frames, Haar 120x120 transfer, perturbed start",
+            "plain": out["plain"], "adjoint": out["adjoint"], "adjoint_over_plain": out["adjoint"]["ms"] / out["plain"]["ms"]}
 
 
 def H_FRAME(cfg):

@@ -10,8 +10,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -24,18 +26,6 @@ static const double PI_DA = 3.14159265358979323846;
 static const float UNIT_ANGLE_A = (float)(PI_DA / 180.0);
 enum { G_TX = 0, G_TY = 1, G_DEF = 2, G_CX = 3, G_CY = 4, G_WAIST = 5 };
 
-// Captured power S = sum |c|^2 of the last batch (host copy of the coefficients).
-static int capturedPower(Object& o, double& S) {
-    const size_t n = (size_t)o.batchCount * o.polCount * o.modeCount;
-    std::vector<float> hc(2 * n);
-    if (cudaMemcpyAsync(hc.data(), o.dCoefs.ptr, hc.size() * sizeof(float), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess)
-        return ERR_ERROR;
-    if (cudaStreamSynchronize(o.stream) != cudaSuccess) return ERR_ERROR;
-    S = 0.0;
-    for (size_t i = 0; i < hc.size(); i++) S += (double)hc[i] * hc[i];
-    return ERR_SUCCESS;
-}
-
 // grad12[pol * 6 + k], k in {tiltX, tiltY, defocus, beamCentreX, beamCentreY,
 // waist} (config units: degrees, dioptre, m, m); parameters tied by the
 // polarisation locks carry the sum on polarisation 0 and zero on 1.
@@ -43,11 +33,14 @@ static int capturedPower(Object& o, double& S) {
 int objAlignGradient(Object& o, float* grad12, float* ilOut) {
     Config& c = o.cfg;
     if (c.maxMG <= 0) return fail(o, ERR_ERROR, "adjoint AutoAlign needs a modal basis (maxMG > 0)");
+    using Clock = std::chrono::steady_clock;
+    const auto t0 = Clock::now();
     const int keep = o.keepField32;
     o.keepField32 = 1;
     int r = objProcessForAlign(o);
     o.keepField32 = keep;
     if (r) return r;
+    const auto t1 = Clock::now();
     const Geometry& g = o.geo;
     const int P = o.polCount, B = o.batchCount, G = c.maxMG, M = o.modeCount;
     const int units = B * P;
@@ -77,14 +70,14 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
     DH_CUDA(o, o.dGradV.ensure(2 * (size_t)units * npix * sizeof(float2)));
     float2* Vx = o.dGradV.as<float2>();
     float2* Vy = Vx + (size_t)units * npix;
-    DH_CUDA(o, o.dGradScratch.ensure(2 * (size_t)units * npix * sizeof(short) + (size_t)7 * P * (B + 1) * sizeof(float)));
+    // both derivative windows in one launch: a batch of 2B frames (Wy follows Wx, Vy follows Vx)
+    DH_CUDA(o, o.dGradScratch.ensure(4 * (size_t)units * npix * sizeof(short) + (size_t)7 * P * (2 * B + 1) * sizeof(float)));
     short* sR = o.dGradScratch.as<short>();
-    short* sI = sR + (size_t)units * npix;
-    float* sStats = reinterpret_cast<float*>(sI + (size_t)units * npix);
-    r = objInverseAux(o, Wx, Vx, sR, sI, sStats);
+    short* sI = sR + 2 * (size_t)units * npix;
+    float* sStats = reinterpret_cast<float*>(sI + 2 * (size_t)units * npix);
+    r = objInverseAux(o, Wx, 2 * B, Vx, sR, sI, sStats);
     if (r) return r;
-    r = objInverseAux(o, Wy, Vy, sR, sI, sStats);
-    if (r) return r;
+    const auto t2 = Clock::now();
     // float modes up to order G + 1 (the waist derivative reaches m + 2)
     const int GE = G + 2;
     const int L = std::max(g.nx, g.ny);
@@ -96,6 +89,7 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
     short* s16 = reinterpret_cast<short*>(scale + GE);
     r = objBasisFloat(o, GE, hx, hy, s16, scale);
     if (r) return r;
+    const auto t3 = Clock::now();
 
     DhGradParams gp;
     memset(&gp, 0, sizeof(gp));
@@ -125,19 +119,28 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
         gp.waist[p] = wv == 0 ? 400e-6f : wv;
     }
     gp.piOverLambda = (float)(PI_DA / c.wavelengthCentre);
-    DH_CUDA(o, o.dGradOut.ensure((size_t)units * 6 * sizeof(float)));
+    DH_CUDA(o, o.dGradOut.ensure((size_t)units * 7 * sizeof(float)));
     gp.out = o.dGradOut.as<float>();
     DH_CUDA(o, dh_launch_align_grad(gp, o.stream));
-    std::vector<float> part((size_t)units * 6);
-    DH_CUDA(o, cudaMemcpyAsync(part.data(), gp.out, part.size() * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
-    double S = 0.0;
-    r = capturedPower(o, S);   // synchronises the stream
-    if (r) return r;
+    if (!o.hGradOut.ensure((size_t)units * 7 * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "gradient host buffer");
+    const float* part = o.hGradOut.as<float>();
+    DH_CUDA(o, cudaMemcpyAsync(o.hGradOut.ptr, gp.out, (size_t)units * 7 * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    const auto t4 = Clock::now();
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    const auto t5 = Clock::now();
+    if (c.verbosity >= 3) {
+        auto us = [](Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::micro>(b - a).count(); };
+        fprintf(stderr, "digholo_b200: gradient host us: batch %.0f, derivative fields %.0f, basis %.0f, adjoint %.0f, wait %.0f\n",
+                us(t0, t1), us(t1, t2), us(t2, t3), us(t3, t4), us(t4, t5));
+    }
     r = objCheckStatus(o);
     if (r) return r;
     double acc[2][6] = {};
-    for (int u = 0; u < units; u++)
-        for (int k = 0; k < 6; k++) acc[u % P][k] += part[(size_t)u * 6 + k];
+    double S = 0.0;
+    for (int u = 0; u < units; u++) {
+        for (int k = 0; k < 6; k++) acc[u % P][k] += part[(size_t)u * 7 + k];
+        S += part[(size_t)u * 7 + 6];
+    }
     // d IL / d theta = 10 / ln 10 * dS / S, dS = 2 Re sum conj(c) dc
     const double f = (S > 0) ? 20.0 / std::log(10.0) / S : 0.0;
     for (int p = 0; p < 2; p++)
@@ -248,6 +251,11 @@ float objAutoAlignAdjoint(Object& o) {
         if (r) return r;
         f = -(double)il;
         for (int i = 0; i < n; i++) gg[i] = -(double)g12[prm[i].pol * 6 + prm[i].kind] * prm[i].scale;
+        if (c.verbosity >= 2) {
+            fprintf(stderr, "digholo_b200: adjoint AutoAlign evaluation %d: IL %.5f dB, z =", o.alignEvaluations, il);
+            for (int i = 0; i < n; i++) fprintf(stderr, " %.4f", zz[i]);
+            fprintf(stderr, "\n");
+        }
         return ERR_SUCCESS;
     };
     // The FFT window stays where the first evaluation put it; the Fourier
@@ -267,9 +275,10 @@ float objAutoAlignAdjoint(Object& o) {
     gn = std::sqrt(gn);
     for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
     const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.1);   // dB
-    const int maxIter = 40, maxRounds = 3;
+    const int maxIter = 60, maxRounds = 4;
     int quiet = 0, round = 0;
-    double roundStart = f;
+    bool firstUpdate = true;
+    double lastRoundEnd = f;   // objective at the end of the previous round (before re-selection)
     std::vector<double> d(n), s(n), y(n), Hy(n);
     for (int it = 0; it < maxIter; it++) {
         double slope = 0.0;
@@ -312,6 +321,14 @@ float objAutoAlignAdjoint(Object& o) {
         for (double v : gz) gn += v * v;
         gn = std::sqrt(gn);
         if (sy > 1e-12) {
+            if (firstUpdate) {
+                // scale the initial estimate by s.y / y.y before the first update
+                double yy = 0.0;
+                for (int i = 0; i < n; i++) yy += y[i] * y[i];
+                for (size_t i = 0; i < Hi.size(); i++) Hi[i] = 0.0;
+                for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = sy / yy;
+                firstUpdate = false;
+            }
             // BFGS update of the inverse Hessian
             double yHy = 0.0;
             for (int i = 0; i < n; i++) {
@@ -325,22 +342,38 @@ float objAutoAlignAdjoint(Object& o) {
                 for (int j = 0; j < n; j++)
                     Hi[(size_t)i * n + j] += (1.0 + yHy * rho) * rho * s[i] * s[j] - rho * (Hy[i] * s[j] + s[i] * Hy[j]);
         }
+        // converged: a step below the tolerance and a predicted gain of the
+        // next quasi-Newton step (g' H^-1 g / 2) below it too, or two small steps
+        double decrement = 0.0;
+        for (int i = 0; i < n; i++) {
+            double v = 0.0;
+            for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * gz[j];
+            decrement += 0.5 * v * gz[i];
+        }
         quiet = (df < tol) ? quiet + 1 : 0;
-        if (quiet >= 2) {
+        if ((quiet >= 1 && decrement < tol) || quiet >= 2) {
             // converged with these windows: re-select them at the reached point
-            const double gain = roundStart - f;
+            // unless the last re-selection and its round gained too little
+            const double gain = lastRoundEnd - f;
             if (++round >= maxRounds || (round > 1 && gain < tol)) break;
+            lastRoundEnd = f;
             const float ap = o.ifftSnap.apertureSize;
             o.ifftSnap = c;
             o.ifftSnap.apertureSize = ap;
             if (evalF(z, f, gz)) return -FLT_MAX;
-            roundStart = f;
             quiet = 0;
         }
     }
     apply(z);
-    o.useSnaps = 0;
-    // final pass and the metrics of the reached configuration
+    // final pass and the metrics of the reached configuration, with the
+    // Fourier window re-selected there and the FFT window still where the
+    // search found it (the reference's search moves the FFT window only at
+    // the next digHoloFFT either)
+    {
+        const float ap = o.ifftSnap.apertureSize;
+        o.ifftSnap = c;
+        o.ifftSnap.apertureSize = ap;
+    }
     if (objProcessForAlign(o)) return -FLT_MAX;
     o.alignEvaluations++;
     objCalcMetrics(o);

@@ -20,7 +20,7 @@
 // and for the waist the Hermite-Gaussian ladder relation
 //   dpsi_m/dw = -(1 / 2w) (sqrt(m (m-1)) psi_{m-2} - sqrt((m+1)(m+2)) psi_{m+2}).
 // One block per (frame, polarisation) field; per-field partial sums of
-// Re sum conj(c) dc for the six parameters.
+// Re sum conj(c) dc for the six parameters and the field's sum |c|^2.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -59,15 +59,17 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
     float2* Uw = U + (size_t)G * ny;                   // [G][ny]  sum_n conj(c_mn) Hy'_n(y)
     float* dhx = reinterpret_cast<float*>(Uw + (size_t)G * ny);   // [G][nx] Hx'_m
     float* dhy = dhx + (size_t)G * nx;                              // [G][ny] Hy'_n
-    float* red = dhy + (size_t)G * ny;                              // [8 warps][6]
+    float* red = dhy + (size_t)G * ny;                              // [8 warps][7]
     const float* hxp = p.hx + (size_t)pol * GE * nx;
     const float* hyp = p.hy + (size_t)pol * GE * ny;
     const float w0 = p.waist[pol];
     const int tid = threadIdx.x;
 
+    float spow = 0.f;   // captured power of this field
     for (int mode = tid; mode < M; mode += blockDim.x) {
         const float2 c = p.coefs[(size_t)frame * P * M + (size_t)pol * M + mode];
         cc[mode] = make_float2(c.x, -c.y);
+        spow = fmaf(c.x, c.x, fmaf(c.y, c.y, spow));
     }
     // ladder derivatives of the modes with respect to the waist
     for (int e = tid; e < G * nx; e += blockDim.x) {
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
     const float k0u = p.k0u[pol];
     const float txr = p.tiltX[pol], tyr = p.tiltY[pol];
     const float bx = p.bcx[pol], by = p.bcy[pol];
-    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float s[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, spow};
     for (int e = tid; e < nx * ny; e += blockDim.x) {
         const int y = e / nx, x = e - y * nx;
         float2 a = make_float2(0.f, 0.f), aw = make_float2(0.f, 0.f);
@@ -130,15 +132,15 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
         s[5] += aw.x * v.x - aw.y * v.y;
     }
 #pragma unroll
-    for (int k = 0; k < 6; k++)
+    for (int k = 0; k < 7; k++)
         for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
     if ((tid & 31) == 0)
-        for (int k = 0; k < 6; k++) red[(tid >> 5) * 6 + k] = s[k];
+        for (int k = 0; k < 7; k++) red[(tid >> 5) * 7 + k] = s[k];
     __syncthreads();
-    if (tid < 6) {
+    if (tid < 7) {
         float t = 0.f;
-        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 6 + tid];
-        p.out[(size_t)unit * 6 + tid] = t;
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 7 + tid];
+        p.out[(size_t)unit * 7 + tid] = t;
     }
 }
 
@@ -153,7 +155,7 @@ cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const floa
 }
 
 cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s) {
-    const size_t smem = sizeof(float2) * ((size_t)p.M + 2 * (size_t)p.G * p.ny) + sizeof(float) * ((size_t)p.G * (p.nx + p.ny) + 8 * 6);
+    const size_t smem = sizeof(float2) * ((size_t)p.M + 2 * (size_t)p.G * p.ny) + sizeof(float) * ((size_t)p.G * (p.nx + p.ny) + 8 * 7);
     if (smem > 200 * 1024) return cudaErrorNotSupported;
     cudaError_t e = cudaFuncSetAttribute(k_align_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -68,6 +68,7 @@ int digHoloDestroy(int h) {
             if (o->evStart) cudaEventDestroy(o->evStart);
             if (o->evStop) cudaEventDestroy(o->evStop);
             if (o->hStatus) cudaFreeHost(o->hStatus);
+            if (o->evUpload) cudaEventDestroy(o->evUpload);
             dh_eigen_destroy(o->eigen);
         }
         delete o;

@@ -18,7 +18,7 @@ struct DhGradParams {
     float bcx[2], bcy[2];       // beam centre (m) of this polarisation
     float piOverLambda;
     float waist[2];
-    float* out;             // [unit][6]: tx, ty, defocus, bcx, bcy, waist
+    float* out;             // [unit][7]: tx, ty, defocus, bcx, bcy, waist, sum |c|^2
 };
 
 cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const float* kyw, int w, int h, int polCount, int units,

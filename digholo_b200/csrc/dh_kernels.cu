@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "dh_common.cuh"
 #include "dh_params.h"
@@ -337,8 +338,13 @@ __global__ void __launch_bounds__(INV_THREADS) k_inverse(DhInvParams p) {
     }
 }
 
-// One block per axis; blockDim >= 256, up to 4 samples per thread.
-__global__ void __launch_bounds__(1024) k_basis(DhBasisParams p) {
+// Up to four axes per launch (one block each); up to 4 samples per thread.
+struct DhBasisJobs {
+    DhBasisParams job[4];
+};
+
+__global__ void __launch_bounds__(1024) k_basis(DhBasisJobs jobs) {
+    const DhBasisParams& p = jobs.job[blockIdx.x];
     __shared__ double red[32];
     __shared__ double sMax;
     const int L = p.count;
@@ -392,13 +398,14 @@ __global__ void __launch_bounds__(1024) k_basis(DhBasisParams p) {
         __syncthreads();
         const double sf = 32767.0 / sMax;
         const float sff = (float)sf;
-        if (threadIdx.x == 0) p.scale[mode] = (float)(1.0 / sf);
+        const bool q16 = mode < p.modes16;
+        if (threadIdx.x == 0 && q16) p.scale[mode] = (float)(1.0 / sf);
 #pragma unroll
         for (int q = 0; q < PER; q++) {
             if (idx[q] < L) {
                 const float r = rintf(__fmul_rn((float)val[q], sff));
                 const int ir = (r >= -2147483648.0f && r < 2147483648.0f) ? (int)r : INT32_MIN;
-                p.out16[(size_t)mode * L + idx[q]] = (short)max(-32768, min(32767, ir));
+                if (q16) p.out16[(size_t)mode * L + idx[q]] = (short)max(-32768, min(32767, ir));
                 if (p.outF) p.outF[(size_t)mode * L + idx[q]] = (float)val[q];
             }
         }
@@ -467,14 +474,24 @@ cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s) {
-    int threads = (p.count + 3) / 4;
-    threads = ((threads + 31) / 32) * 32;
-    if (threads < 32) threads = 32;
+// n <= 4 axes in one launch.
+cudaError_t dh_launch_basis_jobs(const DhBasisParams* ps, int n, cudaStream_t s) {
+    if (n < 1 || n > 4) return cudaErrorInvalidValue;
+    DhBasisJobs jobs;
+    memset(&jobs, 0, sizeof(jobs));
+    int threads = 32;
+    for (int i = 0; i < n; i++) {
+        jobs.job[i] = ps[i];
+        int t = (ps[i].count + 3) / 4;
+        t = ((t + 31) / 32) * 32;
+        threads = t > threads ? t : threads;
+    }
     if (threads > 1024) return cudaErrorInvalidValue;
-    k_basis<<<1, threads, 0, s>>>(p);
+    k_basis<<<n, threads, 0, s>>>(jobs);
     return cudaGetLastError();
 }
+
+cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s) { return dh_launch_basis_jobs(&p, 1, s); }
 
 cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
                                     int polCount, int frameCount, int npix, float2* out, cudaStream_t s) {

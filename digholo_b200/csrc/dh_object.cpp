@@ -20,6 +20,7 @@ cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStre
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
+cudaError_t dh_launch_basis_jobs(const DhBasisParams* ps, int n, cudaStream_t s);
 cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
                                     int polCount, int frameCount, int npix, float2* out, cudaStream_t s);
 cudaError_t dh_launch_batchsum(const short* R, const short* I, const float* stats, int statsStride,
@@ -464,14 +465,30 @@ static int prepare(Object& o) {
         o.preparedU16 == o.framesU16 && o.preparedBatchCal == o.batchCalVersion)
         return ERR_SUCCESS;
     o.preparedValid = 0;
-    DH_CUDA(o, o.dKx.ensure(g.W * sizeof(float)));
-    DH_CUDA(o, o.dKy.ensure(g.H * sizeof(float)));
-    DH_CUDA(o, cudaMemcpyAsync(o.dKx.ptr, g.kx.data(), g.W * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    DH_CUDA(o, cudaMemcpyAsync(o.dKy.ptr, g.ky.data(), g.H * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    DH_CUDA(o, o.dX.ensure(g.nx * sizeof(float)));
-    DH_CUDA(o, o.dY.ensure(g.ny * sizeof(float)));
-    DH_CUDA(o, cudaMemcpyAsync(o.dX.ptr, g.x.data(), g.nx * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    DH_CUDA(o, cudaMemcpyAsync(o.dY.ptr, g.y.data(), g.ny * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+    // Uploads go through one pinned staging buffer; its previous contents
+    // must have left before it is rewritten (no stream-wide synchronisation).
+    if (o.evUpload) DH_CUDA(o, cudaEventSynchronize(o.evUpload));
+    std::vector<float> split, col, adj;
+    forwardTables(o, split, col, adj);
+    std::vector<short> ref;
+    std::vector<float> refF;
+    referenceWave(c, o.polCount, g, ref, &refF);
+    const size_t nUp = (size_t)g.W + g.H + g.nx + g.ny + 2 * (split.size() + col.size() + adj.size()) + refF.size() +
+                       (ref.size() + 1) / 2 + (o.batchCalEnabled ? o.batchCal.size() : 0) + 64;
+    if (!o.hUpload.ensure(nUp * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "pinned upload buffer");
+    float* up = o.hUpload.as<float>();
+    size_t upOff = 0;
+    auto stage = [&](DevBuf& dst, const void* src, size_t bytes) -> int {
+        DH_CUDA(o, dst.ensure(bytes));
+        memcpy(up + upOff, src, bytes);
+        DH_CUDA(o, cudaMemcpyAsync(dst.ptr, up + upOff, bytes, cudaMemcpyHostToDevice, o.stream));
+        upOff += (bytes + sizeof(float) - 1) / sizeof(float);
+        return ERR_SUCCESS;
+    };
+    if ((r = stage(o.dKx, g.kx.data(), g.W * sizeof(float)))) return r;
+    if ((r = stage(o.dKy, g.ky.data(), g.H * sizeof(float)))) return r;
+    if ((r = stage(o.dX, g.x.data(), g.nx * sizeof(float)))) return r;
+    if ((r = stage(o.dY, g.y.data(), g.ny * sizeof(float)))) return r;
     const size_t B = (size_t)o.batchCount, P = (size_t)o.polCount;
     DH_CUDA(o, o.dWindow.ensure(B * P * g.w * g.h * sizeof(float2)));
     const size_t npix = (size_t)g.nx * g.ny;
@@ -480,32 +497,22 @@ static int prepare(Object& o) {
     if (o.keepField32) DH_CUDA(o, o.dField32.ensure(B * P * npix * sizeof(float2)));
     DH_CUDA(o, o.dStats.ensure((size_t)ANALYSIS_COUNT * P * (B + 1) * sizeof(float)));
     if (o.batchCalEnabled && o.batchCalCount > 0) {
-        const size_t n = o.batchCal.size() * sizeof(float);
-        DH_CUDA(o, o.dBatchCal.ensure(n));
-        DH_CUDA(o, cudaMemcpyAsync(o.dBatchCal.ptr, o.batchCal.data(), n, cudaMemcpyHostToDevice, o.stream));
+        if ((r = stage(o.dBatchCal, o.batchCal.data(), o.batchCal.size() * sizeof(float)))) return r;
     }
     {
-        std::vector<float> split, col, adj;
-        forwardTables(o, split, col, adj);
-        const size_t n = split.size() + col.size() + adj.size();
-        DH_CUDA(o, o.dTables.ensure(n * sizeof(float)));
-        float* t = o.dTables.as<float>();
-        DH_CUDA(o, cudaMemcpyAsync(t, split.data(), split.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-        DH_CUDA(o, cudaMemcpyAsync(t + split.size(), col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-        DH_CUDA(o, cudaMemcpyAsync(t + split.size() + col.size(), adj.data(), adj.size() * sizeof(float),
-                                   cudaMemcpyHostToDevice, o.stream));
-        DH_CUDA(o, cudaStreamSynchronize(o.stream));
+        // tables: split, column-sum and window factors, contiguous on the device
+        std::vector<float> tabs;
+        tabs.reserve(split.size() + col.size() + adj.size());
+        tabs.insert(tabs.end(), split.begin(), split.end());
+        tabs.insert(tabs.end(), col.begin(), col.end());
+        tabs.insert(tabs.end(), adj.begin(), adj.end());
+        if ((r = stage(o.dTables, tabs.data(), tabs.size() * sizeof(float)))) return r;
     }
-    // reference wave (cached inputs are cheap to recompute on the host)
-    std::vector<short> ref;
-    std::vector<float> refF;
-    referenceWave(c, o.polCount, g, ref, &refF);
-    DH_CUDA(o, o.dRef.ensure(ref.size() * sizeof(short)));
-    DH_CUDA(o, cudaMemcpyAsync(o.dRef.ptr, ref.data(), ref.size() * sizeof(short), cudaMemcpyHostToDevice, o.stream));
-    DH_CUDA(o, o.dRefF.ensure(refF.size() * sizeof(float)));
-    DH_CUDA(o, cudaMemcpyAsync(o.dRefF.ptr, refF.data(), refF.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    // the pageable sources must stay alive until the copies complete
-    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    // reference wave (cheap to recompute on the host)
+    if ((r = stage(o.dRef, ref.data(), ref.size() * sizeof(short)))) return r;
+    if ((r = stage(o.dRefF, refF.data(), refF.size() * sizeof(float)))) return r;
+    if (!o.evUpload) DH_CUDA(o, cudaEventCreateWithFlags(&o.evUpload, cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventRecord(o.evUpload, o.stream));
     o.preparedCfg = c;
     o.preparedKeep32 = o.keepField32;
     o.preparedU16 = o.framesU16;
@@ -559,7 +566,7 @@ static int updateBasis(Object& o) {
             // one set of modes on the longer axis; the shorter axis reads its centred sub-range
             const std::vector<float>& la = nx >= ny ? xa : ya;
             DH_CUDA(o, cudaMemcpyAsync(dAxis, la.data(), L * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-            DhBasisParams bp{dAxis, L, G, (double)waist[p], dLong, sx, nullptr};
+            DhBasisParams bp{dAxis, L, G, (double)waist[p], dLong, sx, nullptr, G};
             DH_CUDA(o, dh_launch_basis(bp, o.stream));
             DH_CUDA(o, cudaMemcpyAsync(sy, sx, (size_t)G * sizeof(float), cudaMemcpyDeviceToDevice, o.stream));
             const int off = (L - std::min(nx, ny)) / 2;
@@ -572,9 +579,9 @@ static int updateBasis(Object& o) {
         } else {
             DH_CUDA(o, cudaMemcpyAsync(dAxis, xa.data(), nx * sizeof(float), cudaMemcpyHostToDevice, o.stream));
             DH_CUDA(o, cudaMemcpyAsync(dAxis + nx, ya.data(), ny * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-            DhBasisParams bx{dAxis, nx, G, (double)waist[p], hx, sx, nullptr};
+            DhBasisParams bx{dAxis, nx, G, (double)waist[p], hx, sx, nullptr, G};
             DH_CUDA(o, dh_launch_basis(bx, o.stream));
-            DhBasisParams by{dAxis + nx, ny, G, (double)waist[p], hy, sy, nullptr};
+            DhBasisParams by{dAxis + nx, ny, G, (double)waist[p], hy, sy, nullptr, G};
             DH_CUDA(o, dh_launch_basis(by, o.stream));
         }
         DH_CUDA(o, cudaStreamSynchronize(o.stream));
@@ -851,9 +858,12 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
 // Inverse stage on another window buffer of the current geometry: the float
 // field -conj(A R) to field32, the int16 field and statistics to scratch, no
 // overlap.  The beam-centre derivative fields of the adjoint use it.
-int objInverseAux(Object& o, const float2* window, float2* field32, short* scratchR, short* scratchI, float* scratchStats) {
+int objInverseAux(Object& o, const float2* window, int frameCount, float2* field32, short* scratchR, short* scratchI,
+                  float* scratchStats) {
     DhInvParams ip;
     inverseParams(o, ip, 0);
+    ip.frameCount = frameCount;
+    ip.statsStride = frameCount + 1;
     ip.window = window;
     ip.field32 = field32;
     ip.fieldR = scratchR;
@@ -872,14 +882,17 @@ int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch
     const Config& c = o.cfg;
     const Geometry& g = o.geo;
     const int P = o.polCount;
+    DhBasisParams jobs[4];
+    int n = 0;
     for (int p = 0; p < P; p++) {
         float w = c.waist[c.polLockBasisWaist ? 0 : p];
         if (w == 0) w = 400e-6f;
-        DhBasisParams bx{o.dX.as<float>(), g.nx, modes, (double)w, scratch16, scratchScale, outX + (size_t)p * modes * g.nx};
-        DH_CUDA(o, dh_launch_basis(bx, o.stream));
-        DhBasisParams by{o.dY.as<float>(), g.ny, modes, (double)w, scratch16, scratchScale, outY + (size_t)p * modes * g.ny};
-        DH_CUDA(o, dh_launch_basis(by, o.stream));
+        jobs[n++] = DhBasisParams{o.dX.as<float>(), g.nx, modes, (double)w, scratch16, scratchScale,
+                                  outX + (size_t)p * modes * g.nx, 0};
+        jobs[n++] = DhBasisParams{o.dY.as<float>(), g.ny, modes, (double)w, scratch16, scratchScale,
+                                  outY + (size_t)p * modes * g.ny, 0};
     }
+    DH_CUDA(o, dh_launch_basis_jobs(jobs, n, o.stream));
     return ERR_SUCCESS;
 }
 

@@ -142,6 +142,7 @@ struct Object {
     DevBuf dMetricA, dMetricG, dCoefsBackup, dAlignFrames;
     // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums
     DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab;
+    HostBuf hGradOut;
     DhEigen* eigen = nullptr;
     int alignEvaluations = 0;
     // stage snapshots used while AutoAlign runs: the FFT window comes from
@@ -165,6 +166,8 @@ struct Object {
 
     // host mirrors
     HostBuf hCoefs, hFields, hFieldR, hFieldI, hStats, hStatsFFT, hWindow, hBatchSum;
+    HostBuf hUpload;                    // pinned staging of the per-configuration tables
+    cudaEvent_t evUpload = nullptr;     // the last staged upload has left
     std::vector<float> hX, hY;
     float autoAlignMetrics[METRIC_COUNT][2] = {};
     int metricsValid = 0;
@@ -201,7 +204,8 @@ int objWindowToHost(Object& o);
 int objStageTimes(Object& o, float* ms);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
-int objInverseAux(Object& o, const float2* window, float2* field32, short* scratchR, short* scratchI, float* scratchStats);
+int objInverseAux(Object& o, const float2* window, int frameCount, float2* field32, short* scratchR, short* scratchI,
+                  float* scratchStats);
 int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);
 int objAlignGradient(Object& o, float* grad12, float* ilOut);
 float objAutoAlignAdjoint(Object& o);

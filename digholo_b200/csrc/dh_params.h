@@ -84,4 +84,5 @@ struct DhBasisParams {
     short* out16;        // [modes][count]
     float* scale;        // [modes] float value of one int16 step
     float* outF;         // optional [modes][count] unquantised float modes
+    int modes16;         // modes written to out16 / scale (the first modes16)
 };

@@ -14,7 +14,10 @@ waist +10 %).
   in step-normalised coordinates (the test harness is the only torch user);
 * digHoloB200AutoAlignAdjoint reaches the plain search's (digHoloAutoAlign,
   TWEAK) IL and MDL within 0.01 dB (both metrics: higher is better; MDL in dB
-  is s_min^2 / s_max^2 <= 1).
+  is s_min^2 / s_max^2 <= 1).  In IFFT resolution mode 1 the reconstructed
+  field is 16 pixels across: a waist below a pixel leaves the sampled basis
+  unnormalised and the IL objective grows without bound there (the plain
+  search runs into the waist limit), so that comparison holds the waist.
 """
 import ctypes as C
 import time
@@ -158,17 +161,25 @@ def test_autograd_gradcheck(lib):
     assert ok
 
 
-def _align(L, cfg, frames, adjoint):
+def _align(L, cfg, frames, adjoint, waist=True):
+    # the second search on the same handle is timed (the first one allocates
+    # the handle's buffers); both start from the same perturbed settings
     h, fr = _handle(L, cfg, frames)
-    L.digHoloConfigSetAutoAlignMode(h, 1)
-    L.digHoloConfigSetAutoAlignGoalIdx(h, 0)
-    L.digHoloConfigSetAutoAlignTol(h, 0.01)
-    L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
-    L.digHoloB200Synchronize(h)
-    t = time.perf_counter()
-    val = L.digHoloB200AutoAlignAdjoint(h) if adjoint else L.digHoloAutoAlign(h)
-    L.digHoloB200Synchronize(h)
-    dt = time.perf_counter() - t
+    for run in range(2):
+        if run:
+            api.configure(L, h, cfg)
+            b, m, p = C.c_int(), C.c_int(), C.c_int()
+            L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+        L.digHoloConfigSetAutoAlignBasisWaist(h, 1 if waist else 0)
+        L.digHoloConfigSetAutoAlignMode(h, 1)
+        L.digHoloConfigSetAutoAlignGoalIdx(h, 0)
+        L.digHoloConfigSetAutoAlignTol(h, 0.01)
+        L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
+        L.digHoloB200Synchronize(h)
+        t = time.perf_counter()
+        val = L.digHoloB200AutoAlignAdjoint(h) if adjoint else L.digHoloAutoAlign(h)
+        L.digHoloB200Synchronize(h)
+        dt = time.perf_counter() - t
     metrics = np.array([L.digHoloAutoAlignGetMetric(h, i) for i in range(9)])
     ev = L.digHoloB200GetAutoAlignEvaluations(h)
     L.digHoloDestroy(h)
@@ -179,9 +190,9 @@ def _align(L, cfg, frames, adjoint):
 def test_adjoint_autoalign_matches_plain(lib, mode):
     hol = _case(32)
     cfg = _perturbed(hol, mode)
-    _align(lib, cfg, hol.frames, True)   # warm-up (allocations, basis tables)
-    mp, tp, ep = _align(lib, cfg, hol.frames, False)
-    ma, ta, ea = _align(lib, cfg, hol.frames, True)
+    waist = mode == 0
+    mp, tp, ep = _align(lib, cfg, hol.frames, False, waist)
+    ma, ta, ea = _align(lib, cfg, hol.frames, True, waist)
     print("mode %d plain search IL %.4f MDL %.4f in %.1f ms (%d evaluations); adjoint IL %.4f MDL %.4f in %.1f ms (%d)"
           % (mode, mp[0], mp[1], 1e3 * tp, ep, ma[0], ma[1], 1e3 * ta, ea))
     assert ma[0] >= mp[0] - 0.01
