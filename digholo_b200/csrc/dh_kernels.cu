@@ -413,6 +413,39 @@ __global__ void __launch_bounds__(1024) k_basis(DhBasisJobs jobs) {
     }
 }
 
+// Transpose of each frame: in is [Ny rows][Nx columns], out[f][i * Ny + j] =
+// in[f][j * Nx + i] ([Nx rows][Ny columns]).  32 x 32 tiles through shared
+// memory.
+__global__ void k_untranspose_u16(const unsigned short* __restrict__ in, unsigned short* __restrict__ out, int Nx,
+                                  int Ny, int frames) {
+    __shared__ unsigned short tile[32][33];
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const size_t fp = (size_t)Nx * Ny;
+    for (int f = blockIdx.z; f < frames; f += gridDim.z) {
+        const unsigned short* src = in + (size_t)f * fp;
+        unsigned short* dst = out + (size_t)f * fp;
+        for (int k = 0; k < 32; k += 8) {
+            const int j = j0 + ty + k, i = i0 + tx;
+            if (j < Ny && i < Nx) tile[ty + k][tx] = src[(size_t)j * Nx + i];
+        }
+        __syncthreads();
+        for (int k = 0; k < 32; k += 8) {
+            const int i = i0 + ty + k, j = j0 + tx;
+            if (i < Nx && j < Ny) dst[(size_t)i * Ny + j] = tile[tx][ty + k];
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t dh_launch_untranspose_u16(const unsigned short* in, unsigned short* out, int Nx, int Ny, int frames,
+                                      cudaStream_t s) {
+    if (frames <= 0) return cudaSuccess;
+    dim3 grid((Nx + 31) / 32, (Ny + 31) / 32, frames < 65535 ? frames : 65535);
+    k_untranspose_u16<<<grid, dim3(32, 8), 0, s>>>(in, out, Nx, Ny, frames);
+    return cudaGetLastError();
+}
+
 // int16 field -> complex64 x (1/scale) (digHolo.cpp:4947-4981).
 __global__ void k_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
                                 int polCount, int frameCount, int npix, float2* out) {

@@ -20,6 +20,8 @@ cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStre
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
+cudaError_t dh_launch_untranspose_u16(const unsigned short* in, unsigned short* out, int Nx, int Ny, int frames,
+                                      cudaStream_t s);
 cudaError_t dh_launch_basis_jobs(const DhBasisParams* ps, int n, cudaStream_t s);
 cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float* stats, int statsStride,
                                     int polCount, int frameCount, int npix, float2* out, cudaStream_t s);
@@ -267,7 +269,6 @@ static int checkSupported(Object& o) {
     if (!isPow2(g.w) || !isPow2(g.h))
         return fail(o, ERR_INVALIDDIMENSION, "IFFT window sides must be powers of two on this build");
     if (o.avgCount != 1) return fail(o, ERR_INVALIDARGUMENT, "frame averaging (avgCount > 1) is not supported on this build");
-    if (o.framesTransposed) return fail(o, ERR_INVALIDARGUMENT, "transposed uint16 input is not supported on this build");
     return ERR_SUCCESS;
 }
 
@@ -754,8 +755,44 @@ int objStageTimes(Object& o, float* out) {
 // Full pipeline for the batch: stage -> forward -> inverse (+overlap).
 // With host frames the batch is split in chunks whose window copies overlap
 // the previous chunk's kernels.
+static int processBatchLocked(Object& o, int syncCoefs);
+
+// Transposed uint16 frames (digHoloSetBatchUint16 with transpose): each frame
+// is stored with x and y swapped (frameWidth rows of frameHeight pixels); it
+// is transposed on the device (k_untranspose_u16), then processed like any
+// device batch.  This is the documented intent of the reference's transposing
+// converter (convert_int16tofloat32, digHolo.cpp:1206-1229), whose lane
+// permutation scrambles every other output row.
 int objProcessBatch(Object& o, int syncCoefs) {
     std::lock_guard<std::mutex> guard(o.lock);
+    if (!(o.framesTransposed && o.framesU16)) return processBatchLocked(o, syncCoefs);
+    int r = objInitDevice(o);
+    if (r) return r;
+    if (!o.frames) return fail(o, ERR_NULLPOINTER, "frame buffer not set");
+    const Config& c = o.cfg;
+    const int frames = std::max(1, c.batchCount) * std::max(1, c.avgCount);
+    const size_t bytes = (size_t)frames * c.frameWidth * c.frameHeight * sizeof(unsigned short);
+    const void* src = o.frames;
+    if (!isDevicePointer(o.frames)) {
+        DH_CUDA(o, o.dTransRaw.ensure(bytes));
+        DH_CUDA(o, cudaMemcpyAsync(o.dTransRaw.ptr, o.frames, bytes, cudaMemcpyHostToDevice, o.stream));
+        src = o.dTransRaw.ptr;
+    }
+    DH_CUDA(o, o.dTransFrames.ensure(bytes));
+    // input [frameWidth rows][frameHeight columns] -> [frameHeight rows][frameWidth columns]
+    DH_CUDA(o, dh_launch_untranspose_u16(static_cast<const unsigned short*>(src), o.dTransFrames.as<unsigned short>(),
+                                         c.frameHeight, c.frameWidth, frames, o.stream));
+    struct Restore {
+        Object& o; const void* f; int d;
+        ~Restore() { o.frames = f; o.framesOnDevice = d; o.framesTransposed = 1; }
+    } restore{o, o.frames, o.framesOnDevice};
+    o.frames = o.dTransFrames.ptr;
+    o.framesOnDevice = 1;
+    o.framesTransposed = 0;
+    return processBatchLocked(o, syncCoefs);
+}
+
+static int processBatchLocked(Object& o, int syncCoefs) {
     int r = prepare(o);
     if (r) return r;
     r = updateBasis(o);
