@@ -628,12 +628,12 @@ int digHoloB200SetForwardKernel(int h, int kernel) {
 }
 int digHoloB200SetInverseKernel(int h, int kernel) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    if (kernel < 0 || kernel > 1) return dh::ERR_INVALIDARGUMENT;
+    if (kernel < 0 || kernel > 2) return dh::ERR_INVALIDARGUMENT;
     o->inverseKernel = kernel;
     return dh::ERR_SUCCESS;
 }
 // Inverse kernel used by the last batch: 1 block per unit, 2 warp per unit,
-// 3 full-resolution field kernel + overlap kernel.
+// 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands.
 int digHoloB200GetInverseKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastInverseKernel;

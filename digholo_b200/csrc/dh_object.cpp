@@ -17,6 +17,9 @@ cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
 cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStream_t s);
+size_t dh_field_big_scratch_bytes(const DhInvParams& p, int overlapKind);
+cudaError_t dh_launch_field_big(const DhInvParams& p, int overlapKind, void* scratch, size_t scratchBytes,
+                                int* overlapUsed, cudaStream_t s);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
@@ -649,9 +652,31 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
     return fe;
 }
 
+// Full-resolution fields by bands of 64 rows (any field size); its scratch
+// grows here unless the caller may not allocate.
+static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) {
+    const size_t need = dh_field_big_scratch_bytes(ip, o.overlapKernel);
+    if (need == 0) return cudaErrorNotSupported;
+    if (o.dBigScratch.bytes < need) {
+        if (!mayAlloc) return cudaErrorMemoryAllocation;
+        cudaError_t e = o.dBigScratch.ensure(need);
+        if (e != cudaSuccess) return e;
+    }
+    int used = 0;
+    cudaError_t e = dh_launch_field_big(ip, o.overlapKernel, o.dBigScratch.ptr, o.dBigScratch.bytes, &used, o.stream);
+    if (e == cudaSuccess) {
+        o.lastInverseKernel = 4;
+        o.lastOverlapKernel = used;
+    }
+    return e;
+}
+
 // Inverse stage: the warp-per-unit kernel for 16/32-pixel low-resolution
-// fields, else the block-per-unit kernel.
-static cudaError_t launchInverse(Object& o, const DhInvParams& ip) {
+// fields; for full-resolution fields the pruned field kernel (fields up to
+// 128 x 128) followed by the overlap kernel, else the band kernels; else the
+// block-per-unit kernel.
+static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc = true) {
+    if (o.inverseKernel == 2) return launchBands(o, ip, mayAlloc);
     if (o.inverseKernel == 0) {
         cudaError_t e = dh_launch_inverse_lo(ip, o.stream);
         if (e == cudaSuccess) { o.lastInverseKernel = 2; return e; }
@@ -671,10 +696,15 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip) {
             if (e == cudaSuccess) { o.lastInverseKernel = 3; o.lastOverlapKernel = 1; return e; }
             if (e != cudaErrorNotSupported) return e;
             cudaGetLastError();
-            // overlap shape not covered: rerun the whole stage with the block kernel
+            // overlap shape not covered: rerun the whole stage with another kernel
         } else if (e != cudaErrorNotSupported) {
             return e;
         } else {
+            cudaGetLastError();
+        }
+        if (!ip.lowres && ((1 << ip.logW) > 128 || (1 << ip.logH) > 128)) {
+            e = launchBands(o, ip, mayAlloc);
+            if (e != cudaErrorNotSupported) return e;
             cudaGetLastError();
         }
     }
@@ -888,7 +918,10 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     if (!ip.coefs) ip.maxMG = 0;
     cudaError_t fe = launchForward(o, fp);
     if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
-    DH_CUDA(o, launchInverse(o, ip));
+    fe = launchInverse(o, ip, false);
+    if (fe == cudaErrorMemoryAllocation)
+        return fail(o, ERR_MEMORYALLOCATION, "no-alloc path: the band scratch was sized for a smaller batch");
+    DH_CUDA(o, fe);
     return ERR_SUCCESS;
 }
 

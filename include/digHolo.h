@@ -331,13 +331,16 @@ int digHoloB200SetForwardKernel(int handleIdx, int kernel);
 /* Forward kernel the last batch ran: 1 generic, 2 register, 3 TMA-fed. */
 int digHoloB200GetForwardKernel(int handleIdx);
 /* Inverse kernel choice (testing aid): 0 automatic (one warp per frame and
- * polarisation for 16- and 32-pixel low-resolution fields; the pruned
- * full-resolution field kernel followed by the overlap kernel for
- * full-resolution fields; else one block), 1 one block per frame and
- * polarisation. */
+ * polarisation for 16- and 32-pixel low-resolution fields; for
+ * full-resolution fields the pruned field kernel followed by the overlap
+ * kernel up to 128 x 128 pixels, bands of 64 rows beyond; else one block),
+ * 1 one block per frame and polarisation, 2 full-resolution bands only (the
+ * batch fails where they do not apply: low resolution, fields under 64 x 64,
+ * windows under 16 pixels, maxMG > 32). */
 int digHoloB200SetInverseKernel(int handleIdx, int kernel);
 /* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit,
- * 3 full-resolution field kernel + overlap kernel. */
+ * 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands
+ * (statistics pass, quantising pass with the overlap, coefficient sum). */
 int digHoloB200GetInverseKernel(int handleIdx);
 /* Overlap of full-resolution fields: 0 (default) on the tensor cores in
  * split-BF16 precision (bf16 hi + lo of both int16 operands, three products,

@@ -1,0 +1,96 @@
+"""Full-resolution fields by bands of 64 rows (inverse kernel 4): a
+statistics pass, a quantising pass with the overlap (split-BF16 tensor cores
+or FP32 CUDA cores) and a coefficient sum.  Fields larger than 128 x 128 take
+this path by default; digHoloB200SetInverseKernel(h, 2) forces it for smaller
+fields.
+
+Cases: 512 x 512 uint16 frames with a 256 x 256 FFT window (32 x 32 IFFT
+window); 640 x 512 float frames, two polarisations, a 256 x 128 window
+(32 x 16 IFFT window, rectangular); the 640 x 512 uint16 two-polarisation
+batch with its 128 x 128 window forced onto the bands.  Tolerances as in
+test_gpu_parity: int16 fields within 2 LSB of the quantised oracle, field
+relative L2 <= 5e-5, scales relative <= 1e-5, coefficients relative L2 <=
+5e-5 (FP32) or 1e-4 (split-BF16), FP32 fields before rounding relative L2 <=
+1e-5 against the unquantised oracle.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import digholo_oracle as O
+from digholo_b200 import api, synth
+from helpers import config_for, make_case, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import digholo_b200
+    return digholo_b200.load()
+
+
+def _case(name):
+    if name == "square256":
+        return synth.generate(frame_count=6, frame_width=512, frame_height=512, pol_count=1, max_mg=9, waist=250e-6,
+                              snr_db=30, window=(256, 256), dtype="uint16", seed=11)
+    if name == "rect256x128":
+        return synth.generate(frame_count=6, frame_width=640, frame_height=512, pol_count=2, max_mg=12, waist=220e-6,
+                              snr_db=30, window=(256, 128), dtype="float32", seed=12)
+    return make_case("batched_640x512_u16_2pol", 6)
+
+
+def _run(L, hol, cfg, inverse, overlap):
+    h = L.digHoloCreate()
+    api.configure(L, h, cfg)
+    assert L.digHoloB200SetInverseKernel(h, inverse) == 0
+    assert L.digHoloB200SetOverlapKernel(h, overlap) == 0
+    L.digHoloB200SetKeepField32(h, 1)
+    out = api.run_batch(L, h, hol.frames)
+    assert out["coefs"] is not None, L.digHoloB200GetLastError(h)
+    out["kernel"] = L.digHoloB200GetInverseKernel(h)
+    out["overlap"] = L.digHoloB200GetOverlapKernel(h)
+    b, p, w, hh = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    fp = L.digHoloB200GetFields32(h, C.byref(b), C.byref(p), C.byref(w), C.byref(hh))
+    n = b.value * p.value * w.value * hh.value
+    out["field32"] = np.ctypeslib.as_array(fp, shape=(2 * n,)).copy().view(np.complex64).reshape(
+        b.value, p.value, hh.value, w.value)
+    L.digHoloDestroy(h)
+    return out
+
+
+@pytest.mark.parametrize("overlap", [0, 1])
+@pytest.mark.parametrize("name,inverse", [("square256", 0), ("rect256x128", 0), ("batched128", 2)])
+def test_bands_vs_oracle(lib, name, inverse, overlap):
+    hol = _case(name)
+    cfg = config_for(hol, 0)
+    g = _run(lib, hol, cfg, inverse, overlap)
+    assert g["kernel"] == 4
+    assert g["overlap"] == (2 if overlap == 0 else 1)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    assert g["R"].shape == o["R"].shape
+    np.testing.assert_array_equal(g["x"], o["x"])
+    np.testing.assert_array_equal(g["y"], o["y"])
+    assert np.max(np.abs(g["scale"].T - o["scale"]) / o["scale"]) <= 1e-5
+    assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
+    assert rel_l2(g["field"], o["field"]) <= 5e-5
+    err = rel_l2(g["coefs"], o["coefs"])
+    print("%s overlap %d: coefficient rel L2 %.2e" % (name, overlap, err))
+    assert err <= (1e-4 if overlap == 0 else 5e-5)
+    ex = O.process_batch(hol.frames, cfg, quantised=False)
+    assert rel_l2(g["field32"], ex["field_v"]) <= 1e-5
+
+
+def test_bands_match_field_kernel(lib):
+    """The 128 x 128 batch through the bands and through the pruned
+    full-resolution field kernel: the same int16 fields within 1 LSB and the
+    same statistics (batch summary) within FP32 rounding."""
+    hol = _case("batched128")
+    cfg = config_for(hol, 0)
+    a = _run(lib, hol, cfg, 2, 1)
+    b = _run(lib, hol, cfg, 0, 1)
+    assert b["kernel"] == 3
+    assert max(np.abs(a["R"].astype(int) - b["R"]).max(), np.abs(a["I"].astype(int) - b["I"]).max()) <= 1
+    np.testing.assert_allclose(a["summary"], b["summary"], rtol=1e-5, atol=1e-6)
+    assert rel_l2(a["coefs"], b["coefs"]) <= 1e-5
