@@ -56,6 +56,8 @@ def parse():
                     help="overlap of full-resolution fields: split-BF16 tensor cores or FP32 CUDA cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autoalign", action="store_true", help="skip the AutoAlign (plain vs adjoint) measurement")
+    ap.add_argument("--no-largefield", action="store_true",
+                    help="skip the large-field measurement (2048x2048 frames, 512x512 fields, 465 modes)")
     return ap.parse_args()
 
 
@@ -66,10 +68,10 @@ def dist_env():
     return rank, world, local
 
 
-def workload_config(mode, frames):
+def workload_config(mode, frames, workload=WORKLOAD):
     """Hologram parameters (beam centres, tilts, window radius) and the matching digHolo configuration."""
     from digholo_b200 import synth
-    kw = dict(synth.WORKLOADS[WORKLOAD])
+    kw = dict(synth.WORKLOADS[workload])
     kw["frame_count"] = 1
     hol = synth.generate(**kw)
 
@@ -91,7 +93,8 @@ def workload_config(mode, frames):
     c.beam_centre = hol.beam_centres
     c.tilt_deg = hol.tilts_deg
     c.defocus = [0.0, 0.0]
-    c.snr_db = synth.WORKLOADS[WORKLOAD]["snr_db"]
+    c.snr_db = synth.WORKLOADS[workload]["snr_db"]
+    c.taper = bool(synth.WORKLOADS[workload].get("taper", False))
     c.frames = frames
     return c
 
@@ -123,6 +126,8 @@ def torch_frames(cfg, n, seed, device):
             f1 = min(n, f0 + 128)
             c = torch.complex(torch.randn((f1 - f0, M), generator=g, device=device),
                               torch.randn((f1 - f0, M), generator=g, device=device)) / math.sqrt(2)
+            if getattr(cfg, "taper", False):
+                c = c / (torch.as_tensor(ms + ns, device=device, dtype=torch.float32) + 1.0)
             cm = torch.zeros((f1 - f0, G, G), device=device, dtype=torch.complex64)
             cm[:, torch.as_tensor(ms, device=device), torch.as_tensor(ns, device=device)] = c
             s = torch.einsum("fmn,ny,mx->fyx", cm, hy.to(torch.complex64), hx.to(torch.complex64))
@@ -445,6 +450,13 @@ def main():
             cpu = {"value": None, "unit": "frames/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % exc}
 
+    large = None
+    if not args.no_largefield:
+        try:
+            large = largefield_leg(L, torch, device, stream, args.no_cpu_baseline)
+        except Exception as exc:
+            large = {"unavailable": str(exc)}
+
     align = None
     if not args.no_autoalign:
         try:
@@ -472,12 +484,77 @@ def main():
         "clocks": clocks,
         "cpu_baseline": cpu,
         "autoalign": align,
+        "largefield": large,
     }
     print(json.dumps(line))
     L.digHoloDestroy(h)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def largefield_leg(L, torch, device, stream, no_cpu):
+    """frames/s on the large-field workload: 256 frames of 2048x2048 uint16,
+    two polarisations, FFT window 512x512, full resolution (IFFT mode 0,
+    the reference's default: 512x512 fields by the band kernels), maxMG 30
+    (465 modes), waist 600 um, 20 dB SNR, 1/(group+1) coefficient taper; the
+    overlap in split-BF16 on the tensor cores and in FP32 on the CUDA cores.
+    Two device-resident batches (2.1 GB each, beyond L2) alternate; CUDA
+    events on the library's stream; 3 warm-up and 5 timed batches each."""
+    import ctypes as C
+    import numpy as np
+    from digholo_b200 import api
+    B, steps, warmup = 256, 5, 3
+    cfg = workload_config(0, B, "largefield_2048_u16_2pol")
+    batches = [torch_frames(cfg, B, 5000 + i, device) for i in range(2)]
+    torch.cuda.synchronize()
+    out = {"metric": "frames/s (FFT->window->IFFT->tilt->HG overlap), device-resident frames",
+           "workload": "largefield_2048_u16_2pol_mode0: 256 frames 2048x2048 uint16, 2 pol, window 512x512, "
+                       "maxMG 30 (465 modes)", "steps": steps, "warmup": warmup}
+    for name, ov in (("split_bf16", 0), ("fp32", 1)):
+        h = L.digHoloCreate()
+        api.configure(L, h, cfg)
+        L.digHoloB200SetStream(h, C.c_void_p(stream.cuda_stream))
+        L.digHoloB200SetTiming(h, 1)
+        L.digHoloB200SetOverlapKernel(h, ov)
+
+        def step(i):
+            t = batches[i % 2]
+            L.digHoloSetBatchUint16(h, B, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_ushort)), 0)
+            if L.digHoloB200ProcessBatchDevice(h) != 0:
+                raise RuntimeError("ProcessBatchDevice failed: %s" % L.digHoloB200GetLastError(h))
+        for i in range(warmup):
+            step(i)
+        torch.cuda.synchronize()
+        st = (C.c_float * 3)()
+        L.digHoloB200GetStageTimes(h, st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            step(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        L.digHoloB200GetStageTimes(h, st)
+        n = max(st[2], 1.0)
+        out[name] = {"value": B * steps / (ms / 1e3), "unit": "frames/s", "ms_per_step": ms / steps,
+                     "stage_ms_per_step": {"forward": st[0] / n, "inverse": st[1] / n},
+                     "inverse_kernel": L.digHoloB200GetInverseKernel(h),
+                     "overlap_kernel": L.digHoloB200GetOverlapKernel(h)}
+        L.digHoloDestroy(h)
+    if not no_cpu:
+        try:
+            sample = np.ascontiguousarray(batches[0][:4].cpu().numpy().view(np.uint16))
+            threads = os.cpu_count() or 1
+            fps, calls, el = reference_run(cfg, sample, 8.0, threads)
+            out["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "reference",
+                                   "sample": "4 of the 256 frames, digHoloProcessBatch repeated for %.1f s (%d calls)"
+                                             % (el, calls)}
+        except Exception as exc:
+            out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % exc}
+    del batches
+    torch.cuda.empty_cache()
+    return out
 
 
 def autoalign_leg(L, torch, device):

@@ -622,7 +622,7 @@ int digHoloB200GetGeometry(int h, int* out10) {
 // the shared-memory kernel (used by the tests to cover both).
 int digHoloB200SetForwardKernel(int h, int kernel) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    if (kernel < 0 || kernel > 3) return dh::ERR_INVALIDARGUMENT;
+    if (kernel < 0 || kernel > 4) return dh::ERR_INVALIDARGUMENT;
     o->forwardKernel = kernel;
     return dh::ERR_SUCCESS;
 }
@@ -649,7 +649,8 @@ int digHoloB200GetOverlapKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastOverlapKernel;
 }
-// Forward kernel used by the last batch: 1 generic, 2 register, 3 TMA-fed.
+// Forward kernel used by the last batch: 1 generic, 2 register, 3 TMA-fed,
+// 4 tensor-core row DFT (uint16 frames).
 int digHoloB200GetForwardKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastForwardKernel;

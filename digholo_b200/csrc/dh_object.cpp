@@ -14,6 +14,8 @@ size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s);
+int dh_forward_i8_npad(int w);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
 cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStream_t s);
@@ -385,6 +387,52 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
     }
 }
 
+// Byte digits of the tensor-core row DFT (k_forward_i8): for every kept kx
+// column k = sx0 + c the 22-bit fixed-point values v = round((cos(2 pi k x / W)
+// + 1) 2^22) and round((1 - sin(2 pi k x / W)) 2^22), v = d0 2^16 + d1 2^8 +
+// d2, and a ones column (v = 1).  Accumulator q pairs the low byte of pixel x
+// with digit q - 1 and the high byte with digit q (digits -1 and 3 are zero).
+// Layout [pol][q][atom][npad][128 B], 16-byte chunk c of row n at c ^ (n & 7)
+// (the K-major 128-byte-swizzled operand).  Empty when the kernel does not
+// apply to the geometry.
+static void dftDigits(const Object& o, std::vector<unsigned char>& out) {
+    out.clear();
+    const Geometry& g = o.geo;
+    const int W = g.W, w = g.w, P = o.polCount;
+    if (!o.framesU16 || g.H != 128 || (W != 64 && W != 128) || g.h != w || (w != 16 && w != 32)) return;
+    const int npad = dh_forward_i8_npad(w), natom = 2 * W / 128;
+    out.assign((size_t)P * 4 * natom * npad * 128, 0);
+    for (int p = 0; p < P; p++) {
+        const int sx0 = g.SX[p] - W / 2;
+        for (int n = 0; n < npad; n++) {
+            for (int x = 0; x < W; x++) {
+                long long v = 0;
+                if (n < 2 * w) {
+                    const int k = sx0 + (n < w ? n : n - w);
+                    const int m = (int)((((long long)k * x) % W + W) % W);
+                    const double ang = 2.0 * PI_D * (double)m / (double)W;
+                    const double val = n < w ? cos(ang) + 1.0 : 1.0 - sin(ang);
+                    v = llround(val * 4194304.0);
+                } else if (n == 2 * w) {
+                    v = 1;
+                }
+                const unsigned char d[3] = {(unsigned char)(v >> 16), (unsigned char)((v >> 8) & 255),
+                                            (unsigned char)(v & 255)};
+                for (int q = 0; q < 4; q++) {
+                    for (int hi = 0; hi < 2; hi++) {
+                        const int di = q - 1 + hi;
+                        const unsigned char byte = (di >= 0 && di <= 2) ? d[di] : 0;
+                        const int b = 2 * x + hi, a = b >> 7, bb = b & 127, ch = bb >> 4;
+                        const size_t off = (((size_t)p * 4 + q) * natom + a) * npad * 128 + (size_t)n * 128 +
+                                           (size_t)((ch ^ (n & 7)) << 4) + (bb & 15);
+                        out[off] = byte;
+                    }
+                }
+            }
+        }
+    }
+}
+
 static void forwardParams(Object& o, DhFwdParams& fp) {
     const Config& c = o.useSnaps ? o.ifftSnap : o.cfg;
     const Geometry& g = o.geo;
@@ -436,6 +484,10 @@ static void forwardParams(Object& o, DhFwdParams& fp) {
         fp.tabCol = t + P * gg.w;
         fp.tabAdj = t + P * gg.w + P * gg.h * (gg.H / gg.h);
     }
+    if (o.digitsValid && o.dDigits.ptr) {
+        fp.dftDigits = o.dDigits.as<unsigned char>();
+        fp.dftNpad = o.digitsValid;
+    }
 }
 
 // digHoloFFT_SetWindow + digHoloIFFT_SetWindow: geometry, axes, buffers.
@@ -474,11 +526,13 @@ static int prepare(Object& o) {
     if (o.evUpload) DH_CUDA(o, cudaEventSynchronize(o.evUpload));
     std::vector<float> split, col, adj;
     forwardTables(o, split, col, adj);
+    std::vector<unsigned char> digits;
+    dftDigits(o, digits);
     std::vector<short> ref;
     std::vector<float> refF;
     referenceWave(c, o.polCount, g, ref, &refF);
     const size_t nUp = (size_t)g.W + g.H + g.nx + g.ny + 2 * (split.size() + col.size() + adj.size()) + refF.size() +
-                       (ref.size() + 1) / 2 + (o.batchCalEnabled ? o.batchCal.size() : 0) + 64;
+                       (ref.size() + 1) / 2 + (o.batchCalEnabled ? o.batchCal.size() : 0) + digits.size() / 4 + 64;
     if (!o.hUpload.ensure(nUp * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "pinned upload buffer");
     float* up = o.hUpload.as<float>();
     size_t upOff = 0;
@@ -511,6 +565,11 @@ static int prepare(Object& o) {
         tabs.insert(tabs.end(), col.begin(), col.end());
         tabs.insert(tabs.end(), adj.begin(), adj.end());
         if ((r = stage(o.dTables, tabs.data(), tabs.size() * sizeof(float)))) return r;
+    }
+    o.digitsValid = 0;
+    if (!digits.empty()) {
+        if ((r = stage(o.dDigits, digits.data(), digits.size()))) return r;
+        o.digitsValid = dh_forward_i8_npad(g.w);
     }
     // reference wave (cheap to recompute on the host)
     if ((r = stage(o.dRef, ref.data(), ref.size() * sizeof(short)))) return r;
@@ -635,6 +694,12 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
 static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
     const int mode = o.forwardKernel;
     cudaError_t fe = cudaErrorNotSupported;
+    if (mode == 0 || mode == 4) {
+        fe = dh_launch_forward_i8(fp, o.stream);
+        if (fe == cudaSuccess) { o.lastForwardKernel = 4; return fe; }
+        if (fe != cudaErrorNotSupported || mode == 4) return fe;
+        cudaGetLastError();
+    }
     if (mode == 0 || mode == 3) {
         fe = dh_launch_forward_tma(fp, o.stream);
         if (fe == cudaSuccess) { o.lastForwardKernel = 3; return fe; }

@@ -140,6 +140,8 @@ struct Object {
     int keepField32 = 0;
     // power meter / AutoAlign
     DevBuf dMetricA, dMetricG, dCoefsBackup, dAlignFrames;
+    DevBuf dDigits;                     // tensor-core row DFT digits (uint16 frames)
+    int digitsValid = 0;
     DevBuf dBigScratch;                 // band kernels: partial statistics and coefficients, prepared Hx
     DevBuf dTransRaw, dTransFrames;     // transposed uint16 input: raw host copy, converted frames
     // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums

@@ -39,6 +39,11 @@ struct DhFwdParams {
     const float2* tabSplit; // [pol][w]    exp(-2 pi i (sx0 + c) / W), the R2C split twiddles
     const float2* tabCol;   // [pol][h][Q] exp(-2 pi i row_j b / H), Q = H / h
     const float2* tabAdj;   // [pol][h][w] mask x norm x 1/sinc x exp(i (kx bcx + ky bcy))
+    // Tensor-core row DFT of uint16 frames: 22-bit fixed-point (cos + 1,
+    // -sin + 1) of the kept kx columns plus a ones column, as byte digits in
+    // the swizzled K-major operand layout [pol][4][2W / 128][dftNpad][128 B].
+    const unsigned char* dftDigits;
+    int dftNpad;
     int* status;            // set to 1 by a kernel whose bounded wait expired (host-mapped)
 };
 

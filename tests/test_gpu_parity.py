@@ -38,11 +38,13 @@ def lib():
     return digholo_b200.load()
 
 
-# (forward, inverse) kernel choices: forward 0 automatic (the TMA-fed
-# persistent kernel wherever it applies), 1 generic shared-memory kernel,
-# 2 register kernel; inverse 0 automatic (one warp per unit for 16/32-pixel
-# low-resolution fields), 1 one block per unit
-KERNELS = [(0, 0), (1, 1), (2, 0), (0, 1)]
+# (forward, inverse) kernel choices: forward 0 automatic (the tensor-core
+# row-DFT kernel for uint16 frames, else the TMA-fed persistent kernel
+# wherever they apply), 1 generic shared-memory kernel, 2 register kernel,
+# 3 TMA-fed kernel, 4 tensor-core row DFT (uint16 frames only); inverse 0
+# automatic (one warp per unit for 16/32-pixel low-resolution fields), 1 one
+# block per unit
+KERNELS = [(0, 0), (1, 1), (2, 0), (0, 1), (3, 0)]
 
 
 def _run(lib, hol, cfg, keep32=False, kernel=(0, 0), overlap=0):
@@ -72,9 +74,11 @@ def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, kernel):
     hol = make_case(workload, frames)
     cfg = config_for(hol, mode)
     g = _run(lib, hol, cfg, keep32=True, kernel=kernel)
-    # every workload here fits the TMA-fed forward kernel, and in mode 1 the
-    # warp-per-unit inverse kernel; otherwise the kernels asked for run
-    assert g["kernel"][0] == (3 if kernel[0] == 0 else kernel[0])
+    # every workload here fits the TMA-fed forward kernel (the uint16 ones the
+    # tensor-core kernel), and in mode 1 the warp-per-unit inverse kernel;
+    # otherwise the kernels asked for run
+    auto = 4 if hol.frames.dtype == np.uint16 else 3
+    assert g["kernel"][0] == (auto if kernel[0] == 0 else kernel[0])
     assert g["kernel"][1] == ((2 if mode == 1 else 3) if kernel[1] == 0 else 1)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert g["R"].shape == o["R"].shape
