@@ -27,6 +27,7 @@
 
 #include "dh_common.cuh"
 #include "dh_grad.h"
+#include "dh_host.h"
 
 using namespace dh;
 
@@ -157,7 +158,7 @@ cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const floa
 cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s) {
     const size_t smem = sizeof(float2) * ((size_t)p.M + 2 * (size_t)p.G * p.ny) + sizeof(float) * ((size_t)p.G * (p.nx + p.ny) + 8 * 7);
     if (smem > 200 * 1024) return cudaErrorNotSupported;
-    cudaError_t e = cudaFuncSetAttribute(k_align_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_align_grad), (int)smem);
     if (e != cudaSuccess) return e;
     k_align_grad<<<(unsigned)(p.frameCount * p.polCount), 256, smem, s>>>(p);
     return cudaGetLastError();

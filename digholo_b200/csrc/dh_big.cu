@@ -31,6 +31,7 @@
 
 #include "dh_common.cuh"
 #include "dh_fft.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 #include "dh_tc.cuh"
 
@@ -571,7 +572,7 @@ cudaError_t planBig(const DhInvParams& p, int overlapKind, BigPlan& pl) {
 template <int PASS, int GN>
 cudaError_t launchBand(const DhInvParams& p, const BigArgs& a, size_t smem, unsigned blocks, cudaStream_t s) {
     auto kern = k_field_big<PASS, GN>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(kern), (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, NT, smem, s>>>(p, a);
     return cudaGetLastError();

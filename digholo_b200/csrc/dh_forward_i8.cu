@@ -11,7 +11,8 @@
 // fixed point v = d0 2^16 + d1 2^8 + d2 (unsigned bytes d0 <= 128).  The
 // frame rows go from HBM into shared memory by TMA exactly as stored (their
 // bytes are the u8 A operand, K = 2W bytes per row), and four
-// tcgen05.mma.kind::i8 products accumulate in tensor memory (int32):
+// tcgen05.mma.kind::i8 products accumulate in tensor memory (int32), the
+// four accumulators side by side as one wide MMA per K step:
 //
 //   D_0 = sum hi d0,   D_1 = sum lo d0 + hi d1,   D_2 = sum lo d1 + hi d2,
 //   D_3 = sum lo d2,   T = D_0 2^24 + D_1 2^16 + D_2 2^8 + D_3 = sum f v,
@@ -26,8 +27,11 @@
 // inverse pixel sinc, beam-centre phase and batch calibration.
 //
 // Persistent, warp-specialised, one block per SM: warp 0 issues the TMA
-// loads (NA stages), warp 1 the MMAs (two tensor-memory accumulator sets
-// when they fit), warps 2-9 read the accumulators and run the column stage.
+// loads (NA stages), warp 1 the MMAs into (up to) two tensor-memory
+// accumulator sets, and NG groups of four epilogue warps take the units in turn (each
+// group reads its unit's accumulators, frees them, and runs the column stage
+// in its own buffer under its own named barrier), so NG units are in the
+// epilogue at once.
 // Each block serves one polarisation.  Every wait is bounded; on expiry the
 // kernel records the failure in p.status and leaves after its copies land.
 #include <cuda.h>
@@ -39,6 +43,7 @@
 #include <mutex>
 
 #include "dh_common.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 #include "dh_tc.cuh"
 #include "dh_twiddle128.h"
@@ -47,8 +52,6 @@ using namespace dh;
 
 namespace {
 
-constexpr int NTHREADS = 320;   // 10 warps
-constexpr int NEPI = 256;       // epilogue threads (warps 2-9)
 constexpr int MROWS = 128;      // FFT-window rows (M of the MMA)
 
 template <int LOG>
@@ -125,7 +128,21 @@ __device__ __forceinline__ void tmemLd1(uint32_t taddr, uint32_t& r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
 }
 __device__ __forceinline__ void tmemWaitLd() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void epiSync() { asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory"); }
+
+// Named barrier over one epilogue group (128 threads) that also returns
+// whether any thread of the group passed true.
+__device__ __forceinline__ bool groupSyncOr(unsigned id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
 
 __device__ __forceinline__ void flagFail(const DhFwdParams& p, volatile int* abortFlag) {
     *abortFlag = 1;
@@ -138,11 +155,14 @@ __device__ __forceinline__ void flagFail(const DhFwdParams& p, volatile int* abo
 }  // namespace
 
 // W: FFT-window width (K = 2W bytes per row), HW: IFFT window (h = w),
-// NPAD: accumulator columns (2 w + ones column, rounded up to 16), NB:
-// accumulator sets in tensor memory, NA: TMA stages.  H = 128 rows.
-template <int W, int HW, int NPAD, int NB, int NA>
-__global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constant__ CUtensorMap tmap, DhFwdParams p) {
+// NPAD: accumulator columns (2 w + ones column, rounded up to 8), NA: TMA
+// stages, NG: epilogue groups of four warps.  H = 128 rows; two
+// tensor-memory accumulator sets where they fit (w = 16), else one.
+template <int W, int HW, int NPAD, int NA, int NG>
+__global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_constant__ CUtensorMap tmap, DhFwdParams p) {
     constexpr int H = MROWS;
+    constexpr int NT = 64 + 128 * NG;
+    constexpr int NB = 8 * NPAD <= 512 ? 2 : 1;   // accumulator sets
     constexpr int KB = 2 * W;                     // bytes per row
     constexpr int NATOM = KB / 128;               // 128-byte K atoms
     constexpr unsigned ABYTES = (unsigned)H * KB; // one stage
@@ -151,24 +171,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
     constexpr int Q = H / HW;
     constexpr int CLD = w + 1;
     constexpr int LOGHW = ilog2I(HW);
-    constexpr uint32_t IDESC = instrDescI8(128, NPAD);
-    constexpr int TMEMCOLS = (4 * NPAD * NB) <= 256 ? 256 : 512;
+    constexpr int NPART = 4 * NPAD <= 256 ? 1 : 2;  // MMAs per K step
+    constexpr int NMMA = 4 * NPAD / NPART;          // their N
+    static_assert(NMMA % 16 == 0 && NMMA <= 256, "MMA N must be a multiple of 16 up to 256 (M = 128)");
+    constexpr uint32_t IDESC = instrDescI8(128, NMMA);
+    constexpr int TMEMCOLS = 512;
+    static_assert(4 * NPAD * NB <= TMEMCOLS, "accumulator sets exceed tensor memory");
 
     extern __shared__ unsigned char smRaw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smRaw) + 1023) & ~static_cast<uintptr_t>(1023));
     unsigned char* aBuf = base;                                   // [NA][NATOM][128 rows][128 B]
-    unsigned char* bBuf = aBuf + (size_t)NA * ABYTES;             // [4][NATOM][NPAD][128 B]
-    float2* colbuf = reinterpret_cast<float2*>(bBuf + 4 * BQ);    // [H][w + 1]
-    float2* exch = colbuf + (size_t)H * CLD;                      // [HW][Q][w]
-    float2* tCol = exch + (size_t)H * w;                          // [h][Q] (this polarisation)
+    unsigned char* bBuf = aBuf + (size_t)NA * ABYTES;             // [NATOM][4 NPAD][128 B]
+    float2* colAll = reinterpret_cast<float2*>(bBuf + 4 * BQ);    // [NG][H][w + 1]
+    float2* tCol = colAll + (size_t)NG * H * CLD;                 // [h][Q] (this polarisation)
     float2* tAdj = tCol + (size_t)h * Q;                          // [h][w]
     uint64_t* bars = reinterpret_cast<uint64_t*>(tAdj + (size_t)h * w);
     uint64_t* full = bars;                // [NA]
     uint64_t* empty = bars + NA;          // [NA]
-    uint64_t* accFull = bars + 2 * NA;    // [NB]
-    uint64_t* accEmpty = accFull + NB;    // [NB]
-    uint64_t* bLoad = accEmpty + NB;      // the operand table
+    uint64_t* accFull = bars + 2 * NA;    // [NG] one per epilogue group
+    uint64_t* accEmpty = accFull + NG;    // [NG]
+    uint64_t* bLoad = accEmpty + NG;      // the operand table
     uint64_t* drain = bLoad + 1;          // final MMA commit
     uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abortFlag = reinterpret_cast<volatile int*>(tmemSlot + 1);
@@ -180,11 +203,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
     const int frame0 = blockIdx.x / P;
     const int nIt = frame0 < p.frameCount ? (p.frameCount - frame0 + frameStep - 1) / frameStep : 0;
 
-    for (int e = tid; e < h * Q; e += NTHREADS) tCol[e] = p.tabCol[(size_t)pol * h * Q + e];
-    for (int e = tid; e < h * w; e += NTHREADS) tAdj[e] = p.tabAdj[(size_t)pol * h * w + e];
+    for (int e = tid; e < h * Q; e += NT) tCol[e] = p.tabCol[(size_t)pol * h * Q + e];
+    for (int e = tid; e < h * w; e += NT) tAdj[e] = p.tabAdj[(size_t)pol * h * w + e];
     if (tid == 0) {
         for (int s = 0; s < NA; s++) { mbarInitN(&full[s], 1); mbarInitN(&empty[s], 1); }
-        for (int b = 0; b < NB; b++) { mbarInitN(&accFull[b], 1); mbarInitN(&accEmpty[b], 1); }
+        for (int g = 0; g < NG; g++) { mbarInitN(&accFull[g], 1); mbarInitN(&accEmpty[g], 1); }
         mbarInitN(bLoad, 1);
         mbarInitN(drain, 1);
         *abortFlag = 0;
@@ -208,7 +231,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
             const unsigned char* tab = p.dftDigits + (size_t)pol * 4 * BQ;
             tc::fenceProxyAsync();
             tc::mbarExpectTxTc(bLoad, 4 * BQ);
-            for (int q = 0; q < 4; q++) tc::bulkLoad(bBuf + q * BQ, tab + q * BQ, BQ, bLoad);
+            tc::bulkLoad(bBuf, tab, 4 * BQ, bLoad);
             int issued = 0;
             for (int it = 0; it < nIt; it++) {
                 const int s = it % NA;
@@ -231,14 +254,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
                 tc::mbarWaitTc(&full[it % NA], (unsigned)((it / NA) & 1));
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer
+        // ---------------- MMA issuer: unit it -> accumulator set it % 2, group it % NG
         if (lane == 0) {
             bool ok = tc::mbarWaitTc(bLoad, 0);
             if (!ok) flagFail(p, abortFlag);
             for (int it = 0; ok && it < nIt; it++) {
-                const int s = it % NA, b = it % NB;
+                const int s = it % NA, b = it % NB, g = it % NG;
                 if (!tc::mbarWaitTc(&full[s], (unsigned)((it / NA) & 1))) { flagFail(p, abortFlag); break; }
-                if (it >= NB && !tc::mbarWaitTc(&accEmpty[b], (unsigned)(((it / NB) - 1) & 1))) {
+                // the set was last read for unit it - 2, by group (it - 2) % NG
+                if (it >= NB && !tc::mbarWaitTc(&accEmpty[(it - NB) % NG], (unsigned)(((it - NB) / NG) & 1))) {
                     flagFail(p, abortFlag);
                     break;
                 }
@@ -246,83 +270,97 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
                 tc::fenceAfterSync();
                 const uint32_t aS = tc::sAddr(aBuf + (size_t)s * ABYTES);
                 const uint32_t bS = tc::sAddr(bBuf);
+                // the four accumulators side by side: one MMA of N = 4 NPAD per
+                // K step (two of 2 NPAD where 4 NPAD exceeds 256)
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    const uint32_t d = tmem + (uint32_t)(b * 4 * NPAD + q * NPAD);
+                for (int part = 0; part < NPART; part++) {
+                    const uint32_t d = tmem + (uint32_t)(b * 4 * NPAD + part * NMMA);
 #pragma unroll
                     for (int a = 0; a < NATOM; a++) {
 #pragma unroll
                         for (int ks = 0; ks < 4; ks++) {
                             const uint32_t ao = (uint32_t)a * H * 128 + (uint32_t)ks * 32;
-                            const uint32_t bo = (uint32_t)(q * BQ + a * NPAD * 128 + ks * 32);
+                            const uint32_t bo = (uint32_t)(a * 4 * NPAD * 128 + part * NMMA * 128 + ks * 32);
                             mmaI8(d, tc::smemDesc(aS + ao), tc::smemDesc(bS + bo), IDESC, (a > 0 || ks > 0) ? 1u : 0u);
                         }
                     }
                 }
                 tc::mmaCommit(&empty[s]);
-                tc::mmaCommit(&accFull[b]);
+                tc::mmaCommit(&accFull[g]);
             }
             // every MMA issued here completes before the accumulators are freed
             tc::mmaCommit(drain);
             tc::mbarWaitTc(drain, 0);
         }
     } else {
-        // ---------------- accumulator readback, column stage, output
-        const int et = tid - 64;                 // 0 .. 255
+        // ---------------- epilogue group g: units it = g, g + NG, ...
+        const int g = (warp - 2) >> 2;
+        const int gt = tid - 64 - 128 * g;       // 0 .. 127
         const int quarter = warp & 3;            // tensor-memory lanes 32 quarter .. + 31
-        const int grp = (warp - 2) >> 2;         // 0: real columns, 1: imaginary columns
         const int r = 32 * quarter + lane;       // FFT-window row
-        for (int it = 0; it < nIt; it++) {
+        const unsigned barId = 1 + g;
+        float2* colbuf = colAll + (size_t)g * H * CLD;
+        int k = 0;
+        for (int it = g; it < nIt; it += NG, k++) {
             const int b = it % NB;
             const int frame = frame0 + it * frameStep;
-            const bool okAcc = tc::mbarWaitTc(&accFull[b], (unsigned)((it / NB) & 1));
-            if (!okAcc) flagFail(p, abortFlag);
-            // all epilogue threads agree before touching the accumulators
-            epiSync();
-            if (*abortFlag) break;
+            bool bad = !tc::mbarWaitTc(&accFull[g], (unsigned)(k & 1));
+            if (bad) flagFail(p, abortFlag);
+            // one decision for the whole group
+            if (groupSyncOr(barId, bad || *abortFlag)) break;
             tc::fenceAfterSync();
             {
+                // X = (D_0 4 - S) + D_1 2^-6 + D_2 2^-14 + D_3 2^-22: the first
+                // difference is exact (both below 2^24), then three roundings
                 const uint32_t rowAddr = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * 4 * NPAD);
-                uint32_t dv[4][HW], sv[4];
+                float xr[2 * HW];
+                uint32_t s2, s3;
+                tmemLd1(rowAddr + (uint32_t)(2 * NPAD + 2 * w), s2);
+                tmemLd1(rowAddr + (uint32_t)(3 * NPAD + 2 * w), s3);
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int c0 = 0; c0 < 2 * HW; c0 += 16) {
+                    uint32_t t16[16];
+                    tmemLdX<16>(rowAddr + (uint32_t)c0, t16);
+                    tmemWaitLd();
 #pragma unroll
-                    for (int c0 = 0; c0 < HW; c0 += 16) {
+                    for (int i = 0; i < 16; i++) xr[c0 + i] = 4.0f * (float)(int)t16[i];
+                }
+                const float S = (float)((int)s2 * 256 + (int)s3);
+#pragma unroll
+                for (int i = 0; i < 2 * HW; i++) xr[i] -= S;
+                const float scl[3] = {1.0f / 64.0f, 1.0f / 16384.0f, 1.0f / 4194304.0f};
+#pragma unroll
+                for (int q = 1; q < 4; q++) {
+#pragma unroll
+                    for (int c0 = 0; c0 < 2 * HW; c0 += 16) {
                         uint32_t t16[16];
-                        tmemLdX<16>(rowAddr + (uint32_t)(q * NPAD + grp * w + c0), t16);
+                        tmemLdX<16>(rowAddr + (uint32_t)(q * NPAD + c0), t16);
+                        tmemWaitLd();
 #pragma unroll
-                        for (int i = 0; i < 16; i++) dv[q][c0 + i] = t16[i];
+                        for (int i = 0; i < 16; i++) xr[c0 + i] = fmaf((float)(int)t16[i], scl[q - 1], xr[c0 + i]);
                     }
-                    tmemLd1(rowAddr + (uint32_t)(q * NPAD + 2 * w), sv[q]);
                 }
-                tmemWaitLd();
                 tc::fenceBeforeSync();
-                epiSync();
-                if (et == 0) mbarArrive(&accEmpty[b]);
-                const long long S = ((long long)(int)sv[0] << 24) + ((long long)(int)sv[1] << 16) +
-                                    ((long long)(int)sv[2] << 8) + (long long)(int)sv[3];
-                const long long S22 = S << 22;
-                float* cr = reinterpret_cast<float*>(colbuf + (size_t)r * CLD) + grp;
+                asm volatile("bar.sync %0, 128;" ::"r"(barId) : "memory");
+                if (gt == 0) mbarArrive(&accEmpty[g]);
+                float2* crow = colbuf + (size_t)r * CLD;
 #pragma unroll
-                for (int c = 0; c < HW; c++) {
-                    const long long T = ((long long)(int)dv[0][c] << 24) + ((long long)(int)dv[1][c] << 16) +
-                                        ((long long)(int)dv[2][c] << 8) + (long long)(int)dv[3][c];
-                    cr[2 * c] = __ll2float_rn(T - S22) * 2.384185791015625e-07f;   // 2^-22
-                }
+                for (int c = 0; c < HW; c++) crow[c] = make_float2(xr[c], xr[HW + c]);
             }
-            epiSync();
+            asm volatile("bar.sync %0, 128;" ::"r"(barId) : "memory");
 
-            // column transforms of the decimated sequences X[Q a + bq][c], a < HW
-            for (int e = et; e < w * Q; e += NEPI) {
+            // column transforms of the decimated sequences X[Q a + bq][c], a < HW,
+            // in place: the outputs of (c, bq) go to the rows Q brev(i) + bq it read
+            for (int e = gt; e < w * Q; e += 128) {
                 const int c = e % w, bq = e / w;
                 float2 v[HW];
 #pragma unroll
                 for (int a = 0; a < HW; a++) v[a] = colbuf[(size_t)(Q * a + bq) * CLD + c];
                 fftDIFi<HW>(v);
 #pragma unroll
-                for (int i = 0; i < HW; i++) exch[((size_t)brevI<LOGHW>(i) * Q + bq) * w + c] = v[i];
+                for (int i = 0; i < HW; i++) colbuf[(size_t)(Q * brevI<LOGHW>(i) + bq) * CLD + c] = v[i];
             }
-            epiSync();
+            asm volatile("bar.sync %0, 128;" ::"r"(barId) : "memory");
 
             // kept rows: Y = sum_b tCol[j][b] Z_b[row mod HW], then the window factors
             float2 bc = make_float2(1.0f, 0.0f);
@@ -330,17 +368,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
                 bc = p.batchCal[pol * p.batchCalCount + ((p.frameOffset + frame) % p.batchCalCount)];
             const int sy = p.sy[pol];
             float2* out = p.window + (size_t)(frame * P + pol) * h * w;
-            for (int e = et; e < h * w; e += NEPI) {
+            for (int e = gt; e < h * w; e += 128) {
                 const int j = e / w, c = e - j * w;
                 const int row = (j + sy + H / 2) & (H - 1);
-                const float2* zb = exch + (size_t)(row & (HW - 1)) * Q * w + c;
+                const float2* zb = colbuf + (size_t)(Q * (row & (HW - 1))) * CLD + c;
                 const float2* tcj = tCol + (size_t)j * Q;
                 float2 Y = zb[0];
-                for (int bq = 1; bq < Q; bq++) Y = cadd(Y, cmul(zb[(size_t)bq * w], tcj[bq]));
+#pragma unroll
+                for (int bq = 1; bq < Q; bq++) Y = cadd(Y, cmul(zb[(size_t)bq * CLD], tcj[bq]));
                 out[e] = cmul(cmul(Y, bc), tAdj[e]);
             }
-            // the next unit rewrites colbuf only after its first barrier, and
-            // exch only after its second: every thread is past this loop by then
+            // colbuf is rewritten for the group's next unit only after its
+            // first barrier there, which every thread reaches after this loop
         }
     }
 
@@ -354,52 +393,37 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_forward_i8(const __grid_constan
 
 namespace {
 
-PFN_cuTensorMapEncodeTiled_v12000 encodeFnI8() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    });
-    return fn;
-}
-
-template <int W, int HW, int NPAD, int NB, int NA>
+template <int W, int HW, int NPAD, int NA, int NG>
 size_t smemI8() {
     const int H = MROWS, Q = H / HW;
     return 1024 + (size_t)NA * H * 2 * W + (size_t)4 * (2 * W / 128) * NPAD * 128 +
-           sizeof(float2) * ((size_t)H * (HW + 1) + (size_t)H * HW + (size_t)HW * Q + (size_t)HW * HW) +
-           sizeof(uint64_t) * (2 * NA + 2 * NB + 2) + 16;
+           sizeof(float2) * ((size_t)NG * H * (HW + 1) + (size_t)HW * Q + (size_t)HW * HW) +
+           sizeof(uint64_t) * (2 * NA + 2 * NG + 2) + 16;
 }
 
-template <int W, int HW, int NPAD, int NB, int NA>
+template <int W, int HW, int NPAD, int NA, int NG>
 cudaError_t launchI8(const DhFwdParams& p, const CUtensorMap& map, cudaStream_t s) {
-    size_t smem = smemI8<W, HW, NPAD, NB, NA>();
+    size_t smem = smemI8<W, HW, NPAD, NA, NG>();
     if (smem > 227 * 1024) return cudaErrorNotSupported;
     // more than half an SM's shared memory: one block per SM, so one tensor-memory allocation per SM
     if (smem < 120 * 1024) smem = 120 * 1024;
-    auto kern = k_forward_i8<W, HW, NPAD, NB, NA>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = k_forward_i8<W, HW, NPAD, NA, NG>;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(kern), (int)smem);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = smCountCached();
     const int P = p.polCount;
     // one block per SM, each serving one polarisation; at most one block per unit
     int grid = sms < p.frameCount * P ? sms : p.frameCount * P;
     grid = (grid / P) * P;
     if (grid < P) grid = P;
-    kern<<<grid, NTHREADS, smem, s>>>(map, p);
+    kern<<<grid, 64 + 128 * NG, smem, s>>>(map, p);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-// Accumulator columns of the digit table: 2 w + 1 rounded up to 16.
-int dh_forward_i8_npad(int w) { return ((2 * w + 1) + 15) / 16 * 16; }
+// Accumulator columns of the digit table: 2 w + 1 rounded up to 8.
+int dh_forward_i8_npad(int w) { return ((2 * w + 1) + 7) / 8 * 8; }
 
 // Returns cudaErrorNotSupported when the shape, the alignment, the digit
 // table or the driver rules this kernel out (the caller then uses another
@@ -419,21 +443,14 @@ cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s) {
     const long long rowsPerFrame = p.frameStride / p.frameWidth;
     const long long totalRows = rowsPerFrame * p.frameCount;
     if (totalRows >= (1ll << 31)) return cudaErrorNotSupported;
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encodeFnI8();
-    if (!enc) return cudaErrorNotSupported;
     CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)p.frameWidth, (cuuint64_t)totalRows};
-    const cuuint64_t strides[1] = {(cuuint64_t)p.frameWidth * 2};
-    const cuuint32_t box[2] = {64, (cuuint32_t)H};
-    const cuuint32_t estr[2] = {1, 1};
-    CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(p.frames), dims, strides, box, estr,
-                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
-                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (cr != CUDA_SUCCESS) return cudaErrorNotSupported;
+    if (!frameTensorMap(map, p.frames, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, (unsigned long long)p.frameWidth,
+                        (unsigned long long)totalRows, 64, (unsigned)H))
+        return cudaErrorNotSupported;
     if (W == 128) {
-        if (p.w == 16) return launchI8<128, 16, 48, 2, 3>(p, map, s);
-        return launchI8<128, 32, 80, 1, 2>(p, map, s);
+        if (p.w == 16) return launchI8<128, 16, 40, 4, 3>(p, map, s);
+        return launchI8<128, 32, 72, 2, 2>(p, map, s);
     }
-    if (p.w == 16) return launchI8<64, 16, 48, 2, 4>(p, map, s);
-    return launchI8<64, 32, 80, 1, 4>(p, map, s);
+    if (p.w == 16) return launchI8<64, 16, 40, 4, 3>(p, map, s);
+    return launchI8<64, 32, 72, 4, 2>(p, map, s);
 }

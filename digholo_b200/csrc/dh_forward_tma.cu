@@ -30,6 +30,7 @@
 #include <mutex>
 
 #include "dh_common.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 #include "dh_twiddle128.h"
 
@@ -319,26 +320,6 @@ __global__ void __launch_bounds__(256, 2) k_forward_tma(const __grid_constant__ 
 
 namespace {
 
-PFN_cuTensorMapEncodeTiled_v12000 encodeFn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    });
-    return fn;
-}
-
-int smCount() {
-    int dev = 0, n = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n > 0 ? n : 1;
-}
-
 template <int N, int H, int HW, bool U16, int NBUF>
 cudaError_t launchTma(const DhFwdParams& p, const CUtensorMap& map, cudaStream_t s) {
     const int ES = U16 ? 2 : 4;
@@ -349,14 +330,16 @@ cudaError_t launchTma(const DhFwdParams& p, const CUtensorMap& map, cudaStream_t
                         NBUF * sizeof(uint64_t);
     if (smem > 227 * 1024) return cudaErrorNotSupported;
     auto kern = k_forward_tma<N, H, HW, U16, NBUF>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(kern), (int)smem);
     if (e != cudaSuccess) return e;
-    int perSM = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, 2 * H, smem);
-    if (e != cudaSuccess) return e;
+    static int perSM = 0;   // per instantiation; the shared memory and block size are fixed by it
+    if (perSM == 0) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, 2 * H, smem);
+        if (e != cudaSuccess) return e;
+    }
     if (perSM < 1) return cudaErrorNotSupported;
     const int units = p.frameCount * P;
-    const int grid = units < perSM * smCount() ? units : perSM * smCount();
+    const int grid = units < perSM * smCountCached() ? units : perSM * smCountCached();
     kern<<<grid, 2 * H, smem, s>>>(map, p);
     return cudaGetLastError();
 }
@@ -410,19 +393,10 @@ cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s) {
     const long long rowsPerFrame = p.frameStride / p.frameWidth;
     const long long totalRows = rowsPerFrame * p.frameCount;
     if (totalRows >= (1ll << 31)) return cudaErrorNotSupported;
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encodeFn();
-    if (!enc) return cudaErrorNotSupported;
-
     CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)p.frameWidth, (cuuint64_t)totalRows};
-    const cuuint64_t strides[1] = {(cuuint64_t)p.frameWidth * es};
-    const cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)H};
-    const cuuint32_t estr[2] = {1, 1};
-    CUresult cr = enc(&map, p.inputU16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                      const_cast<void*>(p.frames), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (cr != CUDA_SUCCESS) return cudaErrorNotSupported;
+    if (!frameTensorMap(map, p.frames, p.inputU16 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, es,
+                        (unsigned long long)p.frameWidth, (unsigned long long)totalRows, (unsigned)(128 / es), (unsigned)H))
+        return cudaErrorNotSupported;
 
     return dispatchTma(p, map, s);
-    return cudaErrorNotSupported;
 }

@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "dh_common.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 #include "dh_fft.cuh"
 #include "dh_tc.cuh"
@@ -418,7 +419,7 @@ cudaError_t launchField(const DhInvParams& p, cudaStream_t s) {
                         sizeof(StatF) * (NT / 32) + tail;
     if (smem > 227 * 1024) return cudaErrorNotSupported;
     auto kern = k_field_full<W, H, WW, OVL, GN>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(kern), (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)(p.frameCount * p.polCount), NT, smem, s>>>(p);
     return cudaGetLastError();
@@ -428,7 +429,7 @@ template <int GMAX>
 cudaError_t launchOverlapF32(const DhInvParams& p, int nx, int ny, cudaStream_t s) {
     const size_t smem = sizeof(float) * ((size_t)nx * GMAX + (size_t)p.maxMG * ny + 2 * (size_t)ny * (p.maxMG + 1));
     if (smem > 200 * 1024) return cudaErrorNotSupported;
-    cudaError_t e = cudaFuncSetAttribute(k_overlap_f32<GMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_overlap_f32<GMAX>), (int)smem);
     if (e != cudaSuccess) return e;
     k_overlap_f32<GMAX><<<(unsigned)(p.frameCount * p.polCount), 2 * ny, smem, s>>>(p, nx, ny);
     return cudaGetLastError();

@@ -1,0 +1,114 @@
+// Host-side launch helpers shared by the kernel launchers: cached
+// shared-memory attributes, SM counts and TMA tensor maps, so that a launch
+// costs one cudaLaunchKernel and no driver queries.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+
+namespace dh {
+
+inline std::mutex& hostCacheLock() {
+    static std::mutex m;
+    return m;
+}
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize, and the maximal shared
+// memory carveout) once per kernel, device and size (raised when a larger
+// size is asked for).
+inline cudaError_t setSmemOnce(const void* func, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::map<std::pair<const void*, int>, int> done;
+    std::lock_guard<std::mutex> g(hostCacheLock());
+    auto it = done.find({func, dev});
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    // every kernel of the pipeline asks for the same L1 / shared split, so
+    // consecutive launches need no reconfiguration of the SMs
+    e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) done[{func, dev}] = bytes;
+    return e;
+}
+
+// Multiprocessors of the current device.
+inline int smCountCached() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+    static std::map<int, int> counts;
+    std::lock_guard<std::mutex> g(hostCacheLock());
+    auto it = counts.find(dev);
+    if (it != counts.end()) return it->second;
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n < 1) n = 1;
+    counts[dev] = n;
+    return n;
+}
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+// 2-D tiled tensor map over a batch of frames ([rows][width] elements,
+// 128-byte swizzle, no L2 promotion), cached by its arguments: the batch
+// buffers a caller rotates through are encoded once each.
+inline bool frameTensorMap(CUtensorMap& out, const void* base, CUtensorMapDataType type, int elemBytes,
+                           unsigned long long width, unsigned long long rows, unsigned boxX, unsigned boxY) {
+    struct Key {
+        const void* base;
+        int type, es;
+        unsigned long long width, rows;
+        unsigned boxX, boxY;
+        bool operator<(const Key& o) const { return memcmp(this, &o, sizeof(Key)) < 0; }
+    };
+    static std::map<Key, CUtensorMap> cache;
+    Key k;
+    memset(&k, 0, sizeof(k));
+    k.base = base;
+    k.type = (int)type;
+    k.es = elemBytes;
+    k.width = width;
+    k.rows = rows;
+    k.boxX = boxX;
+    k.boxY = boxY;
+    {
+        std::lock_guard<std::mutex> g(hostCacheLock());
+        auto it = cache.find(k);
+        if (it != cache.end()) {
+            out = it->second;
+            return true;
+        }
+    }
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensorMapEncoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)width * elemBytes};
+    const cuuint32_t box[2] = {boxX, boxY};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult cr = enc(&out, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return false;
+    std::lock_guard<std::mutex> g(hostCacheLock());
+    if (cache.size() >= 64) cache.clear();
+    cache[k] = out;
+    return true;
+}
+
+}  // namespace dh

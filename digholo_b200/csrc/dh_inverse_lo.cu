@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #include "dh_common.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 #include "dh_twiddle128.h"
 
@@ -278,11 +279,11 @@ cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s) {
     const unsigned blocks = (unsigned)((units + UPB - 1) / UPB);
     cudaError_t e;
     if (L == 16) {
-        e = cudaFuncSetAttribute(k_inverse_lo<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_lo<16>), (int)smem);
         if (e != cudaSuccess) return e;
         k_inverse_lo<16><<<blocks, 32 * LO_WARPS, smem, s>>>(q);
     } else {
-        e = cudaFuncSetAttribute(k_inverse_lo<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_lo<32>), (int)smem);
         if (e != cudaSuccess) return e;
         k_inverse_lo<32><<<blocks, 32 * LO_WARPS, smem, s>>>(q);
     }

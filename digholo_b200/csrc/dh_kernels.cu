@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include "dh_common.cuh"
+#include "dh_host.h"
 #include "dh_params.h"
 
 using namespace dh;
@@ -471,7 +472,7 @@ size_t dh_forward_smem_bytes(int logW, int logH, int colChunk) {
 
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s) {
     const size_t smem = dh_forward_smem_bytes(p.logW, p.logH, p.colChunk);
-    cudaError_t e = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_forward), (int)smem);
     if (e != cudaSuccess) return e;
     const long long blocks = (long long)p.frameCount * p.polCount * (p.w / p.colChunk);
     k_forward<<<(unsigned)blocks, FWD_THREADS, smem, s>>>(p);
@@ -493,7 +494,7 @@ size_t dh_inverse_smem_bytes(const DhInvParams& p) {
 
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
     const size_t smem = dh_inverse_smem_bytes(p);
-    cudaError_t e = cudaFuncSetAttribute(k_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse), (int)smem);
     if (e != cudaSuccess) return e;
     // small (low-resolution) fields: one thread per pair of pixels, at least two warps
     int threads = INV_THREADS;

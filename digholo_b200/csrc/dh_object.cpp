@@ -392,8 +392,9 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
 // + 1) 2^22) and round((1 - sin(2 pi k x / W)) 2^22), v = d0 2^16 + d1 2^8 +
 // d2, and a ones column (v = 1).  Accumulator q pairs the low byte of pixel x
 // with digit q - 1 and the high byte with digit q (digits -1 and 3 are zero).
-// Layout [pol][q][atom][npad][128 B], 16-byte chunk c of row n at c ^ (n & 7)
-// (the K-major 128-byte-swizzled operand).  Empty when the kernel does not
+// Layout [pol][atom][4 npad][128 B] (row q npad + n: the four accumulators'
+// operands stacked along N), 16-byte chunk c of row n at c ^ (n & 7) (the
+// K-major 128-byte-swizzled operand; npad is a multiple of 8).  Empty when the kernel does not
 // apply to the geometry.
 static void dftDigits(const Object& o, std::vector<unsigned char>& out) {
     out.clear();
@@ -423,7 +424,7 @@ static void dftDigits(const Object& o, std::vector<unsigned char>& out) {
                         const int di = q - 1 + hi;
                         const unsigned char byte = (di >= 0 && di <= 2) ? d[di] : 0;
                         const int b = 2 * x + hi, a = b >> 7, bb = b & 127, ch = bb >> 4;
-                        const size_t off = (((size_t)p * 4 + q) * natom + a) * npad * 128 + (size_t)n * 128 +
+                        const size_t off = (((size_t)p * natom + a) * 4 * npad + (size_t)q * npad + n) * 128 +
                                            (size_t)((ch ^ (n & 7)) << 4) + (bb & 15);
                         out[off] = byte;
                     }
@@ -503,12 +504,18 @@ static int prepare(Object& o) {
     // the reference stores the default window size back into the config (digHolo.cpp:7283-7290)
     if (c.fftWindowSizeX <= 0) c.fftWindowSizeX = c.frameWidth / c.polCount;
     if (c.fftWindowSizeY <= 0) c.fftWindowSizeY = c.frameHeight;
-    // AutoAlign evaluations place the FFT and IFFT windows with the settings of
-    // the last evaluation that reran those stages (stage snapshots)
-    fftWindowGeometry(o.useSnaps ? o.fftSnap : c, o.polCount, o.geo);
-    ifftWindowGeometry(o.useSnaps ? o.ifftSnap : c, o.polCount, o.geo);
-    r = checkSupported(o);
-    if (r) return r;
+    // an unchanged configuration keeps its geometry, tables and buffers
+    const bool unchanged = !o.useSnaps && o.preparedValid && memcmp(&o.preparedCfg, &c, sizeof(Config)) == 0 &&
+                           o.preparedKeep32 == o.keepField32 && o.preparedU16 == o.framesU16 &&
+                           o.preparedBatchCal == o.batchCalVersion;
+    if (!unchanged) {
+        // AutoAlign evaluations place the FFT and IFFT windows with the settings of
+        // the last evaluation that reran those stages (stage snapshots)
+        fftWindowGeometry(o.useSnaps ? o.fftSnap : c, o.polCount, o.geo);
+        ifftWindowGeometry(o.useSnaps ? o.ifftSnap : c, o.polCount, o.geo);
+        r = checkSupported(o);
+        if (r) return r;
+    }
     const Geometry& g = o.geo;
     if (!o.framesOnDevice) {
         o.framesOnDevice = isDevicePointer(o.frames);
@@ -517,9 +524,7 @@ static int prepare(Object& o) {
         const uintptr_t a = reinterpret_cast<uintptr_t>(o.frames);
         if (a % 16) return fail(o, ERR_INVALIDARGUMENT, "device frame buffer must be 16-byte aligned");
     }
-    if (!o.useSnaps && o.preparedValid && memcmp(&o.preparedCfg, &c, sizeof(Config)) == 0 && o.preparedKeep32 == o.keepField32 &&
-        o.preparedU16 == o.framesU16 && o.preparedBatchCal == o.batchCalVersion)
-        return ERR_SUCCESS;
+    if (unchanged) return ERR_SUCCESS;
     o.preparedValid = 0;
     // Uploads go through one pinned staging buffer; its previous contents
     // must have left before it is rewritten (no stream-wide synchronisation).
