@@ -56,6 +56,9 @@ def parse():
                     help="overlap of full-resolution fields: split-BF16 tensor cores or FP32 CUDA cores")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autoalign", action="store_true", help="skip the AutoAlign (plain vs adjoint) measurement")
+    ap.add_argument("--inverse-kernel", type=int, default=0,
+                    help="digHoloB200SetInverseKernel choice (0 automatic; 3 forward and inverse fused into "
+                         "one launch where they can be)")
     ap.add_argument("--no-largefield", action="store_true",
                     help="skip the large-field measurement (2048x2048 frames, 512x512 fields, 465 modes)")
     return ap.parse_args()
@@ -344,6 +347,7 @@ def main():
     L.digHoloB200SetStream(h, C.c_void_p(stream.cuda_stream))
     L.digHoloB200SetTiming(h, 1)
     L.digHoloB200SetOverlapKernel(h, 0 if args.overlap == "tc" else 1)
+    L.digHoloB200SetInverseKernel(h, args.inverse_kernel)
 
     def step_device(i):
         t = batches[i % 4]

@@ -84,7 +84,13 @@ def read_outputs(L, h, B, coef_ptr=None, m=0, pc=0, want_fields=True):
         stats = np.ctypeslib.as_array(params, shape=(pcount.value * pcn.value * tcount.value,)).copy()
         out["summary"] = stats.reshape(pcount.value, pcn.value, tcount.value)
         out["scale"] = out["summary"][3, :, :B]
-        out["batch_intensity"] = np.ctypeslib.as_array(ti, shape=(pcn.value * px.value * py.value,)).copy()
+        # per polarisation the plane occupies the first nx ny of W H floats (the
+        # reference sizes every batch-sum plane by the FFT window)
+        W = L.digHoloConfigGetfftWindowSizeX(h)
+        Hh = L.digHoloConfigGetfftWindowSizeY(h)
+        stride = max(W * Hh, px.value * py.value)
+        tot = np.ctypeslib.as_array(ti, shape=(pcn.value * stride,)).copy().reshape(pcn.value, stride)
+        out["batch_intensity"] = tot[:, :px.value * py.value].reshape(pcn.value, py.value, px.value)
     return out
 
 
@@ -97,3 +103,38 @@ def run_batch(L, h, frames, want_fields=True):
     b, m, pc = C.c_int(), C.c_int(), C.c_int()
     cp = L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(pc))
     return read_outputs(L, h, frames.shape[0], cp, m.value, pc.value, want_fields)
+
+
+def read_fourier(L, h):
+    """digHoloGetFourierPlaneFull and the plane-0 (Fourier plane) summary of
+    digHoloBatchGetSummary.  The plane is returned as (batch, pol, H, W/2+1);
+    the getter reports the FFT window width W as its width, as the reference
+    does (digHolo.cpp:4362-4380).  The batch-sum intensity has a stride of
+    W H floats per polarisation, of which the first (W/2+1) H are the plane's."""
+    b, p, w, hh = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    fp = L.digHoloGetFourierPlaneFull(h, C.byref(b), C.byref(p), C.byref(w), C.byref(hh))
+    out = {}
+    if fp and w.value > 0:
+        nxr = w.value // 2 + 1
+        n = b.value * p.value * hh.value * nxr
+        out["plane"] = np.ctypeslib.as_array(fp, shape=(2 * n,)).copy().view(np.complex64).reshape(
+            b.value, p.value, hh.value, nxr)
+        out["width"] = w.value
+    pcount, tcount, pcn = C.c_int(), C.c_int(), C.c_int()
+    params = C.POINTER(C.c_float)()
+    px, py = C.c_int(), C.c_int()
+    xa, ya, ti = C.POINTER(C.c_float)(), C.POINTER(C.c_float)(), C.POINTER(C.c_float)()
+    rc = L.digHoloBatchGetSummary(h, 0, C.byref(pcount), C.byref(tcount), C.byref(pcn), C.byref(params),
+                                  C.byref(px), C.byref(py), C.byref(xa), C.byref(ya), C.byref(ti))
+    out["summary_rc"] = rc
+    if rc == 0:
+        stats = np.ctypeslib.as_array(params, shape=(pcount.value * pcn.value * tcount.value,)).copy()
+        out["summary"] = stats.reshape(pcount.value, pcn.value, tcount.value)
+        out["px"], out["py"] = px.value, py.value
+        W = 2 * (px.value - 1)
+        stride = W * py.value
+        tot = np.ctypeslib.as_array(ti, shape=(pcn.value * stride,)).copy().reshape(pcn.value, stride)
+        out["batchsum"] = tot[:, :px.value * py.value].reshape(pcn.value, py.value, px.value)
+        out["kx"] = np.ctypeslib.as_array(xa, shape=(W,)).copy()
+        out["ky"] = np.ctypeslib.as_array(ya, shape=(py.value,)).copy()
+    return out

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <thread>
@@ -409,6 +410,52 @@ complex64* digHoloProcessBatch(int h, int* batchCount, int* modeCount, int* polC
     }
     return (complex64*)o->hCoefs.ptr;
 }
+// digHolo.h:1776 / digHolo.cpp (digHoloBenchmark).  Runs digHoloProcessBatch
+// on the current batch for about goalDuration seconds (at least three
+// batches after one untimed batch) and returns batches per second (host
+// clock around the calls, coefficients copied to the host each time, as the
+// reference's batch call does).  info (optional, 6 floats,
+// DIGHOLO_BENCHMARK_*): FFT, IFFT, APPLYTILT and OVERLAP rates are the
+// batches per second of this build's forward and inverse kernels (device
+// time; the IFFT, tilt removal and overlap are one stage here), BASIS the
+// rate of a full HG basis computation, TOTAL the frames per second.
+float digHoloBenchmark(int h, float goalDuration, float* info) {
+    OBJ_OR(h, 0.f);
+    if (dh::objProcessBatch(*o, 1) != dh::ERR_SUCCESS) return 0.f;
+    const int saveTiming = o->timing;
+    o->timing = 1;
+    float st[3];
+    dh::objStageTimes(*o, st);
+    int calls = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    double el = 0.0;
+    do {
+        if (dh::objProcessBatch(*o, 1) != dh::ERR_SUCCESS) { o->timing = saveTiming; return 0.f; }
+        calls++;
+        el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } while (calls < 3 || el < goalDuration);
+    dh::objStageTimes(*o, st);
+    o->timing = saveTiming;
+    const float rate = (float)(calls / el);
+    if (info) {
+        const float n = st[2] > 0 ? st[2] : 1.f;
+        const float fwd = st[0] > 0 ? 1e3f * n / st[0] : 0.f;
+        const float inv = st[1] > 0 ? 1e3f * n / st[1] : fwd;
+        info[0] = fwd;
+        info[1] = inv;
+        info[2] = inv;
+        info[4] = inv;
+        info[5] = rate * (float)o->batchCount;
+        // the basis: one recomputation for the current waists, timed on the host
+        const auto b0 = std::chrono::steady_clock::now();
+        o->basisNx = -1;   // force the recomputation
+        const int rb = dh::objUpdateBasis(*o);
+        const double bt = std::chrono::duration<double>(std::chrono::steady_clock::now() - b0).count();
+        info[3] = (rb == dh::ERR_SUCCESS && bt > 0) ? (float)(1.0 / bt) : 0.f;
+    }
+    return rate;
+}
+
 // digHolo.h:1670-1706 / digHolo.cpp:15146-15200
 int digHoloProcessFFT(int h) { OBJ_OR(h, dh::ERR_INVALIDHANDLE); return dh::objFFT(*o); }
 int digHoloProcessIFFT(int h) { OBJ_OR(h, dh::ERR_INVALIDHANDLE); return dh::objIFFT(*o); }
@@ -472,14 +519,29 @@ int digHoloGetFields16(int h, int* batchCount, int* polCount, short** fieldR, sh
     return dh::ERR_SUCCESS;
 }
 
-// digHolo.h:1659 / digHolo.cpp:4767-4805.  Plane 1 (reconstructed field) is
-// computed on this path; plane 0 (Fourier plane of the camera) needs the full
-// R2C plane, which the pruned forward transform does not form.
+// digHolo.h:1659 / digHolo.cpp:4767-4805.  Plane 1 (reconstructed field)
+// comes from the batch path; plane 0 (the Fourier plane of the camera) is
+// computed from the batch's frames on the first request (the full R2C plane
+// and its analysis, digHolo.cpp:6931-6980).  The batch-sum intensities have
+// W H floats per polarisation (FFT window size), as in the reference.
 int digHoloBatchGetSummary(int h, int planeIdx, int* parameterCount, int* totalCount, int* polCount, float** parameters,
                            int* pixelCountX, int* pixelCountY, float** xAxis, float** yAxis, float** totalIntensity) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     if (planeIdx < 0 || planeIdx > 1) return dh::ERR_INVALIDDIMENSION;
-    if (!o->processedTilt || planeIdx == 0) return dh::ERR_NULLPOINTER;
+    if (!o->processedTilt) return dh::ERR_NULLPOINTER;
+    if (planeIdx == 0) {
+        if (dh::objFourierToHost(*o, 0) != dh::ERR_SUCCESS) return dh::ERR_ERROR;
+        *parameterCount = dh::ANALYSIS_COUNT;
+        *totalCount = o->lastFwd.frameCount + 1;
+        *polCount = o->polCount;
+        *parameters = o->hFftStats.as<float>();
+        *pixelCountX = o->geo.W / 2 + 1;
+        *pixelCountY = o->geo.H;
+        *xAxis = o->hKx.data();
+        *yAxis = o->hKy.data();
+        *totalIntensity = o->hFftBatchSum.as<float>();
+        return dh::ERR_SUCCESS;
+    }
     if (dh::objStatsToHost(*o) != dh::ERR_SUCCESS) return dh::ERR_ERROR;
     o->hX = o->geo.x;
     o->hY = o->geo.y;
@@ -493,6 +555,24 @@ int digHoloBatchGetSummary(int h, int planeIdx, int* parameterCount, int* totalC
     *yAxis = o->hY.data();
     *totalIntensity = o->hBatchSum.as<float>();
     return dh::ERR_SUCCESS;
+}
+
+// digHolo.h:1718 / digHolo.cpp:4362-4380, 15554-15564.  The R2C planes
+// [batch][pol][H][W/2+1] of the last batch, computed from its frames on the
+// first request; as the reference does, *width reports the FFT window width
+// W (the rows hold W/2+1 values).  Null and zero sizes before any batch.
+complex64* digHoloGetFourierPlaneFull(int h, int* batchCount, int* polCount, int* width, int* height) {
+    Object* o = get(h);
+    if (!o) return nullptr;
+    if (!o->processedTilt || dh::objFourierToHost(*o, 1) != dh::ERR_SUCCESS) {
+        *batchCount = *polCount = *width = *height = 0;
+        return nullptr;
+    }
+    *batchCount = o->lastFwd.frameCount;
+    *polCount = o->polCount;
+    *width = o->geo.W;
+    *height = o->geo.H;
+    return (complex64*)o->hFourier.ptr;
 }
 
 // digHolo.h:1732 / digHolo.cpp:4370-4390.  The window is returned in the
@@ -628,12 +708,13 @@ int digHoloB200SetForwardKernel(int h, int kernel) {
 }
 int digHoloB200SetInverseKernel(int h, int kernel) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    if (kernel < 0 || kernel > 2) return dh::ERR_INVALIDARGUMENT;
+    if (kernel < 0 || kernel > 3) return dh::ERR_INVALIDARGUMENT;
     o->inverseKernel = kernel;
     return dh::ERR_SUCCESS;
 }
 // Inverse kernel used by the last batch: 1 block per unit, 2 warp per unit,
-// 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands.
+// 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands,
+// 5 fused into the tensor-core forward kernel.
 int digHoloB200GetInverseKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastInverseKernel;

@@ -40,6 +40,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <cstring>
 #include <mutex>
 
 #include "dh_common.cuh"
@@ -85,6 +86,56 @@ __device__ __forceinline__ void fftDIFi(float2 (&v)[N]) {
                 }
             }
         }
+    }
+}
+
+// In-place radix-2 DIF inverse FFT (exp(+2 pi i / N), unnormalised) of N <= 64
+// values in registers: natural-order input, bit-reversed output.
+template <int N>
+__device__ __forceinline__ void ifftDIFi(float2 (&v)[N]) {
+#pragma unroll
+    for (int m = N / 2; m >= 1; m >>= 1) {
+#pragma unroll
+        for (int blk = 0; blk < N; blk += 2 * m) {
+#pragma unroll
+            for (int j = 0; j < m; j++) {
+                const float2 a = v[blk + j];
+                const float2 b = v[blk + j + m];
+                v[blk + j] = cadd(a, b);
+                const float2 d = csub(a, b);
+                if (j == 0) {
+                    v[blk + j + m] = d;
+                } else if (2 * j == m) {
+                    v[blk + j + m] = make_float2(-d.y, d.x);
+                } else {
+                    const float2 t = tw128(j * (128 / (2 * m)));
+                    v[blk + j + m] = cmul(d, make_float2(t.x, -t.y));
+                }
+            }
+        }
+    }
+}
+
+struct StatI {
+    float maxI;
+    int maxIdx;
+    float P, cx, cy, cyw, e4;
+};
+
+// Reduction over lanes 0 .. L-1 of one warp.
+template <int L>
+__device__ __forceinline__ void laneReduce(StatI& s) {
+    constexpr unsigned mask = L == 32 ? 0xffffffffu : ((1u << L) - 1u);
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) {
+        const float mI = __shfl_xor_sync(mask, s.maxI, off);
+        const int mIdx = __shfl_xor_sync(mask, s.maxIdx, off);
+        if (mI > s.maxI || (mI == s.maxI && mIdx > s.maxIdx)) { s.maxI = mI; s.maxIdx = mIdx; }
+        s.P += __shfl_xor_sync(mask, s.P, off);
+        s.cx += __shfl_xor_sync(mask, s.cx, off);
+        s.cy += __shfl_xor_sync(mask, s.cy, off);
+        s.cyw += __shfl_xor_sync(mask, s.cyw, off);
+        s.e4 += __shfl_xor_sync(mask, s.e4, off);
     }
 }
 
@@ -152,14 +203,197 @@ __device__ __forceinline__ void flagFail(const DhFwdParams& p, volatile int* abo
     }
 }
 
+__host__ __device__ constexpr int dh_forward_i8_npad_impl(int w) { return ((2 * w + 1) + 7) / 8 * 8; }
+
+__device__ __forceinline__ void groupBar(unsigned id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+// Inverse stage of one unit by its epilogue group (128 threads, named
+// barrier barId), for L x L low-resolution fields: the window rows and then
+// columns are inverse-transformed by L threads (the last L-point transforms
+// and the statistics stay inside one warp), the field is rounded to int16,
+// and the separable overlap U[x][n] = sum_y Hy[n][y] V[y][x], c_mn =
+// sum_x Hx[m][x] U[x][n] is spread over the group.  Same arithmetic, in the
+// same order, as k_inverse_lo.  work: at least L (3 L + 3 + G) complex.
+template <int L>
+__device__ __forceinline__ void fusedInverse(const DhInvParams& ip, int gt, unsigned barId, int frame, int pol,
+                                             const float2* winT, float2* work, float* sclSlot, const float* hxT,
+                                             const float* hyT, const float* axT, const int* refT, const float* hsT) {
+    constexpr int LOG = ilog2I(L);
+    constexpr int LD = L + 1;
+    const int P = ip.polCount, G = ip.maxMG, M = ip.modeCount;
+    const int ULD = (G + 1) | 1;
+    float2* t2 = work;               // [L][LD] row transforms
+    float2* Vt = work + L * LD;      // [L][LD] int16 field
+    float2* Ut = work + 2 * L * LD;  // [L][ULD]
+    const int unit = frame * P + pol;
+    groupBar(barId);   // the window tile is complete and the column buffer is free
+    if (gt < L) {
+        // row gt of the window, inverse FFT over kx
+        float2 v[L];
+#pragma unroll
+        for (int c = 0; c < L; c++) v[c] = winT[gt * LD + c];
+        ifftDIFi<L>(v);
+#pragma unroll
+        for (int i = 0; i < L; i++) t2[gt * LD + brevI<LOG>(i)] = v[i];
+    }
+    groupBar(barId);
+    if (gt < L) {
+        // column x = gt over ky: v[i] = F[y = brev(i)][x]
+        const int x = gt;
+        float2 v[L];
+#pragma unroll
+        for (int j = 0; j < L; j++) v[j] = t2[j * LD + x];
+        ifftDIFi<L>(v);
+        // statistics over the untilted field (digHolo.cpp:8866-8870)
+        const float inv = (float)(1.0 / ((double)L * (double)L));
+        const float* yax = axT + L;
+        const float yShift = fabsf((yax[1] - yax[0]) * (float)L);
+        const float xv = axT[x];
+        StatI st = {0.f, -1, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < L; i++) {
+            const int y = brevI<LOG>(i);
+            const float2 a = v[i];
+            const float I0 = fmaf(a.x, a.x, a.y * a.y);
+            const float I = I0 * inv;
+            const int idx = 2 * y * L + x;
+            if (I0 > st.maxI || (I0 == st.maxI && idx > st.maxIdx)) { st.maxI = I0; st.maxIdx = idx; }
+            const float yv = yax[y];
+            st.P += I;
+            st.cx = fmaf(xv, I, st.cx);
+            st.cy = fmaf(yv, I, st.cy);
+            st.cyw = fmaf(yv + (yv < 0.f ? yShift : 0.f), I, st.cyw);
+            st.e4 = fmaf(I, I, st.e4);
+        }
+        laneReduce<L>(st);
+        const float scale = (float)(32767.0 / (double)sqrtf(st.maxI));
+        if (x == 0) {
+            const int S = ip.statsStride;
+            float* sp = ip.stats;
+            const int col = pol * S + frame;
+            const int per = P * S;
+            sp[0 * per + col] = st.P;
+            sp[1 * per + col] = st.cx / st.P;
+            sp[2 * per + col] = st.cy / st.P;
+            sp[3 * per + col] = scale;
+            sp[4 * per + col] = __int_as_float(st.maxIdx);
+            sp[5 * per + col] = ip.dA * (st.P * st.P / st.e4);
+            sp[6 * per + col] = st.cyw / st.P;
+            *sclSlot = scale;
+        }
+        // reference wave, -conj(A . ref), int16 rounding (digHolo.cpp:2741-2833)
+        // the wave and the scales come from shared memory: no global load
+        // waits behind the field stores
+        const int* ref = refT + (size_t)pol * 4 * L;
+        const int xr = ref[x], xi = ref[L + x];
+        const float K = (float)(1.0 / (16383.0 * 16383.0));
+        const size_t fieldOff = (size_t)unit * L * L;
+#pragma unroll
+        for (int i = 0; i < L; i++) {
+            const int y = brevI<LOG>(i);
+            const int yr = ref[2 * L + y], yi = ref[3 * L + y];
+            const float adjR = (float)(yr * xr - yi * xi) * K;
+            const float adjI = (float)(yr * xi + yi * xr) * K;
+            const float2 a = v[i];
+            const float vr = __fsub_rn(__fmul_rn(a.y, adjI), __fmul_rn(a.x, adjR));
+            const float vi = __fadd_rn(__fmul_rn(a.x, adjI), __fmul_rn(a.y, adjR));
+            const size_t o = fieldOff + (size_t)y * L + x;
+            if (ip.field32) {
+                const float* rf = ip.refWaveF + (size_t)pol * 4 * L;
+                const float2 rx = make_float2(rf[x], rf[L + x]);
+                const float2 ry = make_float2(rf[2 * L + y], rf[3 * L + y]);
+                const float2 wv = cmul(a, cmul(ry, rx));
+                ip.field32[o] = make_float2(-wv.x, wv.y);
+            }
+            const short sr = roundSat16(scale * vr);
+            const short si = roundSat16(scale * vi);
+            ip.fieldR[o] = sr;
+            ip.fieldI[o] = si;
+            Vt[y * LD + x] = make_float2((float)sr, (float)si);
+        }
+    }
+    if (G <= 0 || !ip.coefs) return;
+    groupBar(barId);
+    // overlap on the int16 field (digHolo.cpp:2149-2341), contracted over y first
+    const float* hyp = hyT + (size_t)pol * G * LD;
+    const float* hxp = hxT + (size_t)pol * G * LD;
+    for (int e = gt; e < L * G; e += 128) {
+        const int x = e % L, n = e / L;
+        const float* hn = hyp + n * LD;
+        float ur = 0.f, ui = 0.f;
+#pragma unroll
+        for (int i = 0; i < L; i++) {
+            const int y = brevI<LOG>(i);
+            const float hv = hn[y];
+            const float2 vv = Vt[y * LD + x];
+            ur = fmaf(hv, vv.x, ur);
+            ui = fmaf(hv, vv.y, ui);
+        }
+        Ut[x * ULD + n] = make_float2(ur, ui);
+    }
+    groupBar(barId);
+    const float fieldScale = 1.0f / *sclSlot;
+    const float* sxp = hsT + pol * G;
+    const float* syp = hsT + P * G + pol * G;
+    float2* cout = ip.coefs + (size_t)frame * P * M + (size_t)pol * M;
+    for (int mode = gt; mode < M; mode += 128) {
+        int gg = (int)((sqrtf(8.0f * mode + 1.0f) - 1.0f) * 0.5f);
+        while ((gg + 1) * (gg + 2) / 2 <= mode) gg++;
+        while (gg * (gg + 1) / 2 > mode) gg--;
+        const int n = mode - gg * (gg + 1) / 2;
+        const int m = gg - n;
+        const float* hm = hxp + m * LD;
+        float cr = 0.f, ci = 0.f;
+#pragma unroll
+        for (int x = 0; x < L; x++) {
+            const float2 u = Ut[x * ULD + n];
+            cr = fmaf(hm[x], u.x, cr);
+            ci = fmaf(hm[x], u.y, ci);
+        }
+        const float ms = (float)((double)sxp[m] * (double)syp[n] * (double)fieldScale);
+        cout[mode] = make_float2(cr * ms, ci * ms);
+    }
+}
+
+// Shared-memory plan (byte offsets from the 1024-aligned base); the host
+// computes the same numbers.  FUSE adds, per epilogue group, the window
+// tile and, per block, the HG tables of the fused inverse stage.
+struct I8Smem {
+    size_t a, b, col, tcol, tadj, win, scl, hx, hy, ax, ref, hs, bars, total;
+};
+__host__ __device__ inline I8Smem i8Smem(int W, int HW, int NPAD, int NA, int NG, bool fuse, int P, int G) {
+    const int H = MROWS, Q = H / HW, CLD = HW + 1;
+    I8Smem s;
+    s.a = 0;
+    s.b = s.a + (size_t)NA * H * 2 * W;
+    s.col = s.b + (size_t)4 * (2 * W / 128) * NPAD * 128;
+    s.tcol = s.col + sizeof(float2) * (size_t)NG * H * CLD;
+    s.tadj = s.tcol + sizeof(float2) * (size_t)HW * Q;
+    s.win = s.tadj + sizeof(float2) * (size_t)HW * HW;
+    s.scl = s.win + (fuse ? sizeof(float2) * (size_t)NG * HW * CLD : 0);
+    s.hx = s.scl + (fuse ? sizeof(float2) * (size_t)NG : 0);
+    s.hy = s.hx + (fuse ? sizeof(float) * (size_t)P * G * CLD : 0);
+    s.ax = s.hy + (fuse ? sizeof(float) * (size_t)P * G * CLD : 0);
+    s.ref = s.ax + (fuse ? sizeof(float) * 2 * (size_t)HW : 0);
+    s.hs = s.ref + (fuse ? sizeof(int) * 4 * (size_t)P * HW : 0);
+    s.bars = (s.hs + (fuse ? sizeof(float) * 2 * (size_t)P * G : 0) + 7) & ~(size_t)7;
+    s.total = s.bars + sizeof(uint64_t) * (2 * NA + 2 * NG + 2) + 16;
+    return s;
+}
+
 }  // namespace
 
 // W: FFT-window width (K = 2W bytes per row), HW: IFFT window (h = w),
 // NPAD: accumulator columns (2 w + ones column, rounded up to 8), NA: TMA
 // stages, NG: epilogue groups of four warps.  H = 128 rows; two
 // tensor-memory accumulator sets where they fit (w = 16), else one.
-template <int W, int HW, int NPAD, int NA, int NG>
-__global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_constant__ CUtensorMap tmap, DhFwdParams p) {
+// FUSE: the inverse stage of 16 x 16 low-resolution fields runs in the
+// epilogue groups as well (window IFFT -> statistics -> reference wave,
+// -conj, int16 rounding -> HG overlap; digHolo.cpp:8734, 2354, 2701-2837,
+// 2149-2341), with ip its parameters.
+template <int W, int HW, int NPAD, int NA, int NG, bool FUSE>
+__global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_constant__ CUtensorMap tmap, DhFwdParams p,
+                                                                 DhInvParams ip) {
     constexpr int H = MROWS;
     constexpr int NT = 64 + 128 * NG;
     constexpr int NB = 8 * NPAD <= 512 ? 2 : 1;   // accumulator sets
@@ -181,12 +415,21 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
     extern __shared__ unsigned char smRaw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smRaw) + 1023) & ~static_cast<uintptr_t>(1023));
-    unsigned char* aBuf = base;                                   // [NA][NATOM][128 rows][128 B]
-    unsigned char* bBuf = aBuf + (size_t)NA * ABYTES;             // [NATOM][4 NPAD][128 B]
-    float2* colAll = reinterpret_cast<float2*>(bBuf + 4 * BQ);    // [NG][H][w + 1]
-    float2* tCol = colAll + (size_t)NG * H * CLD;                 // [h][Q] (this polarisation)
-    float2* tAdj = tCol + (size_t)h * Q;                          // [h][w]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(tAdj + (size_t)h * w);
+    const int GI = FUSE ? ip.maxMG : 0;
+    const I8Smem L8 = i8Smem(W, HW, NPAD, NA, NG, FUSE, p.polCount, GI);
+    unsigned char* aBuf = base + L8.a;                            // [NA][NATOM][128 rows][128 B]
+    unsigned char* bBuf = base + L8.b;                            // [NATOM][4 NPAD][128 B]
+    float2* colAll = reinterpret_cast<float2*>(base + L8.col);    // [NG][H][w + 1]
+    float2* tCol = reinterpret_cast<float2*>(base + L8.tcol);     // [h][Q] (this polarisation)
+    float2* tAdj = reinterpret_cast<float2*>(base + L8.tadj);     // [h][w]
+    float2* winAll = reinterpret_cast<float2*>(base + L8.win);    // FUSE: [NG][h][w + 1] the unit's window
+    float* sclAll = reinterpret_cast<float*>(base + L8.scl);      // FUSE: [NG] field scale
+    float* hxT = reinterpret_cast<float*>(base + L8.hx);          // FUSE: [P][G][w + 1] Hx
+    float* hyT = reinterpret_cast<float*>(base + L8.hy);          // FUSE: [P][G][h + 1] Hy
+    float* axT = reinterpret_cast<float*>(base + L8.ax);          // FUSE: x axis [w], y axis [h]
+    int* refT = reinterpret_cast<int*>(base + L8.ref);            // FUSE: [P][Xr Xi Yr Yi][16] 14-bit wave
+    float* hsT = reinterpret_cast<float*>(base + L8.hs);          // FUSE: [x, y][P][G] mode scales
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + L8.bars);
     uint64_t* full = bars;                // [NA]
     uint64_t* empty = bars + NA;          // [NA]
     uint64_t* accFull = bars + 2 * NA;    // [NG] one per epilogue group
@@ -205,6 +448,22 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
 
     for (int e = tid; e < h * Q; e += NT) tCol[e] = p.tabCol[(size_t)pol * h * Q + e];
     for (int e = tid; e < h * w; e += NT) tAdj[e] = p.tabAdj[(size_t)pol * h * w + e];
+    if (FUSE) {
+        for (int e = tid; e < P * GI * HW; e += NT) {
+            const int row = e / HW, x = e - row * HW;
+            hxT[row * CLD + x] = (float)ip.hgX[e];
+            hyT[row * CLD + x] = (float)ip.hgY[e];
+        }
+        for (int e = tid; e < HW; e += NT) {
+            axT[e] = ip.xAxis[e];
+            axT[HW + e] = ip.yAxis[e];
+        }
+        for (int e = tid; e < P * 4 * HW; e += NT) refT[e] = ip.refWave[e];
+        for (int e = tid; e < P * GI; e += NT) {
+            hsT[e] = ip.hgScaleX[e];
+            hsT[P * GI + e] = ip.hgScaleY[e];
+        }
+    }
     if (tid == 0) {
         for (int s = 0; s < NA; s++) { mbarInitN(&full[s], 1); mbarInitN(&empty[s], 1); }
         for (int g = 0; g < NG; g++) { mbarInitN(&accFull[g], 1); mbarInitN(&accEmpty[g], 1); }
@@ -376,8 +635,12 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
                 float2 Y = zb[0];
 #pragma unroll
                 for (int bq = 1; bq < Q; bq++) Y = cadd(Y, cmul(zb[(size_t)bq * CLD], tcj[bq]));
-                out[e] = cmul(cmul(Y, bc), tAdj[e]);
+                const float2 wv = cmul(cmul(Y, bc), tAdj[e]);
+                out[e] = wv;
+                if (FUSE) winAll[(size_t)g * HW * CLD + j * CLD + c] = wv;
             }
+            if (FUSE) fusedInverse<HW>(ip, gt, barId, frame, pol, winAll + (size_t)g * HW * CLD, colbuf, sclAll + g, hxT,
+                                       hyT, axT, refT, hsT);
             // colbuf is rewritten for the group's next unit only after its
             // first barrier there, which every thread reaches after this loop
         }
@@ -393,21 +656,13 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
 
 namespace {
 
-template <int W, int HW, int NPAD, int NA, int NG>
-size_t smemI8() {
-    const int H = MROWS, Q = H / HW;
-    return 1024 + (size_t)NA * H * 2 * W + (size_t)4 * (2 * W / 128) * NPAD * 128 +
-           sizeof(float2) * ((size_t)NG * H * (HW + 1) + (size_t)HW * Q + (size_t)HW * HW) +
-           sizeof(uint64_t) * (2 * NA + 2 * NG + 2) + 16;
-}
-
-template <int W, int HW, int NPAD, int NA, int NG>
-cudaError_t launchI8(const DhFwdParams& p, const CUtensorMap& map, cudaStream_t s) {
-    size_t smem = smemI8<W, HW, NPAD, NA, NG>();
+template <int W, int HW, int NPAD, int NA, int NG, bool FUSE>
+cudaError_t launchI8(const DhFwdParams& p, const DhInvParams& ip, const CUtensorMap& map, cudaStream_t s) {
+    size_t smem = 1024 + i8Smem(W, HW, NPAD, NA, NG, FUSE, p.polCount, FUSE ? ip.maxMG : 0).total;
     if (smem > 227 * 1024) return cudaErrorNotSupported;
     // more than half an SM's shared memory: one block per SM, so one tensor-memory allocation per SM
     if (smem < 120 * 1024) smem = 120 * 1024;
-    auto kern = k_forward_i8<W, HW, NPAD, NA, NG>;
+    auto kern = k_forward_i8<W, HW, NPAD, NA, NG, FUSE>;
     cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(kern), (int)smem);
     if (e != cudaSuccess) return e;
     const int sms = smCountCached();
@@ -416,25 +671,17 @@ cudaError_t launchI8(const DhFwdParams& p, const CUtensorMap& map, cudaStream_t 
     int grid = sms < p.frameCount * P ? sms : p.frameCount * P;
     grid = (grid / P) * P;
     if (grid < P) grid = P;
-    kern<<<grid, 64 + 128 * NG, smem, s>>>(map, p);
+    kern<<<grid, 64 + 128 * NG, smem, s>>>(map, p, ip);
     return cudaGetLastError();
 }
 
-}  // namespace
-
-// Accumulator columns of the digit table: 2 w + 1 rounded up to 8.
-int dh_forward_i8_npad(int w) { return ((2 * w + 1) + 7) / 8 * 8; }
-
-// Returns cudaErrorNotSupported when the shape, the alignment, the digit
-// table or the driver rules this kernel out (the caller then uses another
-// forward kernel).
-cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s) {
+// Common checks and the tensor map of the frames.
+cudaError_t prepareI8(const DhFwdParams& p, CUtensorMap& map) {
     const int W = 1 << p.logW, H = 1 << p.logH;
-    if (p.frameCount <= 0) return cudaSuccess;
     if (!p.inputU16 || !p.dftDigits || !p.tabCol || !p.tabAdj) return cudaErrorNotSupported;
     if (H != MROWS || p.h != p.w || (p.w != 16 && p.w != 32)) return cudaErrorNotSupported;
     if (W != 64 && W != 128) return cudaErrorNotSupported;
-    if (p.dftNpad != dh_forward_i8_npad(p.w)) return cudaErrorNotSupported;
+    if (p.dftNpad != dh_forward_i8_npad_impl(p.w)) return cudaErrorNotSupported;
     for (int q = 0; q < p.polCount; q++)
         if ((p.cx[q] * 2) % 16 != 0) return cudaErrorNotSupported;   // TMA x coordinate: 16-byte multiple
     if ((reinterpret_cast<uintptr_t>(p.frames) % 16) != 0 || ((size_t)p.frameWidth * 2) % 16 != 0) return cudaErrorNotSupported;
@@ -443,14 +690,51 @@ cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s) {
     const long long rowsPerFrame = p.frameStride / p.frameWidth;
     const long long totalRows = rowsPerFrame * p.frameCount;
     if (totalRows >= (1ll << 31)) return cudaErrorNotSupported;
-    CUtensorMap map;
     if (!frameTensorMap(map, p.frames, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, (unsigned long long)p.frameWidth,
                         (unsigned long long)totalRows, 64, (unsigned)H))
         return cudaErrorNotSupported;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+// Accumulator columns of the digit table: 2 w + 1 rounded up to 8.
+int dh_forward_i8_npad(int w) { return dh_forward_i8_npad_impl(w); }
+
+// Returns cudaErrorNotSupported when the shape, the alignment, the digit
+// table or the driver rules this kernel out (the caller then uses another
+// forward kernel).
+cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s) {
+    if (p.frameCount <= 0) return cudaSuccess;
+    CUtensorMap map;
+    cudaError_t e = prepareI8(p, map);
+    if (e != cudaSuccess) return e;
+    DhInvParams none;
+    memset(&none, 0, sizeof(none));
+    const int W = 1 << p.logW;
     if (W == 128) {
-        if (p.w == 16) return launchI8<128, 16, 40, 4, 3>(p, map, s);
-        return launchI8<128, 32, 72, 2, 2>(p, map, s);
+        if (p.w == 16) return launchI8<128, 16, 40, 4, 3, false>(p, none, map, s);
+        return launchI8<128, 32, 72, 2, 2, false>(p, none, map, s);
     }
-    if (p.w == 16) return launchI8<64, 16, 40, 4, 3>(p, map, s);
-    return launchI8<64, 32, 72, 4, 2>(p, map, s);
+    if (p.w == 16) return launchI8<64, 16, 40, 4, 3, false>(p, none, map, s);
+    return launchI8<64, 32, 72, 4, 2, false>(p, none, map, s);
+}
+
+// Forward and inverse stages in one launch (16 x 16 low-resolution fields,
+// maxMG <= 32): the frames' Fourier windows, int16 fields, statistics and
+// coefficients.  cudaErrorNotSupported outside those shapes.
+cudaError_t dh_launch_forward_i8_fused(const DhFwdParams& p, const DhInvParams& ip, cudaStream_t s) {
+    if (!ip.lowres || ip.logw != 4 || ip.logh != 4 || p.w != 16 || ip.polCount != p.polCount) return cudaErrorNotSupported;
+    if (ip.frameCount != p.frameCount || ip.maxMG > 32 || !ip.fieldR || !ip.fieldI || !ip.stats) return cudaErrorNotSupported;
+    if (ip.maxMG > 0 && (!ip.hgX || !ip.hgY || !ip.hgScaleX || !ip.hgScaleY)) return cudaErrorNotSupported;
+    if (p.frameCount <= 0) return cudaSuccess;
+    CUtensorMap map;
+    cudaError_t e = prepareI8(p, map);
+    if (e != cudaSuccess) return e;
+    DhInvParams q = ip;
+    if (!q.coefs) q.maxMG = 0;
+    if (q.maxMG <= 0) { q.maxMG = 0; q.modeCount = 0; }
+    const int W = 1 << p.logW;
+    if (W == 128) return launchI8<128, 16, 40, 3, 3, true>(p, q, map, s);
+    return launchI8<64, 16, 40, 4, 3, true>(p, q, map, s);
 }

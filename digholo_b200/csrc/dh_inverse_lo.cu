@@ -106,14 +106,30 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
     float* hx = smf;
     float* hy = hx + P * G * HLD;
     float* yax = hy + P * G * HLD;
-    int* modeMN = reinterpret_cast<int*>(yax + L);
+    float* hsc = yax + L;                                   // [x, y][P][G] mode scales
+    int* refs = reinterpret_cast<int*>(hsc + 2 * P * G);    // [P][Xr Xi Yr Yi][L] 14-bit wave
+    int* modeMN = refs + P * 4 * L;
     float2* tiles = reinterpret_cast<float2*>(modeMN + ((M + 1) & ~1));
-    for (int e = threadIdx.x; e < P * G * L; e += blockDim.x) {
-        const int row = e / L, x = e - row * L;
-        hx[row * HLD + x] = (float)p.hgX[e];
-        hy[row * HLD + x] = (float)p.hgY[e];
+    // 8 mode values per 16-byte load: the tables arrive in about one round of loads
+    for (int e = threadIdx.x; e < P * G * L / 8; e += blockDim.x) {
+        const int row = (8 * e) / L, x0 = 8 * e - row * L;
+        const uint4 ax = __ldg(reinterpret_cast<const uint4*>(p.hgX) + e);
+        const uint4 ay = __ldg(reinterpret_cast<const uint4*>(p.hgY) + e);
+        const unsigned wx[4] = {ax.x, ax.y, ax.z, ax.w}, wy[4] = {ay.x, ay.y, ay.z, ay.w};
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            hx[row * HLD + x0 + t] = (float)(short)((wx[t >> 1] >> (16 * (t & 1))) & 0xFFFFu);
+            hy[row * HLD + x0 + t] = (float)(short)((wy[t >> 1] >> (16 * (t & 1))) & 0xFFFFu);
+        }
     }
     for (int e = threadIdx.x; e < L; e += blockDim.x) yax[e] = p.yAxis[e];
+    // the wave and the scales in shared memory: no global load waits behind
+    // the field and coefficient stores
+    for (int e = threadIdx.x; e < P * 4 * L; e += blockDim.x) refs[e] = p.refWave[e];
+    for (int e = threadIdx.x; e < P * G; e += blockDim.x) {
+        hsc[e] = p.hgScaleX[e];
+        hsc[P * G + e] = p.hgScaleY[e];
+    }
     for (int mode = threadIdx.x; mode < M; mode += blockDim.x) {
         // mode -> (m, n): group g, n = mode - g(g+1)/2, m = g - n (digHolo.cpp:1245-1265)
         int g = (int)((sqrtf(8.0f * mode + 1.0f) - 1.0f) * 0.5f);
@@ -193,7 +209,7 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
     }
 
     // 4. reference wave, -conj(A . ref), int16 rounding (digHolo.cpp:2741-2833)
-    const short* ref = p.refWave + (size_t)pol * 4 * L;
+    const int* ref = refs + (size_t)pol * 4 * L;
     const int xr = ref[ln], xi = ref[L + ln];
     const float K = (float)(1.0 / (16383.0 * 16383.0));
     const size_t fieldOff = (size_t)unit * npix;
@@ -241,8 +257,8 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
     }
     __syncwarp(gmask);
     const float fieldScale = 1.0f / scale;
-    const float* sxp = p.hgScaleX + pol * G;
-    const float* syp = p.hgScaleY + pol * G;
+    const float* sxp = hsc + pol * G;
+    const float* syp = hsc + P * G + pol * G;
     float2* cout = p.coefs + (size_t)frame * P * M + (size_t)pol * M;
     for (int mode = ln; mode < M; mode += L) {
         const int mn = modeMN[mode];
@@ -263,6 +279,9 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
 // Returns cudaErrorNotSupported for shapes this kernel does not cover.
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s) {
     if (!p.lowres || p.logw != p.logh || (p.logw != 4 && p.logw != 5)) return cudaErrorNotSupported;
+    // the table loads read 16-byte chunks of the int16 modes
+    if (p.maxMG > 0 && ((reinterpret_cast<uintptr_t>(p.hgX) | reinterpret_cast<uintptr_t>(p.hgY)) & 15))
+        return cudaErrorNotSupported;
     const int L = 1 << p.logw;
     const int units = p.frameCount * p.polCount;
     if (units <= 0) return cudaSuccess;
@@ -270,7 +289,8 @@ cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s) {
     const int M = p.maxMG > 0 ? p.modeCount : 0;
     const int ULD = (G + 1) | 1;
     const int UPB = (32 / L) * LO_WARPS;
-    const size_t smem = sizeof(float) * ((size_t)2 * p.polCount * G * (L + 1) + L) + sizeof(int) * (size_t)((M + 1) & ~1) +
+    const size_t smem = sizeof(float) * ((size_t)2 * p.polCount * G * (L + 1) + L + 2 * (size_t)p.polCount * G) +
+                        sizeof(int) * ((size_t)p.polCount * 4 * L + (size_t)((M + 1) & ~1)) +
                         sizeof(float2) * (size_t)UPB * L * (ULD > L + 1 ? ULD : L + 1);
     if (smem > 200 * 1024) return cudaErrorNotSupported;
     DhInvParams q = p;

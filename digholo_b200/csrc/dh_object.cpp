@@ -15,6 +15,8 @@ cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_reg(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s);
+cudaError_t dh_launch_forward_i8_fused(const DhFwdParams& p, const DhInvParams& ip, cudaStream_t s);
+cudaError_t dh_launch_fourier_full(const DhFourierParams& q, cudaStream_t s);
 int dh_forward_i8_npad(int w);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
@@ -661,6 +663,13 @@ static int updateBasis(Object& o) {
     return ERR_SUCCESS;
 }
 
+// HG basis for the current configuration (recomputed when the waist, axes or
+// group count changed); the benchmark forces one recomputation.
+int objUpdateBasis(Object& o) {
+    std::lock_guard<std::mutex> guard(o.lock);
+    return updateBasis(o);
+}
+
 static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
     const Geometry& g = o.geo;
     memset(&ip, 0, sizeof(ip));
@@ -747,7 +756,7 @@ static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) 
 // block-per-unit kernel.
 static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc = true) {
     if (o.inverseKernel == 2) return launchBands(o, ip, mayAlloc);
-    if (o.inverseKernel == 0) {
+    if (o.inverseKernel == 0 || o.inverseKernel == 3) {   // 3: as 0 where not fused
         cudaError_t e = dh_launch_inverse_lo(ip, o.stream);
         if (e == cudaSuccess) { o.lastInverseKernel = 2; return e; }
         if (e != cudaErrorNotSupported) return e;
@@ -815,11 +824,8 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         o.evStageUsed++;
         DH_CUDA(o, cudaEventRecord(ev[0], o.stream));
     }
-    cudaError_t fe = launchForward(o, fp);
-    if (fe != cudaSuccess) return failCuda(o, fe, "forward kernel launch");
-    if (timed) DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
+    DhInvParams ip = ip0;
     if (ip0.fieldR) {
-        DhInvParams ip = ip0;
         const size_t npix = (size_t)g.nx * g.ny;
         ip.window = ip0.window + (size_t)f0 * P * g.w * g.h;
         ip.frameCount = f1 - f0;
@@ -828,8 +834,30 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         if (ip.field32) ip.field32 = ip0.field32 + (size_t)f0 * P * npix;
         ip.stats = ip0.stats + f0;
         if (ip.coefs) ip.coefs = ip0.coefs + (size_t)f0 * P * o.modeCount;
-        DH_CUDA(o, launchInverse(o, ip));
+        // both stages in one launch, on request (inverse choice 3): the
+        // tensor-core forward with 16 x 16 low-resolution fields.  Measured
+        // slower than the two launches, whose inverse kernel runs many more
+        // units at once than the forward kernel's epilogue groups can.
+        if ((o.forwardKernel == 0 || o.forwardKernel == 4) && o.inverseKernel == 3) {
+            cudaError_t fe = dh_launch_forward_i8_fused(fp, ip, o.stream);
+            if (fe == cudaSuccess) {
+                o.lastForwardKernel = 4;
+                o.lastInverseKernel = 5;
+                o.lastOverlapKernel = 1;
+                if (timed) {
+                    DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
+                    DH_CUDA(o, cudaEventRecord(ev[2], o.stream));
+                }
+                return ERR_SUCCESS;
+            }
+            if (fe != cudaErrorNotSupported) return failCuda(o, fe, "fused forward/inverse kernel launch");
+            cudaGetLastError();
+        }
     }
+    cudaError_t fe = launchForward(o, fp);
+    if (fe != cudaSuccess) return failCuda(o, fe, "forward kernel launch");
+    if (timed) DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
+    if (ip0.fieldR) DH_CUDA(o, launchInverse(o, ip));
     if (timed) DH_CUDA(o, cudaEventRecord(ev[2], o.stream));
     return ERR_SUCCESS;
 }
@@ -933,6 +961,31 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     o.processedOverlap = o.modeCount > 0;
     o.metricsValid = 0;
     (void)g;
+    // the frame source of this batch, for the Fourier planes on request
+    o.lastFwd = fp;
+    if (!o.framesOnDevice) {
+        o.lastFwd.frames = o.dFrames.ptr;
+        o.lastFwd.frameWidth = g.W;
+        o.lastFwd.frameStride = (long long)P * g.H * g.W;
+        for (int p = 0; p < P; p++) { o.lastFwd.cx[p] = 0; o.lastFwd.cy[p] = p * g.H; }
+    } else {
+        o.lastFwd.frames = o.frames;
+        o.lastFwd.frameWidth = o.cfg.frameWidth;
+        o.lastFwd.frameStride = (long long)o.cfg.frameWidth * o.cfg.frameHeight;
+        for (int p = 0; p < P; p++) { o.lastFwd.cx[p] = g.cx[p]; o.lastFwd.cy[p] = g.cy[p]; }
+    }
+    o.lastFwd.frameCount = B;
+    o.lastFwd.frameOffset = 0;
+    {
+        // the excluded disk of the Fourier-plane analysis: radius 2 k0 sin(aperture)
+        // in float32 (digHolo.cpp:6936-6939)
+        const Config& cc = o.useSnaps ? o.fftSnap : o.cfg;
+        const float k0 = 2 * PI_F / cc.wavelengthCentre;
+        const float R = 2 * k0 * sinf(cc.apertureSize * UNIT_ANGLE);
+        o.lastFourierR2 = R * R;
+    }
+    o.lastFwdValid = 1;
+    o.fourierValid = 0;
     if (syncCoefs) return objCoefsToHost(o);
     return ERR_SUCCESS;
 }
@@ -1120,13 +1173,59 @@ int objOverlap(Object& o) {
     return objCoefsToHost(o);
 }
 
+// Fourier planes of the last batch, their statistics and batch-sum intensity
+// (computed once per batch from the frames it was processed from; those
+// frames must still be valid, as for digHoloProcessBatch), copied to the
+// host mirrors; the plane only when withPlane.
+int objFourierToHost(Object& o, int withPlane) {
+    if (!o.lastFwdValid) return fail(o, ERR_NULLPOINTER, "no batch has been processed");
+    const Geometry& g = o.geo;
+    const int B = o.lastFwd.frameCount, P = o.polCount;
+    const size_t Nx = (size_t)g.W / 2 + 1;
+    const size_t planeN = (size_t)B * P * g.H * Nx;
+    const size_t statsN = (size_t)ANALYSIS_COUNT * P * (B + 1);
+    const size_t sumN = (size_t)P * g.W * g.H;
+    if (!o.fourierValid) {
+        DH_CUDA(o, o.dFourier.ensure(planeN * sizeof(float2)));
+        DH_CUDA(o, o.dFftStats.ensure(statsN * sizeof(float)));
+        DH_CUDA(o, o.dFftBatchSum.ensure(sumN * sizeof(float)));
+        DH_CUDA(o, cudaMemsetAsync(o.dFftBatchSum.ptr, 0, sumN * sizeof(float), o.stream));
+        DhFourierParams q;
+        memset(&q, 0, sizeof(q));
+        q.f = o.lastFwd;
+        q.plane = o.dFourier.as<float2>();
+        q.kx = o.dKx.as<float>();
+        q.ky = o.dKy.as<float>();
+        q.r2 = o.lastFourierR2;
+        q.stats = o.dFftStats.as<float>();
+        q.batchSum = o.dFftBatchSum.as<float>();
+        DH_CUDA(o, dh_launch_fourier_full(q, o.stream));
+        o.fourierValid = 1;
+    }
+    if (!o.hFftStats.ensure(statsN * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host Fourier stats buffer");
+    if (!o.hFftBatchSum.ensure(sumN * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host Fourier batch-sum buffer");
+    DH_CUDA(o, cudaMemcpyAsync(o.hFftStats.ptr, o.dFftStats.ptr, statsN * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.hFftBatchSum.ptr, o.dFftBatchSum.ptr, sumN * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
+    if (withPlane) {
+        if (!o.hFourier.ensure(planeN * sizeof(float2))) return fail(o, ERR_MEMORYALLOCATION, "host Fourier plane buffer");
+        DH_CUDA(o, cudaMemcpyAsync(o.hFourier.ptr, o.dFourier.ptr, planeN * sizeof(float2), cudaMemcpyDeviceToHost, o.stream));
+    }
+    DH_CUDA(o, cudaStreamSynchronize(o.stream));
+    o.hKx = g.kx;
+    o.hKy = g.ky;
+    return objCheckStatus(o);
+}
+
 int objStatsToHost(Object& o) {
     const int B = o.batchCount, P = o.polCount;
     const Geometry& g = o.geo;
     const size_t npix = (size_t)g.nx * g.ny;
     const size_t n = (size_t)ANALYSIS_COUNT * P * (B + 1);
     if (!o.hStats.ensure(n * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host stats buffer");
-    if (!o.hBatchSum.ensure((size_t)P * npix * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host batch-sum buffer");
+    // per polarisation W H floats, the plane in the first nx ny (the reference
+    // sizes every batch-sum plane by the FFT window, digHolo.cpp:7655)
+    const size_t stride = std::max((size_t)g.W * g.H, npix);
+    if (!o.hBatchSum.ensure((size_t)P * stride * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host batch-sum buffer");
     DH_CUDA(o, o.dFieldsC64.ensure((size_t)P * npix * sizeof(float)));
     DH_CUDA(o, dh_launch_batchsum(o.dFieldR.as<short>(), o.dFieldI.as<short>(), o.dStats.as<float>(), B + 1, P, B,
                                   (int)npix, o.dFieldsC64.as<float>(), o.stream));
@@ -1150,7 +1249,9 @@ int objStatsToHost(Object& o) {
                 cy += g.y[y] * I;
                 cyw += (g.y[y] + (g.y[y] < 0 ? yShift : 0.f)) * I;
                 e4 += I * I;
-                const int idx = 2 * y * g.nx + x;
+                // the reference compares the summed intensity against an index
+                // vector already advanced to the next block of 8 (digHolo.cpp:2533-2561)
+                const int idx = 2 * y * g.nx + x + 8;
                 if (I >= mx) { mx = I; mxIdx = idx; }
             }
         const int per = P * S;
@@ -1162,6 +1263,12 @@ int objStatsToHost(Object& o) {
         memcpy(&s[4 * per + col], &mxIdx, sizeof(int));
         s[5 * per + col] = (float)(dA * (Pw * Pw / e4));
         s[6 * per + col] = (float)(cyw / Pw);
+    }
+    // spread the polarisations to their strides (last first: the moves go up)
+    float* sb = o.hBatchSum.as<float>();
+    for (int p = P - 1; p >= 0; p--) {
+        if (p > 0) memmove(sb + (size_t)p * stride, sb + (size_t)p * npix, npix * sizeof(float));
+        memset(sb + (size_t)p * stride + npix, 0, (stride - npix) * sizeof(float));
     }
     return ERR_SUCCESS;
 }

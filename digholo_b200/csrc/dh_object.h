@@ -141,6 +141,14 @@ struct Object {
     // power meter / AutoAlign
     DevBuf dMetricA, dMetricG, dCoefsBackup, dAlignFrames;
     DevBuf dDigits;                     // tensor-core row DFT digits (uint16 frames)
+    // Fourier planes of the last batch (on request): the frame source the
+    // batch was processed from, the planes, their statistics and batch sum
+    DhFwdParams lastFwd;
+    int lastFwdValid = 0, fourierValid = 0;
+    float lastFourierR2 = 0.f;
+    DevBuf dFourier, dFftStats, dFftBatchSum;
+    HostBuf hFourier, hFftStats, hFftBatchSum;
+    std::vector<float> hKx, hKy;
     int digitsValid = 0;
     DevBuf dBigScratch;                 // band kernels: partial statistics and coefficients, prepared Hx
     DevBuf dTransRaw, dTransFrames;     // transposed uint16 input: raw host copy, converted frames
@@ -204,8 +212,10 @@ int objProcessBatch(Object& o, int syncCoefs);
 int objCoefsToHost(Object& o);
 int objFieldsToHost(Object& o, int complexOut);
 int objStatsToHost(Object& o);
+int objFourierToHost(Object& o, int withPlane);
 int objWindowToHost(Object& o);
 int objStageTimes(Object& o, float* ms);
+int objUpdateBasis(Object& o);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
 int objInverseAux(Object& o, const float2* window, int frameCount, float2* field32, short* scratchR, short* scratchI,

@@ -91,3 +91,15 @@ struct DhBasisParams {
     float* outF;         // optional [modes][count] unquantised float modes
     int modes16;         // modes written to out16 / scale (the first modes16)
 };
+
+// Full R2C Fourier planes of the FFT windows and their analysis (the
+// reference's digHoloPixelsFourierPlane and digHoloFFTAnalysis).
+struct DhFourierParams {
+    DhFwdParams f;          // frame source and FFT-window geometry
+    float2* plane;          // out: [frame][pol][H][W/2+1]
+    const float* kx;        // fftshifted kx axis (W)
+    const float* ky;        // fftshifted ky axis (H)
+    float r2;               // squared radius of the excluded disk (0: none)
+    float* stats;           // out: [param][pol][frameCount + 1] (DIGHOLO_ANALYSIS layout)
+    float* batchSum;        // out: [pol][W H], pixel (j, i) at j (W/2+1) + i
+};

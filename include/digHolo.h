@@ -275,8 +275,17 @@ int digHoloProcessIFFT(int handleIdx);
 int digHoloProcessRemoveTilt(int handleIdx);
 /* replaces digHolo.h:1706 */
 int digHoloProcessBasisExtractCoefs(int handleIdx);
+/* replaces digHolo.h:1718.  The R2C Fourier planes [batch][pol][H][W/2+1]
+ * of the last batch, computed from its frames on the first call after the
+ * batch (the frame buffer must still be valid, as for ProcessBatch); *width
+ * is the FFT window width W, as in the reference. */
+complex64* digHoloGetFourierPlaneFull(int handleIdx, int* batchCount, int* polCount, int* width, int* height);
 /* replaces digHolo.h:1732 */
 complex64* digHoloGetFourierPlaneWindow(int handleIdx, int* batchCount, int* polCount, int* width, int* height);
+/* replaces digHolo.h:1776.  Batches per second over about goalDuration
+ * seconds of digHoloProcessBatch; info[6] (optional) per-stage rates
+ * (DIGHOLO_BENCHMARK_FFT .. TOTAL, digHolo.h:1783-1788). */
+float digHoloBenchmark(int handleIdx, float goalDuration, float* info);
 /* replaces digHolo.h:1749 */
 int digHoloConfigSetThreadCount(int handleIdx, int threadCount);
 /* replaces digHolo.h:1757 */
@@ -340,11 +349,14 @@ int digHoloB200GetForwardKernel(int handleIdx);
  * kernel up to 128 x 128 pixels, bands of 64 rows beyond; else one block),
  * 1 one block per frame and polarisation, 2 full-resolution bands only (the
  * batch fails where they do not apply: low resolution, fields under 64 x 64,
- * windows under 16 pixels, maxMG > 32). */
+ * windows under 16 pixels, maxMG > 32), 3 as 0 but fused into the
+ * tensor-core forward kernel where it applies (uint16 frames, 16 x 16
+ * low-resolution fields: one launch per batch). */
 int digHoloB200SetInverseKernel(int handleIdx, int kernel);
 /* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit,
  * 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands
- * (statistics pass, quantising pass with the overlap, coefficient sum). */
+ * (statistics pass, quantising pass with the overlap, coefficient sum),
+ * 5 fused into the tensor-core forward kernel (inverse choice 3). */
 int digHoloB200GetInverseKernel(int handleIdx);
 /* Overlap of full-resolution fields: 0 (default) on the tensor cores in
  * split-BF16 precision (bf16 hi + lo of both int16 operands, three products,

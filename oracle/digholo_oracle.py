@@ -20,6 +20,7 @@ It restates, step by step, the work of digHoloProcessBatch
   ifft_axes           reconstructed-plane axes        digHolo.cpp:8183-8203
   copy_window         Fourier window copy             digHolo.cpp:1808-2122
   field_analysis      power / CoM / max / Aeff        digHolo.cpp:2354-2654, 9103-9176
+  fourier_analysis    the same on the R2C plane       digHolo.cpp:6931-6980, 8990-9180
   reference_wave      separable tilt/defocus wave     digHolo.cpp:10201-10504
   apply_tilt          -conj(A.ref) and int16 rounding digHolo.cpp:2701-2837
   hg_basis            int16 HG modes and scales       digHolo.cpp:1269-1484, 10543-10645
@@ -289,6 +290,68 @@ def field_analysis(E, x, y):
             "scale": np.array([float(F32(32767.0 / m)) if m > 0 else np.inf for m in mx])}
 
 
+def fourier_analysis(F, kx, ky, wavelength, aperture_deg):
+    """FFT-stage analysis of one polarisation's R2C planes (digHoloFFTAnalysis,
+    digHolo.cpp:6931-6980 -> digHoloFieldAnalysisRoutine 8990-9180 ->
+    digHoloFieldAnalysis 2354-2654 with removeZeroOrder1D set and no y wrap).
+
+    F: (B, H, W/2+1) complex R2C planes.  As the reference does, the plane's
+    column i and row j are given the fftshifted axis values kx[i], ky[j].
+    Pixel (j, i) enters when j is neither 0 nor H/2, 0 < i < 8 floor(Nx/8)
+    (Nx = W/2+1), and kx[i]^2 + ky[j]^2 >= R^2 with R = 2 k0 sin(aperture)
+    (float32); the other pixels count as zero.  Intensity I = |F|^2/(Nx Ny).
+    Returns per-frame and batch-sum statistics ((B+1,) arrays: power, comx,
+    comy, comywrap, aeff, maxabs, scale = 32767/maxabs, maxidx = 2 j Nx + i of
+    the maximum, the larger index on ties, plus 8 for the batch-sum entry as
+    the reference reads it) and the batch-sum plane (H, Nx).
+    The per-frame maximum is of |F| (unnormalised), the batch entry's of the
+    summed normalised intensity, as in the reference.
+    """
+    F = np.asarray(F)
+    B, Ny, Nx = F.shape
+    k0 = F32(F32(2) * PI_F / F32(wavelength))
+    R = F32(F32(2) * k0 * F32(np.sin(F32(F32(aperture_deg) * UNIT_ANGLE))))
+    xs = kx[:Nx].astype(F32)
+    ys = ky[:Ny].astype(F32)
+    rx = (xs.astype(F32) * xs.astype(F32)).astype(F32)
+    ry = (ys.astype(F32) * ys.astype(F32)).astype(F32)
+    rr = (ry[:, None] + rx[None, :]).astype(F32)
+    mask = rr >= F32(R * R) if R != 0 else np.ones((Ny, Nx), dtype=bool)
+    nxr = 8 * (Nx // 8)
+    mask[:, nxr:] = False
+    mask[:, 0] = False
+    mask[0, :] = False
+    mask[Ny // 2, :] = False
+    I0 = (np.abs(F) ** 2) * mask[None]
+    I = I0 / (Nx * Ny)
+    S = I.sum(axis=0)
+    allI = np.concatenate([I, S[None]], axis=0)
+    X = xs.astype(np.float64)[None, None, :]
+    Y = ys.astype(np.float64)[None, :, None]
+    shift = abs(float(F32((ys[1] - ys[0]) * F32(Ny))))
+    Yw = Y + shift * (Y < 0)
+    P = allI.sum(axis=(1, 2))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        comx = (allI * X).sum(axis=(1, 2)) / P
+        comy = (allI * Y).sum(axis=(1, 2)) / P
+        comyw = (allI * Yw).sum(axis=(1, 2)) / P
+        E4 = (allI ** 2).sum(axis=(1, 2))
+        dA = abs(float(kx[2] - kx[1])) * abs(float(ky[2] - ky[1]))
+        aeff = dA * P * P / E4
+    peak = np.concatenate([I0, S[None]], axis=0).reshape(B + 1, -1)
+    flat = np.arange(Ny * Nx)
+    idx2 = 2 * (flat // Nx) * Nx + (flat % Nx)
+    maxidx = np.array([int(idx2[np.flatnonzero(p == p.max())[-1]]) for p in peak])
+    # the batch-sum comparison reads the index vector after it has advanced to
+    # the next block of 8 (digHolo.cpp:2533-2561)
+    maxidx[-1] += 8
+    mx = np.sqrt(peak.max(axis=1))
+    with np.errstate(divide="ignore"):
+        scale = np.array([float(F32(32767.0 / m)) if m > 0 else np.inf for m in mx])
+    return {"power": P, "comx": comx, "comy": comy, "comywrap": comyw, "aeff": aeff, "maxabs": mx,
+            "scale": scale, "maxidx": maxidx, "batchsum": S}
+
+
 def _safe_stats(E, x, y):
     with np.errstate(invalid="ignore", divide="ignore"):
         return field_analysis(E, x, y)
@@ -500,7 +563,9 @@ def process_batch(frames, cfg, quantised=True):
     nx, ny = xax.size, yax.size
     Fplanes = r2c_windows(frames, cfg, W, H, cxs, cys)
     res = {"W": W, "H": H, "cx": cxs, "cy": cys, "w": w, "h": h, "SX": SX, "SY": SY,
-           "x": xax, "y": yax, "kx": kx, "ky": ky}
+           "x": xax, "y": yax, "kx": kx, "ky": ky, "fourier": Fplanes,
+           "fft_stats": [fourier_analysis(Fplanes[:, p], kx, ky, cfg.wavelength, cfg.window_radius_deg)
+                         for p in range(P)]}
     windows = np.zeros((B, P, h if cfg.resolution_mode else H, w if cfg.resolution_mode else W),
                        dtype=np.complex128)
     untilted = np.zeros((B, P, ny, nx), dtype=np.complex128)

@@ -79,3 +79,38 @@ def test_tensor_core_forward(lib, name, mode):
     assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
     assert rel_l2(g["field"], o["field"]) <= 5e-5
     assert rel_l2(g["coefs"], o["coefs"]) <= (1e-4 if mode == 0 else 5e-5)
+
+
+@pytest.mark.parametrize("full16", [False, True])
+def test_fused_forward_inverse(lib, full16):
+    """uint16 frames with 16 x 16 low-resolution fields: forward and inverse
+    stages in one launch (inverse choice 3, reported as kernel 5) against the two-launch path
+    (tensor-core forward, warp-per-unit inverse; the automatic choice) on
+    the same frames: equal int16 fields and statistics, coefficients within
+    1e-6 relative L2, and the oracle bounds of test_gpu_parity.  12-bit
+    pixels and the full 16-bit range."""
+    hol = make_case("batched_640x512_u16_2pol", 16)
+    if full16:
+        hol.frames = (hol.frames.astype(np.uint32) * 16 + 7).clip(0, 65535).astype(np.uint16)
+    cfg = config_for(hol, 1)
+    h = lib.digHoloCreate()
+    api.configure(lib, h, cfg)
+    sep = api.run_batch(lib, h, hol.frames)
+    ks = (lib.digHoloB200GetForwardKernel(h), lib.digHoloB200GetInverseKernel(h))
+    lib.digHoloDestroy(h)
+    h2 = lib.digHoloCreate()
+    api.configure(lib, h2, cfg)
+    assert lib.digHoloB200SetInverseKernel(h2, 3) == 0
+    g2 = api.run_batch(lib, h2, hol.frames)
+    kf = lib.digHoloB200GetInverseKernel(h2)
+    lib.digHoloDestroy(h2)
+    assert ks == (4, 2) and kf == 5
+    np.testing.assert_array_equal(g2["R"], sep["R"])
+    np.testing.assert_array_equal(g2["I"], sep["I"])
+    np.testing.assert_array_equal(g2["summary"], sep["summary"])
+    d = rel_l2(g2["coefs"], sep["coefs"])
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    print("fused vs two launches: coefficient rel L2 %.2e; vs oracle %.2e" % (d, rel_l2(g2["coefs"], o["coefs"])))
+    assert d <= 1e-6
+    assert max(np.abs(g2["R"].astype(int) - o["R"]).max(), np.abs(g2["I"].astype(int) - o["I"]).max()) <= 2
+    assert rel_l2(g2["coefs"], o["coefs"]) <= 5e-5

@@ -43,8 +43,8 @@ def lib():
 # wherever they apply), 1 generic shared-memory kernel, 2 register kernel,
 # 3 TMA-fed kernel, 4 tensor-core row DFT (uint16 frames only); inverse 0
 # automatic (one warp per unit for 16/32-pixel low-resolution fields), 1 one
-# block per unit
-KERNELS = [(0, 0), (1, 1), (2, 0), (0, 1), (3, 0)]
+# block per unit, 3 fused into the tensor-core forward kernel where it applies
+KERNELS = [(0, 0), (1, 1), (2, 0), (0, 1), (3, 0), (0, 3)]
 
 
 def _run(lib, hol, cfg, keep32=False, kernel=(0, 0), overlap=0):
@@ -77,9 +77,15 @@ def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, kernel):
     # every workload here fits the TMA-fed forward kernel (the uint16 ones the
     # tensor-core kernel), and in mode 1 the warp-per-unit inverse kernel;
     # otherwise the kernels asked for run
-    auto = 4 if hol.frames.dtype == np.uint16 else 3
+    u16 = hol.frames.dtype == np.uint16
+    auto = 4 if u16 else 3
     assert g["kernel"][0] == (auto if kernel[0] == 0 else kernel[0])
-    assert g["kernel"][1] == ((2 if mode == 1 else 3) if kernel[1] == 0 else 1)
+    if kernel == (0, 3) and u16 and mode == 1:
+        # uint16 frames with 16 x 16 low-resolution fields: one fused launch
+        assert g["kernel"][1] == 5
+        kernel = (0, 3, "fused")
+    if len(kernel) == 2:
+        assert g["kernel"][1] == ((2 if mode == 1 else 3) if kernel[1] in (0, 3) else 1)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert g["R"].shape == o["R"].shape
     np.testing.assert_array_equal(g["x"], o["x"])

@@ -86,3 +86,42 @@ def test_metrics_on_unitary_batch():
     m = O.power_meter(q.T.reshape(6, 1, 6))
     assert abs(m["il_db"]) < 1e-9 and abs(m["mdl_db"]) < 1e-9
     assert abs(m["il_frob_db"]) < 1e-9
+
+
+def check_fourier(o, f, cfg, plane_tol=1e-6):
+    """Plane-0 outputs (Fourier plane, its statistics and batch sum) against
+    the oracle: plane relative L2 <= plane_tol, power / CoM / Aeff / scale
+    relative <= 1e-4 (FP32 sums over the plane), the maximum's index equal,
+    batch-sum plane relative L2 <= 1e-5 over the analysed pixels."""
+    P = cfg.pol_count
+    planes = o["fourier"]
+    assert rel_l2(f["plane"], planes) <= plane_tol
+    assert f["width"] == o["W"]
+    s = f["summary"]
+    for pol in range(P):
+        st = o["fft_stats"][pol]
+        for k, name in ((0, "power"), (1, "comx"), (2, "comy"), (5, "aeff"), (6, "comywrap"), (3, "scale")):
+            got = s[k, pol].astype(np.float64)
+            ref = st[name]
+            assert np.all(np.abs(got - ref) <= 1e-4 * np.abs(ref) + 1e-30), (name, got, ref)
+        np.testing.assert_array_equal(s[4, pol].view(np.int32), st["maxidx"])
+        bs = f["batchsum"][pol]
+        assert rel_l2(bs, st["batchsum"]) <= 1e-5
+
+
+@pytest.mark.parametrize("workload", ["plain_320x256_f32_1pol", "batched_640x512_u16_2pol"])
+def test_fourier_analysis_matches_live_reference(workload):
+    """The FFT-stage analysis of the oracle against the reference's own
+    digHoloGetFourierPlaneFull and digHoloBatchGetSummary(plane 0)."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from digholo_b200 import api
+    hol = make_case(workload, 4)
+    cfg = config_for(hol, 1)
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    ref_lib.run_batch(L, h, hol.frames)
+    f = api.read_fourier(L, h)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    check_fourier(o, f, cfg)
