@@ -438,10 +438,14 @@ def main():
     w, hh, nx, ny = geo[2], geo[3], geo[4], geo[5]
     fwd_bytes = B * (P * W * H * 2 + P * w * hh * 8)
     inv_bytes = B * (P * w * hh * 8 + P * nx * ny * 4 + P * M * 8 + 7 * P * 4)
+    fwd_name = {1: "k_forward", 2: "k_forward_reg", 3: "k_forward_tma", 4: "k_forward_i8"}.get(
+        L.digHoloB200GetForwardKernel(h), "k_forward")
+    inv_name = {1: "k_inverse", 2: "k_inverse_lo", 3: "k_field_full", 4: "k_field_big"}.get(
+        L.digHoloB200GetInverseKernel(h), "k_inverse")
     if fwd_ms >= inv_ms:
-        kname, kbytes, kms = "k_forward", fwd_bytes, fwd_ms / max(timed, 1)
+        kname, kbytes, kms = fwd_name, fwd_bytes, fwd_ms / max(timed, 1)
     else:
-        kname, kbytes, kms = "k_inverse", inv_bytes, inv_ms / max(timed, 1)
+        kname, kbytes, kms = inv_name, inv_bytes, inv_ms / max(timed, 1)
     achieved = kbytes / (kms / 1e3) / 1e9
     traffic = profile_traffic(kname, args.mode)
 

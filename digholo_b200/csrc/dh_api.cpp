@@ -702,7 +702,7 @@ int digHoloB200GetGeometry(int h, int* out10) {
 // the shared-memory kernel (used by the tests to cover both).
 int digHoloB200SetForwardKernel(int h, int kernel) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    if (kernel < 0 || kernel > 4) return dh::ERR_INVALIDARGUMENT;
+    if (kernel < 0 || kernel > 5) return dh::ERR_INVALIDARGUMENT;
     o->forwardKernel = kernel;
     return dh::ERR_SUCCESS;
 }
@@ -731,7 +731,7 @@ int digHoloB200GetOverlapKernel(int h) {
     return o->lastOverlapKernel;
 }
 // Forward kernel used by the last batch: 1 generic, 2 register, 3 TMA-fed,
-// 4 tensor-core row DFT (uint16 frames).
+// 4 tensor-core row DFT (uint16 frames), 5 full planes.
 int digHoloB200GetForwardKernel(int h) {
     OBJ_OR(h, 0);
     return o->lastForwardKernel;

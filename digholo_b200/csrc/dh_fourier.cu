@@ -211,6 +211,58 @@ __global__ void __launch_bounds__(FT) k_fourier_sum_stats(DhFourierParams q) {
 
 }  // namespace
 
+// Fourier window of each (frame, polarisation) from its full plane: rows
+// (j + SY + H/2) mod H, columns sx0 .. sx0 + w - 1 of the R2C plane, times the
+// batch calibration and the window factors (mask, normalisation, inverse
+// pixel sinc, beam-centre phase: tabAdj), as digHoloCopyWindow
+// (digHolo.cpp:1808-2122) and the pruned forward kernels.
+__global__ void k_window_from_plane(DhFourierParams q) {
+    const DhFwdParams& f = q.f;
+    const int W = 1 << f.logW, H = 1 << f.logH, Nx = W / 2 + 1;
+    const int P = f.polCount, w = f.w, h = f.h;
+    const int total = f.frameCount * P * h * w;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int c = e % w, j = (e / w) % h, unit = e / (w * h);
+        const int pol = unit % P, frame = unit / P;
+        const int row = (j + f.sy[pol] + H / 2) & (H - 1);
+        float2 Y = q.plane[((size_t)unit * H + row) * Nx + f.sx0[pol] + c];
+        if (f.batchCal && f.batchCalCount > 0)
+            Y = cmul(Y, f.batchCal[pol * f.batchCalCount + ((f.frameOffset + frame) % f.batchCalCount)]);
+        f.window[e] = cmul(Y, f.tabAdj[((size_t)pol * h + j) * w + c]);
+    }
+}
+
+// Forward stage through the full planes (windows of 256 pixels or more,
+// where the pruned kernels do not apply): q.plane receives the R2C planes,
+// q.f.window the Fourier windows.  cudaErrorNotSupported when a window
+// column falls outside the R2C half plane or the tables are missing.
+cudaError_t dh_launch_forward_plane(const DhFourierParams& q, cudaStream_t s) {
+    const DhFwdParams& f = q.f;
+    const int W = 1 << f.logW, H = 1 << f.logH, N = W / 2;
+    if (!f.tabAdj || !q.plane || W < 16 || H < 16 || W > TW_N || H > TW_N) return cudaErrorNotSupported;
+    for (int p = 0; p < f.polCount; p++)
+        if (f.sx0[p] < 0 || f.sx0[p] + f.w > N + 1) return cudaErrorNotSupported;
+    const int units = f.frameCount * f.polCount;
+    if (units <= 0) return cudaSuccess;
+    int RB = FBUF / N;
+    if (RB > H) RB = H;
+    int CB = FBUF / H;
+    if (CB < 1) CB = 1;
+    const int Nx = N + 1;
+    const size_t smemR = sizeof(float2) * (size_t)RB * N, smemC = sizeof(float2) * (size_t)H * CB;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_fourier_rows), (int)smemR);
+    if (e != cudaSuccess) return e;
+    e = setSmemOnce(reinterpret_cast<const void*>(k_fourier_cols), (int)smemC);
+    if (e != cudaSuccess) return e;
+    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(q);
+    k_fourier_cols<<<(unsigned)(units * ((Nx + CB - 1) / CB)), FT, smemC, s>>>(q);
+    const int total = units * f.h * f.w;
+    int g = (total + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    k_window_from_plane<<<g, 256, 0, s>>>(q);
+    return cudaGetLastError();
+}
+
 // Fourier planes and their analysis for q.f.frameCount frames.
 // cudaErrorNotSupported for window sides above 4096 or under 16.
 cudaError_t dh_launch_fourier_full(const DhFourierParams& q, cudaStream_t s) {

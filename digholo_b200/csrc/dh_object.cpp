@@ -17,6 +17,7 @@ cudaError_t dh_launch_forward_tma(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_i8_fused(const DhFwdParams& p, const DhInvParams& ip, cudaStream_t s);
 cudaError_t dh_launch_fourier_full(const DhFourierParams& q, cudaStream_t s);
+cudaError_t dh_launch_forward_plane(const DhFourierParams& q, cudaStream_t s);
 int dh_forward_i8_npad(int w);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
@@ -724,6 +725,22 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
         fe = dh_launch_forward_reg(fp, o.stream);
         if (fe == cudaSuccess) { o.lastForwardKernel = 2; return fe; }
         if (fe != cudaErrorNotSupported || mode == 2) return fe;
+        cudaGetLastError();
+    }
+    // windows of 256 pixels and more: through the full planes (the plane
+    // buffer of the Fourier-plane requests, batch-sized)
+    if ((mode == 0 && (1 << fp.logW) >= 256) || mode == 5) {
+        const size_t Nx = (size_t)(1 << fp.logW) / 2 + 1;
+        const size_t need = (size_t)o.batchCount * o.polCount * (1 << fp.logH) * Nx * sizeof(float2);
+        fe = o.dFourier.ensure(need);
+        if (fe != cudaSuccess) return fe;
+        DhFourierParams q;
+        memset(&q, 0, sizeof(q));
+        q.f = fp;
+        q.plane = o.dFourier.as<float2>() + (size_t)fp.frameOffset * o.polCount * (1 << fp.logH) * Nx;
+        fe = dh_launch_forward_plane(q, o.stream);
+        if (fe == cudaSuccess) { o.lastForwardKernel = 5; return fe; }
+        if (fe != cudaErrorNotSupported || mode == 5) return fe;
         cudaGetLastError();
     }
     fe = dh_launch_forward(fp, o.stream);

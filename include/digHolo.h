@@ -337,11 +337,12 @@ int digHoloB200GetGeometry(int handleIdx, int* out10);
  * and alignment allow, else the register kernel, else the generic one),
  * 1 generic shared-memory kernel, 2 register kernel, 3 TMA-fed kernel only,
  * 4 tensor-core row-DFT kernel only (uint16 frames, 128-row FFT windows 64
- * or 128 wide, 16- or 32-pixel IFFT windows; the batch fails where the
- * chosen kernel does not apply). */
+ * or 128 wide, 16- or 32-pixel IFFT windows), 5 full R2C planes (rows, then
+ * columns, then the window; automatic for windows 256 pixels wide or more);
+ * the batch fails where the chosen kernel does not apply. */
 int digHoloB200SetForwardKernel(int handleIdx, int kernel);
 /* Forward kernel the last batch ran: 1 generic, 2 register, 3 TMA-fed,
- * 4 tensor-core row DFT. */
+ * 4 tensor-core row DFT, 5 full planes. */
 int digHoloB200GetForwardKernel(int handleIdx);
 /* Inverse kernel choice (testing aid): 0 automatic (one warp per frame and
  * polarisation for 16- and 32-pixel low-resolution fields; for
