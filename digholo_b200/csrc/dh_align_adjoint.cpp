@@ -42,6 +42,8 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
     if (r) return r;
     const auto t1 = Clock::now();
     const Geometry& g = o.geo;
+    if ((g.w & (g.w - 1)) || (g.h & (g.h - 1)))
+        return fail(o, ERR_INVALIDDIMENSION, "the adjoint AutoAlign needs power-of-two IFFT window sides on this build");
     const int P = o.polCount, B = o.batchCount, G = c.maxMG, M = o.modeCount;
     const int units = B * P;
     const int w = g.w, h = g.h, W = g.W, H = g.H;

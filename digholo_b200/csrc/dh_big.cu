@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(NT, 1) k_field_big(DhInvParams p, BigArgs a) {
     constexpr bool TC = PASS == PASS_TC;
     constexpr bool F32 = PASS == PASS_F32;
     constexpr bool OV = TC || F32;
-    const int W = 1 << p.logW, H = 1 << p.logH, w = 1 << p.logw, h = 1 << p.logh;
+    const int W = 1 << p.logW, H = 1 << p.logH, w = p.w, h = p.h;
     const int TXc = W / SL, TYc = H / SL;
     const int nb = H / BR;
     const int Fx = w / SL, Fy = h / SL;
@@ -544,8 +544,9 @@ size_t alignUp(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // cudaErrorNotSupported outside the kernel's shapes.
 cudaError_t planBig(const DhInvParams& p, int overlapKind, BigPlan& pl) {
     if (p.lowres) return cudaErrorNotSupported;
-    const int W = 1 << p.logW, H = 1 << p.logH, w = 1 << p.logw, h = 1 << p.logh;
+    const int W = 1 << p.logW, H = 1 << p.logH, w = p.w, h = p.h;
     if (W < 64 || H < 64 || W > TW_N || H > TW_N || w < SL || h < SL || w > W || h > H) return cudaErrorNotSupported;
+    if (w % SL || h % SL) return cudaErrorNotSupported;
     const bool ov = p.maxMG > 0 && p.coefs;
     if (ov && p.maxMG > GNMAX) return cudaErrorNotSupported;
     pl.nb = H / BR;

@@ -443,6 +443,7 @@ cudaError_t launchOverlapF32(const DhInvParams& p, int nx, int ny, cudaStream_t 
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s) {
     *fused = 0;
     if (p.lowres || p.logw != p.logh || p.logW != p.logH) return cudaErrorNotSupported;
+    if (p.w != (1 << p.logw) || p.h != (1 << p.logh)) return cudaErrorNotSupported;   // power-of-two windows only
     if (p.frameCount * p.polCount <= 0) return cudaSuccess;
     const int W = 1 << p.logW, w = 1 << p.logw;
     const bool ovl = withOverlap && p.maxMG > 0 && p.coefs && p.maxMG <= 32 && W == 128;

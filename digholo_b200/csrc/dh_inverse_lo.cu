@@ -279,6 +279,7 @@ __global__ void __launch_bounds__(32 * LO_WARPS) k_inverse_lo(DhInvParams p) {
 // Returns cudaErrorNotSupported for shapes this kernel does not cover.
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s) {
     if (!p.lowres || p.logw != p.logh || (p.logw != 4 && p.logw != 5)) return cudaErrorNotSupported;
+    if (p.w != (1 << p.logw) || p.h != (1 << p.logh)) return cudaErrorNotSupported;   // power-of-two windows only
     // the table loads read 16-byte chunks of the int16 modes
     if (p.maxMG > 0 && ((reinterpret_cast<uintptr_t>(p.hgX) | reinterpret_cast<uintptr_t>(p.hgY)) & 15))
         return cudaErrorNotSupported;

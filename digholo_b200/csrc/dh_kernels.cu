@@ -493,6 +493,7 @@ size_t dh_inverse_smem_bytes(const DhInvParams& p) {
 }
 
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
+    if (p.w != (1 << p.logw) || p.h != (1 << p.logh)) return cudaErrorNotSupported;   // power-of-two windows only
     const size_t smem = dh_inverse_smem_bytes(p);
     cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse), (int)smem);
     if (e != cudaSuccess) return e;

@@ -274,8 +274,16 @@ static int checkSupported(Object& o) {
     const Geometry& g = o.geo;
     if (!isPow2(g.W) || !isPow2(g.H) || g.W > 2048 || g.H > 2048)
         return fail(o, ERR_INVALIDDIMENSION, "FFT window sides must be powers of two up to 2048 on this build");
-    if (!isPow2(g.w) || !isPow2(g.h))
-        return fail(o, ERR_INVALIDDIMENSION, "IFFT window sides must be powers of two on this build");
+    // IFFT windows whose sides are multiples of 16 but not powers of two:
+    // full resolution through the full-plane forward and the band kernels
+    // (FFT windows of 256 pixels and more); not in low-resolution mode
+    if (!isPow2(g.w) || !isPow2(g.h)) {
+        const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 256 && g.H >= 64 && g.w % 16 == 0 && g.h % 16 == 0;
+        if (!bands)
+            return fail(o, ERR_INVALIDDIMENSION,
+                        "IFFT window sides that are not powers of two need full resolution (IFFTResolutionMode 0) and an "
+                        "FFT window of at least 256 x 64 on this build");
+    }
     if (o.avgCount != 1) return fail(o, ERR_INVALIDARGUMENT, "frame averaging (avgCount > 1) is not supported on this build");
     return ERR_SUCCESS;
 }
@@ -680,6 +688,7 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
     ip.lowres = o.cfg.resolutionIdx;
     ip.logW = ilog2(g.W); ip.logH = ilog2(g.H);
     ip.logw = ilog2(g.w); ip.logh = ilog2(g.h);
+    ip.w = g.w; ip.h = g.h;
     for (int p = 0; p < o.polCount; p++) { ip.sx0[p] = g.SX[p] - g.W / 2; ip.sy[p] = g.SY[p]; }
     ip.refWave = o.dRef.as<short>();
     ip.refWaveF = o.dRefF.as<float>();

@@ -55,7 +55,8 @@ struct DhInvParams {
     int frameCount, polCount;
     int lowres;             // 1: field is h x w, 0: field is H x W
     int logW, logH;         // FFT window (full-res field) sizes
-    int logw, logh;         // IFFT window sizes
+    int logw, logh;         // IFFT window sizes (ceil log2; exact for power-of-two windows)
+    int w, h;               // IFFT window sides (multiples of 16)
     int sx0[DH_MAXPOL];     // kx column of window column 0 (full-res placement)
     int sy[DH_MAXPOL];      // row origin for full-res placement
     const short* refWave;   // [pol][2*(nx+ny)]: Xr, Xi, Yr, Yi (14-bit ints)

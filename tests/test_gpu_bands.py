@@ -125,3 +125,32 @@ def test_forward_through_full_planes(lib, name, mode):
         assert rel_l2(out[0][1]["window"], o["window"].ravel()) <= 1e-6
     assert max(np.abs(out[0][1]["R"].astype(int) - o["R"]).max(), np.abs(out[0][1]["I"].astype(int) - o["I"]).max()) <= 2
     assert rel_l2(out[0][1]["coefs"], o["coefs"]) <= 1e-4
+
+
+@pytest.mark.parametrize("overlap", [0, 1])
+def test_non_power_of_two_ifft_window(lib, overlap):
+    """A carrier of 0.38 Nyquist with a 256 x 256 FFT window gives a 48 x 48
+    IFFT window.  At full resolution (the reference's default) it runs
+    through the full-plane forward and the band kernels, which fold any
+    multiple of 16 onto 16-point transforms: int16 fields within 2 LSB of the
+    quantised oracle, coefficients relative L2 <= 1e-4 (split-BF16) or 5e-5
+    (FP32).  In low-resolution mode the batch fails with an error."""
+    hol = synth.generate(frame_count=4, frame_width=1280, frame_height=1024, pol_count=2, max_mg=9, waist=640e-6,
+                         snr_db=30, window=(256, 256), dtype="float32", seed=2999, carrier=(0.38, 0.304))
+    cfg = config_for(hol, 0)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    assert o["w"] == 48 and o["h"] == 48
+    h = lib.digHoloCreate()
+    api.configure(lib, h, cfg)
+    assert lib.digHoloB200SetOverlapKernel(h, overlap) == 0
+    g = api.run_batch(lib, h, hol.frames)
+    assert g["coefs"] is not None, lib.digHoloB200GetLastError(h)
+    assert lib.digHoloB200GetForwardKernel(h) == 5 and lib.digHoloB200GetInverseKernel(h) == 4
+    assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
+    assert rel_l2(g["field"], o["field"]) <= 5e-5
+    assert rel_l2(g["coefs"], o["coefs"]) <= (1e-4 if overlap == 0 else 5e-5)
+    cfg1 = config_for(hol, 1)
+    api.configure(lib, h, cfg1)
+    g1 = api.run_batch(lib, h, hol.frames)
+    assert g1["coefs"] is None and lib.digHoloB200GetLastError(h)
+    lib.digHoloDestroy(h)
