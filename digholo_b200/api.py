@@ -16,7 +16,8 @@ def configure(L, h, cfg):
     ``cfg`` needs: frame_width, frame_height, pixel_size, wavelength,
     pol_count, fft_window, window_radius_deg, resolution_mode, max_mg,
     fill_factor, pol_lock_tilt, pol_lock_defocus, pol_lock_waist, and
-    per-polarisation waist, beam_centre, tilt_deg, defocus.
+    per-polarisation waist, beam_centre, tilt_deg, defocus; optionally
+    batch_cal, complex (polCount, batchCount) batch calibration factors.
     """
     L.digHoloConfigSetFrameDimensions(h, int(cfg.frame_width), int(cfg.frame_height))
     L.digHoloConfigSetFramePixelSize(h, float(cfg.pixel_size))
@@ -37,6 +38,10 @@ def configure(L, h, cfg):
         L.digHoloConfigSetTilt(h, 0, p, float(cfg.tilt_deg[p][0]))
         L.digHoloConfigSetTilt(h, 1, p, float(cfg.tilt_deg[p][1]))
         L.digHoloConfigSetDefocus(h, p, float(cfg.defocus[p]))
+    cal = getattr(cfg, "batch_cal", None)
+    if cal is not None:
+        c = np.ascontiguousarray(np.asarray(cal, dtype=np.complex64))
+        L.digHoloConfigSetBatchCalibration(h, c.ctypes.data_as(C.POINTER(C.c_float)), c.shape[0], c.shape[1])
 
 
 def set_batch(L, h, frames):
@@ -47,6 +52,16 @@ def set_batch(L, h, frames):
     if frames.dtype == np.uint16:
         return L.digHoloSetBatchUint16(h, B, ptr(frames, C.c_ushort), 0)
     return L.digHoloSetBatch(h, B, ptr(frames, C.c_float))
+
+
+def set_batch_avg(L, h, frames, avg_count, avg_mode):
+    """digHoloSetBatchAvg / digHoloSetBatchAvgUint16: frames holds batchCount *
+    avg_count frames, averaged in groups of avg_count (avg_mode 0: adjacent
+    frames, 1: interlaced, 2: sweeps)."""
+    B = frames.shape[0] // avg_count
+    if frames.dtype == np.uint16:
+        return L.digHoloSetBatchAvgUint16(h, B, ptr(frames, C.c_ushort), avg_count, avg_mode, 0)
+    return L.digHoloSetBatchAvg(h, B, ptr(frames, C.c_float), avg_count, avg_mode)
 
 
 def read_outputs(L, h, B, coef_ptr=None, m=0, pc=0, want_fields=True):

@@ -210,7 +210,7 @@ float objAutoAlignAdjoint(Object& o) {
         int r0 = objProcessForAlign(o);
         if (r0) return -FLT_MAX;
         if (!o.framesOnDevice) {
-            const size_t bytes = (size_t)o.batchCount * c.frameWidth * c.frameHeight * (o.framesU16 ? 2 : 4);
+            const size_t bytes = (size_t)o.batchCount * std::max(1, o.avgCount) * c.frameWidth * c.frameHeight * (o.framesU16 ? 2 : 4);
             if (o.dAlignFrames.ensure(bytes) != cudaSuccess) return -FLT_MAX;
             if (cudaMemcpy(o.dAlignFrames.ptr, o.frames, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return -FLT_MAX;
             o.frames = o.dAlignFrames.ptr;

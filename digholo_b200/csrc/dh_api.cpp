@@ -511,7 +511,7 @@ int digHoloGetFields16(int h, int* batchCount, int* polCount, short** fieldR, sh
     *fieldR = o->hFieldR.as<short>();
     *fieldI = o->hFieldR.as<short>() + n;
     // DIGHOLO_ANALYSIS[IFFT][MAXABS][pol][batch]
-    *fieldScale = o->hStats.as<float>() + 3 * o->polCount * (o->batchCount + 1);
+    *fieldScale = o->hStats.as<float>() + 3 * o->polCount * (o->batchCount * o->avgCount + 1);
     *x = o->hX.data();
     *y = o->hY.data();
     *width = o->geo.nx;

@@ -564,3 +564,71 @@ cudaError_t dh_launch_batchsum(const short* R, const short* I, const float* stat
     k_batchsum<<<blocks, 256, 0, s>>>(R, I, stats, statsStride, polCount, frameCount, npix, out);
     return cudaGetLastError();
 }
+
+// Frame averaging of the Fourier windows: the two-pass branch of
+// digHoloCopyWindow (digHolo.cpp:1886-1932, 2062-2118) as driven per batch
+// item by digHolo.cpp:8636-8672.  One block per (batch item, polarisation)
+// over the windows of all batch x avg frames: the first frame's window
+// x 1/avg; each further window x the unit phase of sum(acc conj(window))
+// x 1/avg, added.  Frames of batch item b: b avg + k (sequential, mode 0),
+// k batch + b (interlaced, mode 1), b + k (sweeps of one wavelength, mode 2).
+// The batch calibration factor of item b multiplies every window of it in
+// the reference; the alignment phase is blind to a common factor, so it is
+// applied once to the average.  Each thread owns the same pixels in every
+// pass, so only the correlation needs the block.
+__global__ void __launch_bounds__(256) k_average_windows(const float2* __restrict__ in, float2* __restrict__ out,
+                                                         int batch, int avg, int mode, int polCount, int n,
+                                                         const float2* __restrict__ cal, int calCount) {
+    __shared__ double red[2][8];
+    const int b = blockIdx.x / polCount, pol = blockIdx.x - b * polCount;
+    float2* acc = out + ((size_t)b * polCount + pol) * n;
+    const float inv = (float)(1.0 / avg);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    for (int k = 0; k < avg; k++) {
+        const int f = mode == 0 ? b * avg + k : (mode == 1 ? k * batch + b : b + k);
+        const float2* src = in + ((size_t)f * polCount + pol) * n;
+        if (k == 0) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const float2 v = src[i];
+                acc[i] = make_float2(v.x * inv, v.y * inv);
+            }
+            continue;
+        }
+        double cr = 0, ci = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float2 a = acc[i], v = src[i];
+            cr += (double)a.x * v.x + (double)a.y * v.y;
+            ci += (double)a.y * v.x - (double)a.x * v.y;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            cr += __shfl_xor_sync(0xffffffffu, cr, off);
+            ci += __shfl_xor_sync(0xffffffffu, ci, off);
+        }
+        __syncthreads();   // the previous pass has read red
+        if (lane == 0) { red[0][warp] = cr; red[1][warp] = ci; }
+        __syncthreads();
+        cr = 0; ci = 0;
+        for (int w = 0; w < warps; w++) { cr += red[0][w]; ci += red[1][w]; }
+        const double m = sqrt(cr * cr + ci * ci);
+        const float pr = (float)(cr / m) * inv, pi = (float)(ci / m) * inv;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float2 a = acc[i], v = src[i];
+            acc[i] = make_float2(a.x + (v.x * pr - v.y * pi), a.y + (v.x * pi + v.y * pr));
+        }
+    }
+    if (cal && calCount > 0) {
+        const float2 c = cal[pol * calCount + (b % calCount)];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float2 a = acc[i];
+            acc[i] = make_float2(a.x * c.x - a.y * c.y, a.x * c.y + a.y * c.x);
+        }
+    }
+}
+
+cudaError_t dh_launch_average_windows(const float2* in, float2* out, int batch, int avg, int mode, int polCount,
+                                      int n, const float2* cal, int calCount, cudaStream_t s) {
+    if (batch <= 0 || polCount <= 0 || n <= 0) return cudaSuccess;
+    if (avg < 1 || mode < 0 || mode > 2) return cudaErrorInvalidValue;
+    k_average_windows<<<batch * polCount, 256, 0, s>>>(in, out, batch, avg, mode, polCount, n, cal, calCount);
+    return cudaGetLastError();
+}

@@ -35,6 +35,8 @@ cudaError_t dh_launch_fields_to_c64(const short* R, const short* I, const float*
                                     int polCount, int frameCount, int npix, float2* out, cudaStream_t s);
 cudaError_t dh_launch_batchsum(const short* R, const short* I, const float* stats, int statsStride,
                                int polCount, int frameCount, int npix, float* out, cudaStream_t s);
+cudaError_t dh_launch_average_windows(const float2* in, float2* out, int batch, int avg, int mode, int polCount,
+                                      int n, const float2* cal, int calCount, cudaStream_t s);
 
 namespace dh {
 
@@ -284,7 +286,8 @@ static int checkSupported(Object& o) {
                         "IFFT window sides that are not powers of two need full resolution (IFFTResolutionMode 0) and an "
                         "FFT window of at least 256 x 64 on this build");
     }
-    if (o.avgCount != 1) return fail(o, ERR_INVALIDARGUMENT, "frame averaging (avgCount > 1) is not supported on this build");
+    if (o.avgCount < 1 || o.cfg.avgMode < 0 || o.cfg.avgMode > 2)
+        return fail(o, ERR_INVALIDARGUMENT, "frame averaging: avgCount must be at least 1 and avgMode 0, 1 or 2");
     return ERR_SUCCESS;
 }
 
@@ -309,7 +312,7 @@ static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
         return ERR_SUCCESS;
     }
     const size_t frameBytes = (size_t)P * g.H * g.W * es;
-    DH_CUDA(o, o.dFrames.ensure(frameBytes * (size_t)o.batchCount));
+    DH_CUDA(o, o.dFrames.ensure(frameBytes * (size_t)o.batchCount * std::max(1, o.avgCount)));
     for (int p = 0; p < P; p++) {
         cudaMemcpy3DParms m;
         memset(&m, 0, sizeof(m));
@@ -740,7 +743,8 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
     // buffer of the Fourier-plane requests, batch-sized)
     if ((mode == 0 && (1 << fp.logW) >= 256) || mode == 5) {
         const size_t Nx = (size_t)(1 << fp.logW) / 2 + 1;
-        const size_t need = (size_t)o.batchCount * o.polCount * (1 << fp.logH) * Nx * sizeof(float2);
+        const size_t frames = (size_t)std::max(o.batchCount * std::max(1, o.avgCount), fp.frameOffset + fp.frameCount);
+        const size_t need = frames * o.polCount * (1 << fp.logH) * Nx * sizeof(float2);
         fe = o.dFourier.ensure(need);
         if (fe != cudaSuccess) return fe;
         DhFourierParams q;
@@ -888,6 +892,45 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
     return ERR_SUCCESS;
 }
 
+// Frame averaging (avgCount > 1; digHoloSetBatchAvg, digHolo.cpp:8636-8672):
+// the forward stage over all batch x avg frames into a scratch window
+// buffer, the phase-aligned average of each batch item's windows into the
+// window buffer (k_average_windows, with the batch calibration), then the
+// inverse stage over the batch.  The frames must already be staged (fp0).
+static int launchAveraged(Object& o, const DhFwdParams& fp0, const DhInvParams& ip) {
+    const Geometry& g = o.geo;
+    const int B = o.batchCount, A = o.avgCount, P = o.polCount;
+    const size_t n = (size_t)g.w * g.h;
+    DH_CUDA(o, o.dWindowAvg.ensure((size_t)B * A * P * n * sizeof(float2)));
+    DhFwdParams fp = fp0;
+    fp.frameCount = B * A;
+    fp.frameOffset = 0;
+    fp.window = o.dWindowAvg.as<float2>();
+    fp.batchCal = nullptr;   // per batch item, after the average
+    fp.batchCalCount = 0;
+    cudaEvent_t* ev = nullptr;
+    if (o.timing) {
+        if ((int)o.evStage.size() < 3 * (o.evStageUsed + 1)) {
+            for (int i = 0; i < 3; i++) {
+                cudaEvent_t e;
+                DH_CUDA(o, cudaEventCreate(&e));
+                o.evStage.push_back(e);
+            }
+        }
+        ev = &o.evStage[3 * o.evStageUsed];
+        o.evStageUsed++;
+        DH_CUDA(o, cudaEventRecord(ev[0], o.stream));
+    }
+    cudaError_t fe = launchForward(o, fp);
+    if (fe != cudaSuccess) return failCuda(o, fe, "forward kernel launch");
+    DH_CUDA(o, dh_launch_average_windows(fp.window, fp0.window, B, A, o.cfg.avgMode, P, (int)n, fp0.batchCal,
+                                         fp0.batchCalCount, o.stream));
+    if (ev) DH_CUDA(o, cudaEventRecord(ev[1], o.stream));
+    if (ip.fieldR) DH_CUDA(o, launchInverse(o, ip));
+    if (ev) DH_CUDA(o, cudaEventRecord(ev[2], o.stream));
+    return ERR_SUCCESS;
+}
+
 // Sums the forward / inverse kernel times of the batches timed since the
 // last call: out = {forward ms, inverse ms, batch count}; then resets.
 int objStageTimes(Object& o, float* out) {
@@ -959,7 +1002,12 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     DhInvParams ip;
     inverseParams(o, ip, 1);
     // the last stats column (aggregate over the batch) is filled on request
-    if (o.framesOnDevice) {
+    if (o.avgCount > 1) {
+        r = stageFrames(o, 0, B * o.avgCount, fp, 0);
+        if (r) return r;
+        r = launchAveraged(o, fp, ip);
+        if (r) return r;
+    } else if (o.framesOnDevice) {
         r = stageFrames(o, 0, B, fp, 0);
         if (r) return r;
         r = launchChunk(o, fp, ip, 0, B);
@@ -1000,7 +1048,7 @@ static int processBatchLocked(Object& o, int syncCoefs) {
         o.lastFwd.frameStride = (long long)o.cfg.frameWidth * o.cfg.frameHeight;
         for (int p = 0; p < P; p++) { o.lastFwd.cx[p] = g.cx[p]; o.lastFwd.cy[p] = g.cy[p]; }
     }
-    o.lastFwd.frameCount = B;
+    o.lastFwd.frameCount = B * o.avgCount;
     o.lastFwd.frameOffset = 0;
     {
         // the excluded disk of the Fourier-plane analysis: radius 2 k0 sin(aperture)
@@ -1031,6 +1079,8 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     if (a.fftWindowSizeY <= 0) a.fftWindowSizeY = a.frameHeight;
     if (memcmp(&a, &b, sizeof(Config)) != 0)
         return fail(o, ERR_ERROR, "no-alloc path: configuration changed since the handle was prepared");
+    if (o.avgCount > 1)
+        return fail(o, ERR_INVALIDARGUMENT, "no-alloc path: frame averaging (avgCount > 1) needs digHoloProcessBatch");
     const Geometry& g = o.geo;
     const int P = o.polCount;
     if ((size_t)B * P * g.w * g.h * sizeof(float2) > windowBytes)
@@ -1158,12 +1208,12 @@ static int runStages(Object& o, int withInverse, int withOverlap) {
     }
     DhFwdParams fp;
     forwardParams(o, fp);
-    r = stageFrames(o, 0, o.batchCount, fp, 0);
+    r = stageFrames(o, 0, o.batchCount * o.avgCount, fp, 0);
     if (r) return r;
     DhInvParams ip;
     inverseParams(o, ip, withOverlap);
     if (!withInverse) ip.fieldR = nullptr;
-    r = launchChunk(o, fp, ip, 0, o.batchCount);
+    r = o.avgCount > 1 ? launchAveraged(o, fp, ip) : launchChunk(o, fp, ip, 0, o.batchCount);
     if (r) return r;
     DH_CUDA(o, cudaStreamSynchronize(o.stream));
     return ERR_SUCCESS;
@@ -1247,7 +1297,11 @@ int objStatsToHost(Object& o) {
     const Geometry& g = o.geo;
     const size_t npix = (size_t)g.nx * g.ny;
     const size_t n = (size_t)ANALYSIS_COUNT * P * (B + 1);
-    if (!o.hStats.ensure(n * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "host stats buffer");
+    // host layout [parameter][pol][batch x avg + 1] (digHolo.cpp:7619): with
+    // frame averaging the batch entries and the aggregate fill the first B + 1
+    const int SA = B * std::max(1, o.avgCount) + 1;
+    if (!o.hStats.ensure((size_t)ANALYSIS_COUNT * P * SA * sizeof(float)))
+        return fail(o, ERR_MEMORYALLOCATION, "host stats buffer");
     // per polarisation W H floats, the plane in the first nx ny (the reference
     // sizes every batch-sum plane by the FFT window, digHolo.cpp:7655)
     const size_t stride = std::max((size_t)g.W * g.H, npix);
@@ -1289,6 +1343,12 @@ int objStatsToHost(Object& o) {
         memcpy(&s[4 * per + col], &mxIdx, sizeof(int));
         s[5 * per + col] = (float)(dA * (Pw * Pw / e4));
         s[6 * per + col] = (float)(cyw / Pw);
+    }
+    if (SA != S) {   // spread the rows to the averaged stride (last first: the moves go up)
+        for (int r = ANALYSIS_COUNT * P - 1; r >= 0; r--) {
+            memmove(s + (size_t)r * SA, s + (size_t)r * S, S * sizeof(float));
+            memset(s + (size_t)r * SA + S, 0, (SA - S) * sizeof(float));
+        }
     }
     // spread the polarisations to their strides (last first: the moves go up)
     float* sb = o.hBatchSum.as<float>();

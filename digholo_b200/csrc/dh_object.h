@@ -131,6 +131,7 @@ struct Object {
     Config preparedCfg;
     int preparedValid = 0, preparedKeep32 = -1, preparedU16 = -1, batchCalVersion = 0, preparedBatchCal = -1;
     DevBuf dTwiddle, dFrames, dWindow, dFieldR, dFieldI, dField32, dStats, dCoefs;
+    DevBuf dWindowAvg;                  // frame averaging: the windows of all batch x avg frames
     DevBuf dKx, dKy, dX, dY, dRef, dRefF, dTables, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
     // basis cache key
     int basisNx = 0, basisNy = 0, basisMG = 0;

@@ -19,6 +19,7 @@ It restates, step by step, the work of digHoloProcessBatch
   ifft_windows        IFFT window bounds              digHolo.cpp:7868-8048
   ifft_axes           reconstructed-plane axes        digHolo.cpp:8183-8203
   copy_window         Fourier window copy             digHolo.cpp:1808-2122
+  average_windows     frame averaging of windows      digHolo.cpp:8643-8700, 1886-2118
   field_analysis      power / CoM / max / Aeff        digHolo.cpp:2354-2654, 9103-9176
   fourier_analysis    the same on the R2C plane       digHolo.cpp:6931-6980, 8990-9180
   reference_wave      separable tilt/defocus wave     digHolo.cpp:10201-10504
@@ -59,7 +60,7 @@ class Config:
                  fft_window=(0, 0), window_radius_deg=0.4, resolution_mode=0,
                  wavelength=1565e-9, beam_centre=None, tilt_deg=None, defocus=None,
                  waist=None, max_mg=0, fill_factor=1, pol_lock_tilt=0, pol_lock_defocus=0,
-                 pol_lock_waist=1):
+                 pol_lock_waist=1, avg_count=1, avg_mode=0, batch_cal=None):
         self.frame_width = frame_width
         self.frame_height = frame_height
         self.pixel_size = F32(pixel_size)
@@ -79,6 +80,10 @@ class Config:
         self.pol_lock_tilt = pol_lock_tilt
         self.pol_lock_defocus = pol_lock_defocus
         self.pol_lock_waist = pol_lock_waist
+        self.avg_count = avg_count
+        self.avg_mode = avg_mode
+        # digHoloConfigSetBatchCalibration: complex (polCount, batchCount) factors
+        self.batch_cal = None if batch_cal is None else np.asarray(batch_cal, dtype=np.complex64)
         while len(self.beam_centre) < 2:
             self.beam_centre.append([F32(0), F32(0)])
         while len(self.tilt_deg) < 2:
@@ -535,6 +540,50 @@ def overlap(R, I, Hx, Hy, sx, sy, field_scale, max_mg, quantised=True):
     return out
 
 
+def batch_factors(cfg, pol, batch):
+    """Batch calibration factor of each batch item of one polarisation:
+    cal[pol % calPolCount][item % calBatchCount] (digHolo.cpp:8443-8448,
+    8636-8641), or None when no calibration is set."""
+    cal = getattr(cfg, "batch_cal", None)
+    if cal is None:
+        return None
+    row = cal[pol % cal.shape[0]]
+    return np.array([complex(row[b % cal.shape[1]]) for b in range(batch)])
+
+
+def average_windows(win, batch, avg, mode, lowres, W, H, w, h, SX, SY, cal=None):
+    """Frame averaging of the Fourier windows (digHolo.cpp:8643-8700 and the
+    two-pass branch of digHoloCopyWindow, digHolo.cpp:1886-1932, 2062-2118).
+
+    win: (batch * avg, ...) windows of one polarisation in frame order.
+    Frames of batch item b: b * avg + k (mode 0, sequential), k * batch + b
+    (mode 1, interlaced), b + k (mode 2 with one wavelength, as the
+    reference's formula gives).  The first is scaled by 1/avg; each further
+    window is multiplied by the unit phase of sum(acc * conj(window)) over the
+    window pixels and by 1/avg, and added.  In full-resolution mode only the
+    window's pixels enter the correlation, as in the reference.  ``cal``
+    (one factor per batch item) multiplies every window of its item as it is
+    copied (digHolo.cpp:1831-1835, 2007-2008).
+    """
+    out = np.zeros((batch,) + win.shape[1:], dtype=np.complex128)
+    if lowres:
+        sel = (slice(None), slice(None))
+    else:
+        rows = (np.arange(h) + SY + H // 2) % H
+        cols = (np.arange(w) + SX - W // 2) % W
+        sel = (rows[:, None], cols[None, :])
+    for b in range(batch):
+        for k in range(avg):
+            f = b * avg + k if mode == 0 else (k * batch + b if mode == 1 else b + k)
+            wf = win[f] if cal is None else win[f] * cal[b]
+            if k == 0:
+                out[b] = wf / avg
+            else:
+                c = np.sum(out[b][sel] * np.conj(wf[sel]))
+                out[b] = out[b] + wf * (c / abs(c)) / avg
+    return out
+
+
 def r2c_windows(frames, cfg, W, H, cxs, cys):
     """FP64 R2C of each polarisation's FFT window: (B, P, H, W/2+1)."""
     f = np.asarray(frames, dtype=np.float64)
@@ -554,7 +603,8 @@ def process_batch(frames, cfg, quantised=True):
     ``scale`` (B, P), ``coefs`` (B, P, M), ``stats`` per polarisation.
     """
     frames = np.asarray(frames)
-    B = frames.shape[0]
+    avg = int(getattr(cfg, "avg_count", 1) or 1)
+    B = frames.shape[0] // avg
     P = cfg.pol_count
     W, H, cxs, cys = fft_windows(cfg)
     kx, ky = k_axes(W, H, cfg.pixel_size)
@@ -579,6 +629,12 @@ def process_batch(frames, cfg, quantised=True):
     coefs = np.zeros((B, P, M), dtype=np.complex128)
     for pol in range(P):
         win = copy_window(Fplanes[:, pol], cfg, pol, W, H, w, h, SX[pol], SY[pol], cxs[pol], cys[pol], kx, ky)
+        cal = batch_factors(cfg, pol, B)
+        if avg > 1:
+            win = average_windows(win, B, avg, int(getattr(cfg, "avg_mode", 0)), cfg.resolution_mode == 1,
+                                  W, H, w, h, SX[pol], SY[pol], cal)
+        elif cal is not None:
+            win = win * cal[:, None, None]
         windows[:, pol] = win
         E = np.fft.ifft2(win) * (win.shape[-1] * win.shape[-2])
         untilted[:, pol] = E

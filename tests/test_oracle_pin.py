@@ -125,3 +125,52 @@ def test_fourier_analysis_matches_live_reference(workload):
     f = api.read_fourier(L, h)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     check_fourier(o, f, cfg)
+
+
+@pytest.mark.parametrize("res_mode,avg_mode", [(1, 0), (1, 1), (0, 0)])
+def test_frame_averaging_matches_live_reference(res_mode, avg_mode):
+    """Frame averaging (digHoloSetBatchAvg, 3 frames per batch item): the
+    oracle's phase-aligned window average against the reference build."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    import ctypes as C
+    from digholo_b200 import api
+    hol = make_case("plain_320x256_f32_1pol", 6)
+    cfg = config_for(hol, res_mode)
+    cfg.avg_count, cfg.avg_mode = 3, avg_mode
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    frames = np.ascontiguousarray(hol.frames.astype(np.float32))
+    api.set_batch_avg(L, h, frames, 3, avg_mode)
+    b, m, p = C.c_int(), C.c_int(), C.c_int()
+    cp = L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+    r = api.read_outputs(L, h, 2, cp, m.value, p.value, True)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    assert o["R"].shape[0] == 2
+    _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
+
+
+@pytest.mark.parametrize("avg", [1, 3])
+def test_batch_calibration_matches_live_reference(avg):
+    """Batch calibration (digHoloConfigSetBatchCalibration: one complex
+    factor per polarisation and batch item, applied to the Fourier windows),
+    without and with frame averaging: the oracle against the reference build."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    import ctypes as C
+    from digholo_b200 import api
+    hol = make_case("batched_640x512_u16_2pol", 4 * avg)
+    cfg = config_for(hol, 1)
+    rng = np.random.default_rng(11)
+    cfg.batch_cal = (rng.uniform(0.5, 2.0, (2, 3)) * np.exp(1j * rng.uniform(-np.pi, np.pi, (2, 3))))
+    cfg.avg_count, cfg.avg_mode = avg, 0
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    api.set_batch_avg(L, h, np.ascontiguousarray(hol.frames), avg, 0)
+    b, m, p = C.c_int(), C.c_int(), C.c_int()
+    cp = L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+    r = api.read_outputs(L, h, 4, cp, m.value, p.value, True)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
