@@ -43,6 +43,8 @@ def _bind_extensions(lib, out):
         "digHoloB200GetLastError": (_C.c_char_p, [_C.c_int]),
         "digHoloB200SetStream": (_C.c_int, [_C.c_int, _C.c_void_p]),
         "digHoloB200SetTiming": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200SetGraphs": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200GetGraphCount": (_C.c_int, [_C.c_int]),
         "digHoloB200GetStageTimes": (_C.c_int, [_C.c_int, P(_C.c_float)]),
         "digHoloB200GetGeometry": (_C.c_int, [_C.c_int, P(_C.c_int)]),
         "digHoloB200SetForwardKernel": (_C.c_int, [_C.c_int, _C.c_int]),

@@ -62,6 +62,7 @@ int digHoloDestroy(int h) {
         if (o->device >= 0) {
             cudaSetDevice(o->device);
             if (o->stream) cudaStreamSynchronize(o->stream);
+            dh::objReleaseGraphs(*o);
             if (o->stream && !o->userStream) cudaStreamDestroy(o->stream);
             for (auto e : o->evStage) if (e) cudaEventDestroy(e);
             if (o->copyStream) cudaStreamDestroy(o->copyStream);
@@ -681,6 +682,23 @@ int digHoloB200SetTiming(int h, int enable) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     o->timing = enable ? 1 : 0;
     return dh::ERR_SUCCESS;
+}
+// CUDA-graph replay of device-frame batches (on by default): 0 launches
+// every batch directly and releases the captured graphs.
+int digHoloB200SetGraphs(int h, int enable) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    std::lock_guard<std::mutex> guard(o->lock);
+    o->useGraphs = enable ? 1 : 0;
+    o->graphFailures = 0;
+    if (!enable) {
+        if (o->stream) cudaStreamSynchronize(o->stream);
+        dh::objReleaseGraphs(*o);
+    }
+    return dh::ERR_SUCCESS;
+}
+int digHoloB200GetGraphCount(int h) {
+    OBJ_OR(h, 0);
+    return (int)o->graphs.size();
 }
 // Kernel times of the batches processed with timing on since the last call:
 // out[0] forward-kernel ms (sum), out[1] inverse-kernel ms (sum), out[2] count.

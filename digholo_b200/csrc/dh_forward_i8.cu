@@ -212,8 +212,10 @@ __device__ __forceinline__ void groupBar(unsigned id) { asm volatile("bar.sync %
 // columns are inverse-transformed by L threads (the last L-point transforms
 // and the statistics stay inside one warp), the field is rounded to int16,
 // and the separable overlap U[x][n] = sum_y Hy[n][y] V[y][x], c_mn =
-// sum_x Hx[m][x] U[x][n] is spread over the group.  Same arithmetic, in the
-// same order, as k_inverse_lo.  work: at least L (3 L + 3 + G) complex.
+// sum_x Hx[m][x] U[x][n] is spread over the group.  Radix-2 transforms as in
+// k_inverse_lo<32>; the two-launch 16-pixel kernel (k_inverse_lo16q) splits
+// its transforms 4 x 4 and sums in another order, so the two agree to
+// rounding.  work: at least L (3 L + 3 + G) complex.
 template <int L>
 __device__ __forceinline__ void fusedInverse(const DhInvParams& ip, int gt, unsigned barId, int frame, int pol,
                                              const float2* winT, float2* work, float* sclSlot, const float* hxT,

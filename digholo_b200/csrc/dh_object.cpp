@@ -5,9 +5,12 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
@@ -45,17 +48,24 @@ static const double PI_D = 3.14159265358979323846264338327950288;   // digHolo.c
 static const float UNIT_ANGLE = PI_F / 180.0f;                       // digHolo.h:192
 static const int PIXEL_QUANTA = 16;                                  // digHolo.cpp:94
 
+static std::atomic<unsigned long long> g_devBufGeneration{0};
+unsigned long long devBufGeneration() { return g_devBufGeneration.load(std::memory_order_relaxed); }
+
 cudaError_t DevBuf::ensure(size_t n) {
     if (n <= bytes && ptr) return cudaSuccess;
     release();
     if (n == 0) return cudaSuccess;
+    g_devBufGeneration.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaMalloc(&ptr, n);
     if (e != cudaSuccess) { ptr = nullptr; bytes = 0; return e; }
     bytes = n;
     return cudaSuccess;
 }
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        g_devBufGeneration.fetch_add(1, std::memory_order_relaxed);
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -788,7 +798,7 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
     if (o.inverseKernel == 2) return launchBands(o, ip, mayAlloc);
     if (o.inverseKernel == 0 || o.inverseKernel == 3) {   // 3: as 0 where not fused
         cudaError_t e = dh_launch_inverse_lo(ip, o.stream);
-        if (e == cudaSuccess) { o.lastInverseKernel = 2; return e; }
+        if (e == cudaSuccess) { o.lastInverseKernel = 2; o.lastOverlapKernel = 1; return e; }
         if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
         // full resolution: field kernel, then the overlap kernel
@@ -949,6 +959,84 @@ int objStageTimes(Object& o, float* out) {
     return ERR_SUCCESS;
 }
 
+// Releases the captured batch graphs of the object.
+void objReleaseGraphs(Object& o) {
+    for (auto& g : o.graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    o.graphs.clear();
+    o.graphPending.clear();
+}
+
+// Device-resident frames: the batch's forward and inverse launches replayed
+// from a CUDA graph (one cudaGraphLaunch instead of the launch sequence and
+// its host-side checks).  The key holds every argument of those launches
+// (both parameter blocks, the kernel choices, the batch size and the device
+// allocation generation), so a graph is replayed only for launches identical
+// to the ones it captured.  Launches run directly the first time their
+// arguments other than the frame pointer are seen (kernel attributes, tensor
+// maps and scratch buffers are settled then); after that every new frame
+// buffer is captured on first use (a ring of acquisition buffers gets one
+// graph each).  At most eight graphs and eight settled argument sets are kept.
+static int launchBatchDevice(Object& o, const DhFwdParams& fp, const DhInvParams& ip) {
+    const int B = o.batchCount;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!o.useGraphs || o.timing || cudaStreamIsCapturing(o.stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+        return launchChunk(o, fp, ip, 0, B);
+    const int choice[4] = {o.forwardKernel, o.inverseKernel, o.overlapKernel, B};
+    const unsigned long long gen = devBufGeneration();
+    std::vector<unsigned char> key(sizeof(fp) + sizeof(ip) + sizeof(choice) + sizeof(gen));
+    unsigned char* k = key.data();
+    memcpy(k, &fp, sizeof(fp));
+    memcpy(k + sizeof(fp), &ip, sizeof(ip));
+    memcpy(k + sizeof(fp) + sizeof(ip), choice, sizeof(choice));
+    memcpy(k + sizeof(fp) + sizeof(ip) + sizeof(choice), &gen, sizeof(gen));
+    for (auto& g : o.graphs) {
+        if (g.key != key) continue;
+        DH_CUDA(o, cudaGraphLaunch(g.exec, o.stream));
+        o.lastForwardKernel = g.fwdKernel;
+        o.lastInverseKernel = g.invKernel;
+        o.lastOverlapKernel = g.ovlKernel;
+        return ERR_SUCCESS;
+    }
+    // the same launches on other frames have run directly before: capture now
+    std::vector<unsigned char> shape = key;
+    memset(shape.data() + offsetof(DhFwdParams, frames), 0, sizeof(fp.frames));
+    if (std::find(o.graphPending.begin(), o.graphPending.end(), shape) == o.graphPending.end()) {
+        if (o.graphPending.size() >= 8) o.graphPending.erase(o.graphPending.begin());
+        o.graphPending.push_back(std::move(shape));
+        return launchChunk(o, fp, ip, 0, B);
+    }
+    DH_CUDA(o, cudaStreamBeginCapture(o.stream, cudaStreamCaptureModeThreadLocal));
+    const int r = launchChunk(o, fp, ip, 0, B);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(o.stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (r == ERR_SUCCESS && e == cudaSuccess && graph) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (r != ERR_SUCCESS || e != cudaSuccess || !exec) {
+        // nothing of the capture ran: launch directly; give up on graphs
+        // after repeated failures
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (++o.graphFailures >= 3) o.useGraphs = 0;
+        return launchChunk(o, fp, ip, 0, B);
+    }
+    if (o.graphs.size() >= 8) {
+        cudaGraphExecDestroy(o.graphs.front().exec);
+        o.graphs.erase(o.graphs.begin());
+    }
+    Object::BatchGraph g;
+    g.key = std::move(key);
+    g.exec = exec;
+    g.fwdKernel = o.lastForwardKernel;
+    g.invKernel = o.lastInverseKernel;
+    g.ovlKernel = o.lastOverlapKernel;
+    o.graphs.push_back(std::move(g));
+    DH_CUDA(o, cudaGraphLaunch(exec, o.stream));
+    return ERR_SUCCESS;
+}
+
 // Full pipeline for the batch: stage -> forward -> inverse (+overlap).
 // With host frames the batch is split in chunks whose window copies overlap
 // the previous chunk's kernels.
@@ -1010,7 +1098,7 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     } else if (o.framesOnDevice) {
         r = stageFrames(o, 0, B, fp, 0);
         if (r) return r;
-        r = launchChunk(o, fp, ip, 0, B);
+        r = launchBatchDevice(o, fp, ip);
         if (r) return r;
     } else {
         // copies of this call must not overwrite the staging buffer while an

@@ -64,7 +64,9 @@ struct Config {
     int threadCount = 1;
 };
 
-// Grow-only device allocation.
+// Grow-only device allocation.  Every (re)allocation or release advances
+// devBufGeneration(), which invalidates the captured batch graphs.
+unsigned long long devBufGeneration();
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
@@ -125,6 +127,16 @@ struct Object {
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     int userStream = 0;                 // stream supplied by digHoloB200SetStream (not owned)
     int timing = 0;                     // record per-stage events in ProcessBatch
+    // device-frame batches replayed as CUDA graphs (digHoloB200SetGraphs):
+    // key = every launch argument, exec = the captured forward + inverse launches
+    struct BatchGraph {
+        std::vector<unsigned char> key;
+        cudaGraphExec_t exec = nullptr;
+        int fwdKernel = 0, invKernel = 0, ovlKernel = 0;
+    };
+    std::vector<BatchGraph> graphs;
+    std::vector<std::vector<unsigned char>> graphPending;   // settled argument sets (frame pointer zeroed)
+    int useGraphs = 1, graphFailures = 0;
     std::vector<cudaEvent_t> evStage;   // 3 events per timed batch since the last read
     int evStageUsed = 0;
     // inputs of the last prepare(): geometry and uploads are reused while they match
@@ -219,6 +231,7 @@ int objStageTimes(Object& o, float* ms);
 int objUpdateBasis(Object& o);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
+void objReleaseGraphs(Object& o);
 int objInverseAux(Object& o, const float2* window, int frameCount, float2* field32, short* scratchR, short* scratchI,
                   float* scratchStats);
 int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);

@@ -328,6 +328,14 @@ complex64* digHoloB200GetFields32(int handleIdx, int* batchCount, int* polCount,
 int digHoloB200SetTiming(int handleIdx, int enable);
 int digHoloB200GetStageTimes(int handleIdx, float* out3);
 
+/* Batches on device-resident frames replay their forward and inverse
+ * launches from a CUDA graph once the same launch arguments recur (on by
+ * default; the first batch with new arguments runs directly, the second is
+ * captured).  0 launches directly and releases the graphs.  GetGraphCount:
+ * graphs held (at most 8). */
+int digHoloB200SetGraphs(int handleIdx, int enable);
+int digHoloB200GetGraphCount(int handleIdx);
+
 /* Window geometry of the last batch: W, H, w, h, nx, ny, FFT-window corner
  * (x, y) and IFFT-window origin (SX, SY) of polarisation 0. */
 int digHoloB200GetGeometry(int handleIdx, int* out10);

@@ -85,10 +85,12 @@ def test_tensor_core_forward(lib, name, mode):
 def test_fused_forward_inverse(lib, full16):
     """uint16 frames with 16 x 16 low-resolution fields: forward and inverse
     stages in one launch (inverse choice 3, reported as kernel 5) against the two-launch path
-    (tensor-core forward, warp-per-unit inverse; the automatic choice) on
-    the same frames: equal int16 fields and statistics, coefficients within
-    1e-6 relative L2, and the oracle bounds of test_gpu_parity.  12-bit
-    pixels and the full 16-bit range."""
+    (tensor-core forward, 64-thread-per-unit inverse; the automatic choice)
+    on the same frames.  The fused epilogue runs radix-2 transforms, the
+    two-launch inverse a 4 x 4 split, so the two agree to rounding: int16
+    fields within 1 step, field scales within 1e-6 relative, coefficients
+    within 1e-5 relative L2, and both inside the oracle bounds of
+    test_gpu_parity.  12-bit pixels and the full 16-bit range."""
     hol = make_case("batched_640x512_u16_2pol", 16)
     if full16:
         hol.frames = (hol.frames.astype(np.uint32) * 16 + 7).clip(0, 65535).astype(np.uint16)
@@ -105,12 +107,13 @@ def test_fused_forward_inverse(lib, full16):
     kf = lib.digHoloB200GetInverseKernel(h2)
     lib.digHoloDestroy(h2)
     assert ks == (4, 2) and kf == 5
-    np.testing.assert_array_equal(g2["R"], sep["R"])
-    np.testing.assert_array_equal(g2["I"], sep["I"])
-    np.testing.assert_array_equal(g2["summary"], sep["summary"])
+    assert np.abs(g2["R"].astype(int) - sep["R"]).max() <= 1
+    assert np.abs(g2["I"].astype(int) - sep["I"]).max() <= 1
+    assert np.max(np.abs(g2["scale"] - sep["scale"]) / sep["scale"]) <= 1e-6
     d = rel_l2(g2["coefs"], sep["coefs"])
     o = O.process_batch(hol.frames, cfg, quantised=True)
     print("fused vs two launches: coefficient rel L2 %.2e; vs oracle %.2e" % (d, rel_l2(g2["coefs"], o["coefs"])))
-    assert d <= 1e-6
-    assert max(np.abs(g2["R"].astype(int) - o["R"]).max(), np.abs(g2["I"].astype(int) - o["I"]).max()) <= 2
-    assert rel_l2(g2["coefs"], o["coefs"]) <= 5e-5
+    assert d <= 1e-5
+    for g in (g2, sep):
+        assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
+        assert rel_l2(g["coefs"], o["coefs"]) <= 5e-5
