@@ -444,8 +444,8 @@ def main():
     inv_bytes = B * (P * w * hh * 8 + P * nx * ny * 4 + P * M * 8 + 7 * P * 4)
     fwd_name = {1: "k_forward", 2: "k_forward_reg", 3: "k_forward_tma", 4: "k_forward_i8"}.get(
         L.digHoloB200GetForwardKernel(h), "k_forward")
-    inv_name = {1: "k_inverse", 2: "k_inverse_lo", 3: "k_field_full", 4: "k_field_big"}.get(
-        L.digHoloB200GetInverseKernel(h), "k_inverse")
+    inv_name = {1: "k_inverse", 2: "k_inverse_lo16q" if w == 16 else "k_inverse_lo", 3: "k_field_full",
+                4: "k_field_big"}.get(L.digHoloB200GetInverseKernel(h), "k_inverse")
     if fwd_ms >= inv_ms:
         kname, kbytes, kms = fwd_name, fwd_bytes, fwd_ms / max(timed, 1)
     else:
