@@ -67,6 +67,8 @@ int digHoloDestroy(int h) {
             for (auto e : o->evStage) if (e) cudaEventDestroy(e);
             if (o->copyStream) cudaStreamDestroy(o->copyStream);
             for (auto e : o->evCopy) if (e) cudaEventDestroy(e);
+            if (o->copyStream2) cudaStreamDestroy(o->copyStream2);
+            for (auto e : o->evCopy2) if (e) cudaEventDestroy(e);
             if (o->evStart) cudaEventDestroy(o->evStart);
             if (o->evStop) cudaEventDestroy(o->evStop);
             if (o->hStatus) cudaFreeHost(o->hStatus);

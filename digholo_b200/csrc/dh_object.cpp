@@ -255,6 +255,9 @@ int objInitDevice(Object& o) {
     DH_CUDA(o, cudaStreamCreateWithFlags(&o.copyStream, cudaStreamNonBlocking));
     DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy[0], cudaEventDisableTiming));
     DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy[1], cudaEventDisableTiming));
+    DH_CUDA(o, cudaStreamCreateWithFlags(&o.copyStream2, cudaStreamNonBlocking));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy2[0], cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy2[1], cudaEventDisableTiming));
     DH_CUDA(o, cudaEventCreate(&o.evStart));
     DH_CUDA(o, cudaEventCreate(&o.evStop));
     // twiddle(k) = exp(-2 pi i k / 4096), double precision rounded to float
@@ -333,7 +336,7 @@ static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
         m.dstPos = make_cudaPos(0, (size_t)p * g.H, (size_t)f0);
         m.extent = make_cudaExtent((size_t)g.W * es, (size_t)g.H, (size_t)(f1 - f0));
         m.kind = cudaMemcpyHostToDevice;
-        DH_CUDA(o, cudaMemcpy3DAsync(&m, async ? o.copyStream : o.stream));
+        DH_CUDA(o, cudaMemcpy3DAsync(&m, async ? ((p & 1) ? o.copyStream2 : o.copyStream) : o.stream));
     }
     fp.frames = o.dFrames.ptr;
     fp.frameWidth = g.W;
@@ -1105,6 +1108,7 @@ static int processBatchLocked(Object& o, int syncCoefs) {
         // earlier call's kernels may still read it
         DH_CUDA(o, cudaEventRecord(o.evStart, o.stream));
         DH_CUDA(o, cudaStreamWaitEvent(o.copyStream, o.evStart, 0));
+        if (P > 1) DH_CUDA(o, cudaStreamWaitEvent(o.copyStream2, o.evStart, 0));
         const int chunk = std::max(1, std::min(B, (B + 7) / 8));
         int slot = 0;
         for (int f0 = 0; f0 < B; f0 += chunk) {
@@ -1114,6 +1118,10 @@ static int processBatchLocked(Object& o, int syncCoefs) {
             if (r) return r;
             DH_CUDA(o, cudaEventRecord(o.evCopy[slot], o.copyStream));
             DH_CUDA(o, cudaStreamWaitEvent(o.stream, o.evCopy[slot], 0));
+            if (P > 1) {
+                DH_CUDA(o, cudaEventRecord(o.evCopy2[slot], o.copyStream2));
+                DH_CUDA(o, cudaStreamWaitEvent(o.stream, o.evCopy2[slot], 0));
+            }
             r = launchChunk(o, fpc, ip, f0, f1);
             if (r) return r;
             slot ^= 1;

@@ -124,6 +124,10 @@ struct Object {
     cudaStream_t stream = nullptr;
     cudaStream_t copyStream = nullptr;
     cudaEvent_t evCopy[2] = {nullptr, nullptr};
+    // the second polarisation's window copies run on their own stream (a
+    // second DMA queue next to the first)
+    cudaStream_t copyStream2 = nullptr;
+    cudaEvent_t evCopy2[2] = {nullptr, nullptr};
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     int userStream = 0;                 // stream supplied by digHoloB200SetStream (not owned)
     int timing = 0;                     // record per-stage events in ProcessBatch
