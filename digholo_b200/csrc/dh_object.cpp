@@ -291,13 +291,13 @@ static int checkSupported(Object& o) {
         return fail(o, ERR_INVALIDDIMENSION, "FFT window sides must be powers of two up to 2048 on this build");
     // IFFT windows whose sides are multiples of 16 but not powers of two:
     // full resolution through the full-plane forward and the band kernels
-    // (FFT windows of 256 pixels and more); not in low-resolution mode
+    // (FFT windows of at least 64 x 64); not in low-resolution mode
     if (!isPow2(g.w) || !isPow2(g.h)) {
-        const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 256 && g.H >= 64 && g.w % 16 == 0 && g.h % 16 == 0;
+        const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 64 && g.H >= 64 && g.w % 16 == 0 && g.h % 16 == 0;
         if (!bands)
             return fail(o, ERR_INVALIDDIMENSION,
                         "IFFT window sides that are not powers of two need full resolution (IFFTResolutionMode 0) and an "
-                        "FFT window of at least 256 x 64 on this build");
+                        "FFT window of at least 64 x 64 on this build");
     }
     if (o.avgCount < 1 || o.cfg.avgMode < 0 || o.cfg.avgMode > 2)
         return fail(o, ERR_INVALIDARGUMENT, "frame averaging: avgCount must be at least 1 and avgMode 0, 1 or 2");
@@ -752,9 +752,10 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
         if (fe != cudaErrorNotSupported || mode == 2) return fe;
         cudaGetLastError();
     }
-    // windows of 256 pixels and more: through the full planes (the plane
-    // buffer of the Fourier-plane requests, batch-sized)
-    if ((mode == 0 && (1 << fp.logW) >= 256) || mode == 5) {
+    // windows of 256 pixels and more, and IFFT windows whose sides are not
+    // powers of two: through the full planes (the plane buffer of the
+    // Fourier-plane requests, batch-sized)
+    if ((mode == 0 && ((1 << fp.logW) >= 256 || !isPow2(fp.w) || !isPow2(fp.h))) || mode == 5) {
         const size_t Nx = (size_t)(1 << fp.logW) / 2 + 1;
         const size_t frames = (size_t)std::max(o.batchCount * std::max(1, o.avgCount), fp.frameOffset + fp.frameCount);
         const size_t need = frames * o.polCount * (1 << fp.logH) * Nx * sizeof(float2);
@@ -824,7 +825,7 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
         } else {
             cudaGetLastError();
         }
-        if (!ip.lowres && ((1 << ip.logW) > 128 || (1 << ip.logH) > 128)) {
+        if (!ip.lowres && ((1 << ip.logW) > 128 || (1 << ip.logH) > 128 || !isPow2(ip.w) || !isPow2(ip.h))) {
             e = launchBands(o, ip, mayAlloc);
             if (e != cudaErrorNotSupported) return e;
             cudaGetLastError();

@@ -127,19 +127,29 @@ def test_forward_through_full_planes(lib, name, mode):
     assert rel_l2(out[0][1]["coefs"], o["coefs"]) <= 1e-4
 
 
+NONPOW2 = [
+    # frame, FFT window, carrier (fraction of Nyquist), waist -> IFFT window
+    ((1280, 1024), (256, 256), (0.38, 0.304), 640e-6, (48, 48)),
+    ((640, 512), (128, 128), (0.6, 0.48), 320e-6, (48, 48)),
+    ((640, 512), (128, 64), (0.6, 0.48), 320e-6, (48, 32)),
+]
+
+
+@pytest.mark.parametrize("frame,window,carrier,waist,wh", NONPOW2, ids=["256sq_48", "128sq_48", "128x64_48x32"])
 @pytest.mark.parametrize("overlap", [0, 1])
-def test_non_power_of_two_ifft_window(lib, overlap):
-    """A carrier of 0.38 Nyquist with a 256 x 256 FFT window gives a 48 x 48
-    IFFT window.  At full resolution (the reference's default) it runs
-    through the full-plane forward and the band kernels, which fold any
-    multiple of 16 onto 16-point transforms: int16 fields within 2 LSB of the
-    quantised oracle, coefficients relative L2 <= 1e-4 (split-BF16) or 5e-5
-    (FP32).  In low-resolution mode the batch fails with an error."""
-    hol = synth.generate(frame_count=4, frame_width=1280, frame_height=1024, pol_count=2, max_mg=9, waist=640e-6,
-                         snr_db=30, window=(256, 256), dtype="float32", seed=2999, carrier=(0.38, 0.304))
+def test_non_power_of_two_ifft_window(lib, overlap, frame, window, carrier, waist, wh):
+    """Carriers that give IFFT windows whose sides are multiples of 16 but
+    not powers of two (48, for FFT windows of 256 and 128 pixels).  At full
+    resolution (the reference's default) they run through the full-plane
+    forward and the band kernels, which fold any multiple of 16 onto
+    16-point transforms: int16 fields within 2 LSB of the quantised oracle,
+    coefficients relative L2 <= 1e-4 (split-BF16) or 5e-5 (FP32).  In
+    low-resolution mode the batch fails with an error."""
+    hol = synth.generate(frame_count=4, frame_width=frame[0], frame_height=frame[1], pol_count=2, max_mg=9, waist=waist,
+                         snr_db=30, window=window, dtype="float32", seed=2999, carrier=carrier)
     cfg = config_for(hol, 0)
     o = O.process_batch(hol.frames, cfg, quantised=True)
-    assert o["w"] == 48 and o["h"] == 48
+    assert (o["w"], o["h"]) == wh
     h = lib.digHoloCreate()
     api.configure(lib, h, cfg)
     assert lib.digHoloB200SetOverlapKernel(h, overlap) == 0

@@ -59,8 +59,8 @@ def test_uneven_batches_on_one_handle(lib):
         cfg = config_for(hol, mode)
         o = O.process_batch(hol.frames, cfg, quantised=True)
         pow2 = (o["w"] & (o["w"] - 1)) == 0 and (o["h"] & (o["h"] - 1)) == 0
-        # other multiples of 16 run at full resolution with FFT windows of 256 pixels and more
-        supported = pow2 or (mode == 0 and o["W"] >= 256 and o["H"] >= 64)
+        # other multiples of 16 run at full resolution with FFT windows of at least 64 x 64
+        supported = pow2 or (mode == 0 and o["W"] >= 64 and o["H"] >= 64)
         api.configure(lib, h, cfg)
         g = api.run_batch(lib, h, hol.frames)
         if not supported:
