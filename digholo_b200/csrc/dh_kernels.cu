@@ -339,6 +339,200 @@ __global__ void __launch_bounds__(INV_THREADS) k_inverse(DhInvParams p) {
     }
 }
 
+// Low-resolution fields of any size that is a multiple of 16 (48, 80, 96,
+// 112 ...: the sides FFTW transforms directly in the reference, digHolo.cpp:8734),
+// one block per (frame, polarisation): the h x w inverse DFT as two direct
+// passes through shared memory (rows against exp(+2 pi i kx x / w), then
+// columns against exp(+2 pi i ky y / h), twiddles from sincospi in double
+// rounded once), then the statistics, the reference wave, int16 rounding and
+// the separable overlap of k_inverse.
+constexpr int DFT_THREADS = 256;
+
+struct DftSmem {
+    size_t win, tmp, tw, scratch, total;
+};
+__host__ __device__ inline DftSmem dftSmem(int w, int h, int G) {
+    DftSmem s;
+    const size_t plane = sizeof(float2) * (size_t)h * (w + 1);
+    size_t ov = G > 0 ? sizeof(float) * (size_t)G * (w + h) + sizeof(float2) * (size_t)h * G : 0;
+    s.win = 0;
+    s.tmp = plane;
+    s.tw = s.tmp + (plane > ov ? plane : ov);
+    s.scratch = s.tw + sizeof(float2) * (size_t)(w + h);
+    s.total = s.scratch + sizeof(Stat6) * (DFT_THREADS / 32);
+    return s;
+}
+
+__global__ void __launch_bounds__(DFT_THREADS) k_inverse_dft(DhInvParams p) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int unit = blockIdx.x;
+    const int pol = unit % p.polCount;
+    const int frame = unit / p.polCount;
+    const int nx = p.w, ny = p.h;
+    const int npix = nx * ny;
+    const int ld = nx + 1;
+    const int G = p.maxMG > 0 ? p.maxMG : 0;
+    const DftSmem L = dftSmem(nx, ny, G);
+    float2* fld = reinterpret_cast<float2*>(dsm + L.win);    // window, then the field [ny][ld]
+    float2* tmp = reinterpret_cast<float2*>(dsm + L.tmp);    // row transforms [ny][ld]; later the overlap tables
+    float2* twx = reinterpret_cast<float2*>(dsm + L.tw);     // exp(+2 pi i j / nx)
+    float2* twy = twx + nx;                                  // exp(+2 pi i j / ny)
+    Stat6* scratch = reinterpret_cast<Stat6*>(dsm + L.scratch);
+    const float2* win = p.window + (size_t)unit * npix;
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int j = e / nx, c = e - j * nx;
+        fld[j * ld + c] = win[e];
+    }
+    for (int j = threadIdx.x; j < nx + ny; j += blockDim.x) {
+        const bool isx = j < nx;
+        const int k = isx ? j : j - nx, n = isx ? nx : ny;
+        double sv, cv;
+        sincospi(2.0 * (double)k / (double)n, &sv, &cv);
+        twx[j] = make_float2((float)cv, (float)sv);
+    }
+    __syncthreads();
+    // rows: tmp[ky][x] = sum_kx W[ky][kx] exp(+2 pi i kx x / nx)
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int ky = e / nx, x = e - ky * nx;
+        const float2* row = fld + ky * ld;
+        float ar = 0.f, ai = 0.f;
+        int t = 0;
+        for (int kx = 0; kx < nx; kx++) {
+            const float2 a = row[kx], c = twx[t];
+            ar = fmaf(a.x, c.x, fmaf(-a.y, c.y, ar));
+            ai = fmaf(a.x, c.y, fmaf(a.y, c.x, ai));
+            t += x;
+            if (t >= nx) t -= nx;
+        }
+        tmp[ky * ld + x] = make_float2(ar, ai);
+    }
+    __syncthreads();
+    // columns: fld[y][x] = sum_ky tmp[ky][x] exp(+2 pi i ky y / ny)
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int y = e / nx, x = e - y * nx;
+        float ar = 0.f, ai = 0.f;
+        int t = 0;
+        for (int ky = 0; ky < ny; ky++) {
+            const float2 a = tmp[ky * ld + x], c = twy[t];
+            ar = fmaf(a.x, c.x, fmaf(-a.y, c.y, ar));
+            ai = fmaf(a.x, c.y, fmaf(a.y, c.x, ai));
+            t += y;
+            if (t >= ny) t -= ny;
+        }
+        fld[y * ld + x] = make_float2(ar, ai);
+    }
+    __syncthreads();
+
+    // statistics over the untilted field (digHolo.cpp:8866-8870)
+    const float inv = (float)(1.0 / ((double)nx * (double)ny));
+    const float yShift = fabsf((p.yAxis[1] - p.yAxis[0]) * (float)ny);
+    Stat6 st = {0.f, -1, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int y = e / nx, x = e - y * nx;
+        const float2 a = fld[y * ld + x];
+        const float I0 = fmaf(a.x, a.x, a.y * a.y);
+        const float I = I0 * inv;
+        const int idx = 2 * y * nx + x;
+        if (I0 > st.maxI || (I0 == st.maxI && idx > st.maxIdx)) { st.maxI = I0; st.maxIdx = idx; }
+        const float yv = p.yAxis[y];
+        st.P += I;
+        st.cx = fmaf(p.xAxis[x], I, st.cx);
+        st.cy = fmaf(yv, I, st.cy);
+        st.cyw = fmaf(yv + (yv < 0.f ? yShift : 0.f), I, st.cyw);
+        st.e4 = fmaf(I, I, st.e4);
+    }
+    st = blockReduceStat(st, scratch);
+    const float maxAbs = sqrtf(st.maxI);
+    const float scale = (float)(32767.0 / (double)maxAbs);
+    if (threadIdx.x == 0) {
+        const int S = p.statsStride;
+        float* s = p.stats;
+        const int col = pol * S + frame;
+        const int per = p.polCount * S;
+        s[0 * per + col] = st.P;
+        s[1 * per + col] = st.cx / st.P;
+        s[2 * per + col] = st.cy / st.P;
+        s[3 * per + col] = scale;
+        s[4 * per + col] = __int_as_float(st.maxIdx);
+        s[5 * per + col] = p.dA * (st.P * st.P / st.e4);
+        s[6 * per + col] = st.cyw / st.P;
+    }
+
+    // reference wave, -conj(A . ref), int16 rounding (digHolo.cpp:2741-2833)
+    const short* ref = p.refWave + (size_t)pol * 2 * (nx + ny);
+    const float K = (float)(1.0 / (16383.0 * 16383.0));
+    const size_t fieldOff = (size_t)unit * npix;
+    for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+        const int y = e / nx, x = e - y * nx;
+        const int xr = ref[x], xi = ref[nx + x];
+        const int yr = ref[2 * nx + y], yi = ref[2 * nx + ny + y];
+        const float adjR = (float)(yr * xr - yi * xi) * K;
+        const float adjI = (float)(yr * xi + yi * xr) * K;
+        const float2 a = fld[y * ld + x];
+        const float vr = __fsub_rn(__fmul_rn(a.y, adjI), __fmul_rn(a.x, adjR));
+        const float vi = __fadd_rn(__fmul_rn(a.x, adjI), __fmul_rn(a.y, adjR));
+        if (p.field32) {
+            const float* rf = p.refWaveF + (size_t)pol * 2 * (nx + ny);
+            const float2 rx = make_float2(rf[x], rf[nx + x]);
+            const float2 ry = make_float2(rf[2 * nx + y], rf[2 * nx + ny + y]);
+            const float2 v = cmul(a, cmul(ry, rx));
+            p.field32[fieldOff + e] = make_float2(-v.x, v.y);
+        }
+        const short sr = roundSat16(scale * vr);
+        const short si = roundSat16(scale * vi);
+        p.fieldR[fieldOff + e] = sr;
+        p.fieldI[fieldOff + e] = si;
+        fld[y * ld + x] = make_float2((float)sr, (float)si);
+    }
+    if (G <= 0 || !p.coefs) return;   // uniform over the block
+    __syncthreads();
+
+    // separable overlap on the int16 field (digHolo.cpp:2149-2341):
+    // T[y][m] = sum_x F[y][x] Hx[m][x];  c_mn = sum_y Hy[n][y] T[y][m]
+    float* hx = reinterpret_cast<float*>(tmp);   // [G][nx]
+    float* hy = hx + G * nx;                     // [G][ny]
+    float2* T = reinterpret_cast<float2*>(hy + G * ny);   // [ny][G]
+    const short* gx = p.hgX + (size_t)pol * G * nx;
+    const short* gy = p.hgY + (size_t)pol * G * ny;
+    for (int e = threadIdx.x; e < G * nx; e += blockDim.x) hx[e] = (float)gx[e];
+    for (int e = threadIdx.x; e < G * ny; e += blockDim.x) hy[e] = (float)gy[e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < ny * G; e += blockDim.x) {
+        const int m = e / ny, y = e - m * ny;
+        const float2* row = fld + y * ld;
+        const float* hm = hx + m * nx;
+        float ar = 0.f, ai = 0.f;
+        for (int x = 0; x < nx; x++) {
+            const float2 f = row[x];
+            const float hv = hm[x];
+            ar = fmaf(f.x, hv, ar);
+            ai = fmaf(f.y, hv, ai);
+        }
+        T[y * G + m] = make_float2(ar, ai);
+    }
+    __syncthreads();
+    const float fieldScale = 1.0f / scale;
+    const float* sxp = p.hgScaleX + pol * G;
+    const float* syp = p.hgScaleY + pol * G;
+    for (int mode = threadIdx.x; mode < p.modeCount; mode += blockDim.x) {
+        // mode -> (m, n): group g, n = mode - g(g+1)/2, m = g - n (digHolo.cpp:1245-1265)
+        int g = (int)((sqrtf(8.0f * mode + 1.0f) - 1.0f) * 0.5f);
+        while ((g + 1) * (g + 2) / 2 <= mode) g++;
+        while (g * (g + 1) / 2 > mode) g--;
+        const int n = mode - g * (g + 1) / 2;
+        const int m = g - n;
+        const float* hn = hy + n * ny;
+        float cr = 0.f, ci = 0.f;
+        for (int y = 0; y < ny; y++) {
+            const float2 t = T[y * G + m];
+            cr = fmaf(hn[y], t.x, cr);
+            ci = fmaf(hn[y], t.y, ci);
+        }
+        const float ms = (float)((double)sxp[m] * (double)syp[n] * (double)fieldScale);
+        p.coefs[(size_t)frame * p.polCount * p.modeCount + pol * p.modeCount + mode] = make_float2(cr * ms, ci * ms);
+    }
+}
+
 // Up to four axes per launch (one block each); up to 4 samples per thread.
 struct DhBasisJobs {
     DhBasisParams job[4];
@@ -506,6 +700,22 @@ cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
         if (threads > INV_THREADS) threads = INV_THREADS;
     }
     k_inverse<<<(unsigned)(p.frameCount * p.polCount), threads, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+// Shared memory of the low-resolution DFT kernel for w x h fields and maxMG G.
+size_t dh_inverse_dft_smem_bytes(int w, int h, int G) { return dftSmem(w, h, G > 0 ? G : 0).total; }
+
+// Low-resolution fields whose sides are multiples of 16 (any, including the
+// powers of two); cudaErrorNotSupported when the field does not fit shared memory.
+cudaError_t dh_launch_inverse_dft(const DhInvParams& p, cudaStream_t s) {
+    if (!p.lowres || p.w < 16 || p.h < 16 || p.w % 16 || p.h % 16) return cudaErrorNotSupported;
+    const size_t smem = dh_inverse_dft_smem_bytes(p.w, p.h, p.maxMG);
+    if (smem > 227 * 1024) return cudaErrorNotSupported;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_dft), (int)smem);
+    if (e != cudaSuccess) return e;
+    if (p.frameCount * p.polCount <= 0) return cudaSuccess;
+    k_inverse_dft<<<(unsigned)(p.frameCount * p.polCount), DFT_THREADS, smem, s>>>(p);
     return cudaGetLastError();
 }
 

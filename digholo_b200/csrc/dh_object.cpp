@@ -30,6 +30,8 @@ cudaError_t dh_launch_field_big(const DhInvParams& p, int overlapKind, void* scr
                                 int* overlapUsed, cudaStream_t s);
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
+size_t dh_inverse_dft_smem_bytes(int w, int h, int G);
+cudaError_t dh_launch_inverse_dft(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
 cudaError_t dh_launch_untranspose_u16(const unsigned short* in, unsigned short* out, int Nx, int Ny, int frames,
                                       cudaStream_t s);
@@ -290,14 +292,18 @@ static int checkSupported(Object& o) {
     if (!isPow2(g.W) || !isPow2(g.H) || g.W > 2048 || g.H > 2048)
         return fail(o, ERR_INVALIDDIMENSION, "FFT window sides must be powers of two up to 2048 on this build");
     // IFFT windows whose sides are multiples of 16 but not powers of two:
-    // full resolution through the full-plane forward and the band kernels
-    // (FFT windows of at least 64 x 64); not in low-resolution mode
+    // the full-plane forward, then at full resolution the band kernels (FFT
+    // windows of at least 64 x 64), in low-resolution mode the DFT kernel
+    // (fields that fit its shared memory: up to 112 x 112 with 15 mode groups)
     if (!isPow2(g.w) || !isPow2(g.h)) {
-        const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 64 && g.H >= 64 && g.w % 16 == 0 && g.h % 16 == 0;
-        if (!bands)
+        const bool m16 = g.w % 16 == 0 && g.h % 16 == 0;
+        const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 64 && g.H >= 64 && m16;
+        const bool dft = o.cfg.resolutionIdx != 0 && m16 &&
+                         dh_inverse_dft_smem_bytes(g.w, g.h, o.cfg.maxMG) <= 227 * 1024;
+        if (!bands && !dft)
             return fail(o, ERR_INVALIDDIMENSION,
-                        "IFFT window sides that are not powers of two need full resolution (IFFTResolutionMode 0) and an "
-                        "FFT window of at least 64 x 64 on this build");
+                        "IFFT window sides that are not powers of two need an FFT window of at least 64 x 64 at full "
+                        "resolution, or a low-resolution field that fits the DFT kernel's shared memory, on this build");
     }
     if (o.avgCount < 1 || o.cfg.avgMode < 0 || o.cfg.avgMode > 2)
         return fail(o, ERR_INVALIDARGUMENT, "frame averaging: avgCount must be at least 1 and avgMode 0, 1 or 2");
@@ -794,10 +800,11 @@ static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) 
     return e;
 }
 
-// Inverse stage: the warp-per-unit kernel for 16/32-pixel low-resolution
+// Inverse stage: the warp-per-unit kernels for 16/32-pixel low-resolution
 // fields; for full-resolution fields the pruned field kernel (fields up to
 // 128 x 128) followed by the overlap kernel, else the band kernels; else the
-// block-per-unit kernel.
+// block-per-unit kernel; low-resolution fields whose sides are not powers of
+// two: the DFT kernel.
 static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc = true) {
     if (o.inverseKernel == 2) return launchBands(o, ip, mayAlloc);
     if (o.inverseKernel == 0 || o.inverseKernel == 3) {   // 3: as 0 where not fused
@@ -832,7 +839,12 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
         }
     }
     cudaError_t e = dh_launch_inverse(ip, o.stream);
-    if (e == cudaSuccess) { o.lastInverseKernel = 1; o.lastOverlapKernel = 1; }
+    if (e == cudaSuccess) { o.lastInverseKernel = 1; o.lastOverlapKernel = 1; return e; }
+    if (e != cudaErrorNotSupported || !ip.lowres) return e;
+    // low-resolution fields whose sides are not powers of two
+    cudaGetLastError();
+    e = dh_launch_inverse_dft(ip, o.stream);
+    if (e == cudaSuccess) { o.lastInverseKernel = 6; o.lastOverlapKernel = 1; }
     return e;
 }
 

@@ -362,10 +362,12 @@ int digHoloB200GetForwardKernel(int handleIdx);
  * tensor-core forward kernel where it applies (uint16 frames, 16 x 16
  * low-resolution fields: one launch per batch). */
 int digHoloB200SetInverseKernel(int handleIdx, int kernel);
-/* Inverse kernel the last batch ran: 1 block per unit, 2 warp per unit,
- * 3 full-resolution field kernel + overlap kernel, 4 full-resolution bands
- * (statistics pass, quantising pass with the overlap, coefficient sum),
- * 5 fused into the tensor-core forward kernel (inverse choice 3). */
+/* Inverse kernel the last batch ran: 1 block per unit, 2 low-resolution
+ * 16/32-pixel fields (64 threads / one warp per unit), 3 full-resolution
+ * field kernel + overlap kernel, 4 full-resolution bands (statistics pass,
+ * quantising pass with the overlap, coefficient sum), 5 fused into the
+ * tensor-core forward kernel (inverse choice 3), 6 low-resolution fields
+ * whose sides are multiples of 16 but not powers of two (direct DFT). */
 int digHoloB200GetInverseKernel(int handleIdx);
 /* Overlap of full-resolution fields: 0 (default) on the tensor cores in
  * split-BF16 precision (bf16 hi + lo of both int16 operands, three products,

@@ -144,7 +144,8 @@ def test_non_power_of_two_ifft_window(lib, overlap, frame, window, carrier, wais
     forward and the band kernels, which fold any multiple of 16 onto
     16-point transforms: int16 fields within 2 LSB of the quantised oracle,
     coefficients relative L2 <= 1e-4 (split-BF16) or 5e-5 (FP32).  In
-    low-resolution mode the batch fails with an error."""
+    low-resolution mode the field has the window's size and runs through the
+    DFT kernel (inverse kernel 6): the same bounds with the FP32 overlap."""
     hol = synth.generate(frame_count=4, frame_width=frame[0], frame_height=frame[1], pol_count=2, max_mg=9, waist=waist,
                          snr_db=30, window=window, dtype="float32", seed=2999, carrier=carrier)
     cfg = config_for(hol, 0)
@@ -162,5 +163,12 @@ def test_non_power_of_two_ifft_window(lib, overlap, frame, window, carrier, wais
     cfg1 = config_for(hol, 1)
     api.configure(lib, h, cfg1)
     g1 = api.run_batch(lib, h, hol.frames)
-    assert g1["coefs"] is None and lib.digHoloB200GetLastError(h)
+    assert g1["coefs"] is not None, lib.digHoloB200GetLastError(h)
+    assert lib.digHoloB200GetForwardKernel(h) == 5 and lib.digHoloB200GetInverseKernel(h) == 6
+    o1 = O.process_batch(hol.frames, cfg1, quantised=True)
+    assert g1["R"].shape == o1["R"].shape and o1["R"].shape[-2:] == (wh[1], wh[0])
+    assert np.max(np.abs(g1["scale"].T - o1["scale"]) / o1["scale"]) <= 1e-5
+    assert max(np.abs(g1["R"].astype(int) - o1["R"]).max(), np.abs(g1["I"].astype(int) - o1["I"]).max()) <= 2
+    assert rel_l2(g1["field"], o1["field"]) <= 5e-5
+    assert rel_l2(g1["coefs"], o1["coefs"]) <= 5e-5
     lib.digHoloDestroy(h)
