@@ -17,7 +17,8 @@ def configure(L, h, cfg):
     pol_count, fft_window, window_radius_deg, resolution_mode, max_mg,
     fill_factor, pol_lock_tilt, pol_lock_defocus, pol_lock_waist, and
     per-polarisation waist, beam_centre, tilt_deg, defocus; optionally
-    batch_cal, complex (polCount, batchCount) batch calibration factors.
+    batch_cal, complex (polCount, batchCount) batch calibration factors;
+    basis_type (0 HG, 1 LG, 2 custom with basis_custom, complex [in][out]).
     """
     L.digHoloConfigSetFrameDimensions(h, int(cfg.frame_width), int(cfg.frame_height))
     L.digHoloConfigSetFramePixelSize(h, float(cfg.pixel_size))
@@ -38,6 +39,14 @@ def configure(L, h, cfg):
         L.digHoloConfigSetTilt(h, 0, p, float(cfg.tilt_deg[p][0]))
         L.digHoloConfigSetTilt(h, 1, p, float(cfg.tilt_deg[p][1]))
         L.digHoloConfigSetDefocus(h, p, float(cfg.defocus[p]))
+    bt = int(getattr(cfg, "basis_type", 0) or 0)
+    if bt == 1:
+        L.digHoloConfigSetBasisTypeLG(h)
+    elif bt == 2:
+        t = np.ascontiguousarray(np.asarray(cfg.basis_custom, dtype=np.complex64))
+        L.digHoloConfigSetBasisTypeCustom(h, t.shape[0], t.shape[1], t.ctypes.data_as(C.POINTER(C.c_float)))
+    else:
+        L.digHoloConfigSetBasisTypeHG(h)
     cal = getattr(cfg, "batch_cal", None)
     if cal is not None:
         c = np.ascontiguousarray(np.asarray(cal, dtype=np.complex64))

@@ -44,6 +44,8 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
     const Geometry& g = o.geo;
     if ((g.w & (g.w - 1)) || (g.h & (g.h - 1)))
         return fail(o, ERR_INVALIDDIMENSION, "the adjoint AutoAlign needs power-of-two IFFT window sides on this build");
+    if (o.basisActive)
+        return fail(o, ERR_INVALIDARGUMENT, "the adjoint AutoAlign works on Hermite-Gaussian coefficients (basis type 0)");
     const int P = o.polCount, B = o.batchCount, G = c.maxMG, M = o.modeCount;
     const int units = B * P;
     const int w = g.w, h = g.h, W = g.W, H = g.H;

@@ -339,13 +339,27 @@ float digHoloConfigGetBasisWaist(int h, int polIdx) {
     if (polIdx < 0 || polIdx >= dh::POLMAX) return 0.f;
     return o->cfg.waist[polIdx];
 }
-// digHolo.h:1424-1472: only the Hermite-Gaussian basis is on this build's path
+// digHolo.h:1424-1472 / digHolo.cpp:14736-14805, 4750-4765.  The type is
+// stored as given and, like the reference, an unknown type or an invalid
+// custom matrix processes as Hermite-Gaussian; SetBasisType returns the type.
 int digHoloConfigSetBasisTypeHG(int h) { OBJ_OR(h, dh::ERR_INVALIDHANDLE); o->cfg.basisType = 0; return 0; }
+int digHoloConfigSetBasisTypeLG(int h) { OBJ_OR(h, dh::ERR_INVALIDHANDLE); o->cfg.basisType = 1; return 0; }
+int digHoloConfigSetBasisTypeCustom(int h, int modeCountIn, int modeCountOut, complex64* transform) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    if (!transform) return dh::ERR_NULLPOINTER;
+    if (modeCountIn <= 0 || modeCountOut <= 0) return dh::ERR_INVALIDDIMENSION;
+    o->cfg.basisType = 2;
+    const float* t = reinterpret_cast<const float*>(transform);
+    o->basisCustom.assign(t, t + 2 * (size_t)modeCountIn * modeCountOut);
+    o->basisCustomIn = modeCountIn;
+    o->basisCustomOut = modeCountOut;
+    o->basisCustomVersion++;
+    return dh::ERR_SUCCESS;
+}
 int digHoloConfigSetBasisType(int h, int basisType) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
-    if (basisType != 0) return dh::ERR_INVALIDARGUMENT;
-    o->cfg.basisType = 0;
-    return dh::ERR_SUCCESS;
+    o->cfg.basisType = basisType;
+    return basisType;
 }
 int digHoloConfigGetBasisType(int h) { OBJ_OR(h, 0); return o->cfg.basisType; }
 // digHolo.h:1749-1757: accepted for compatibility; work runs on the GPU
@@ -405,7 +419,7 @@ complex64* digHoloProcessBatch(int h, int* batchCount, int* modeCount, int* polC
     const int r = dh::objProcessBatch(*o, 1);
     *batchCount = o->batchCount;
     *polCount = o->polCount;
-    *modeCount = o->modeCount;
+    *modeCount = dh::objOutputModes(*o);
     if (r != dh::ERR_SUCCESS || o->modeCount <= 0) {
         if (r != dh::ERR_SUCCESS) { *batchCount = 0; *polCount = 0; }
         *modeCount = 0;
@@ -473,7 +487,7 @@ complex64* digHoloBasisGetCoefs(int h, int* batchCount, int* modeCount, int* pol
         return nullptr;
     }
     *batchCount = o->batchCount;
-    *modeCount = o->modeCount;
+    *modeCount = dh::objOutputModes(*o);
     *polCount = o->polCount;
     return (complex64*)o->hCoefs.ptr;
 }
@@ -633,9 +647,9 @@ complex64* digHoloB200GetCoefsDevice(int h, int* batchCount, int* modeCount, int
     Object* o = get(h);
     if (!o || o->modeCount <= 0 || !o->dCoefs.ptr) { *batchCount = 0; *modeCount = 0; *polCount = 0; return nullptr; }
     *batchCount = o->batchCount;
-    *modeCount = o->modeCount;
+    *modeCount = dh::objOutputModes(*o);
     *polCount = o->polCount;
-    return o->dCoefs.as<complex64>();
+    return reinterpret_cast<complex64*>(const_cast<float2*>(dh::objOutputCoefs(*o)));
 }
 // Waits for the handle's GPU work; returns a CUDA error as DIGHOLO_ERROR_ERROR.
 int digHoloB200Synchronize(int h) {

@@ -45,7 +45,7 @@ struct Block {
 // Singular values squared (descending) of a block via the eigenvalues of its
 // smaller Gram matrix.
 static int blockSingular2(Object& o, const Block& blk, std::vector<double>& s2) {
-    const int B = o.batchCount, M = o.modeCount, P = o.polCount;
+    const int B = o.batchCount, M = objOutputModes(o), P = o.polCount;
     const size_t aBytes = (size_t)blk.rows * B * sizeof(float2);
     const int rowsGram = blk.rows <= B;
     const int n = rowsGram ? blk.rows : B;
@@ -70,8 +70,8 @@ static int blockSingular2(Object& o, const Block& blk, std::vector<double>& s2) 
 // polarisation is evaluated with non-independent polarisations.
 int powerMeter(Object& o, float* out, int polIdx, int polsIndependent, const float2* other, bool doIL, bool doMDL,
                bool doXtalk, bool mulConj) {
-    const int B = o.batchCount, P = o.polCount, M = o.modeCount;
-    const float2* coefs = o.dCoefs.as<float2>();
+    const int B = o.batchCount, P = o.polCount, M = objOutputModes(o);
+    const float2* coefs = objOutputCoefs(o);
     float il = 0.f, mdl = 0.f;
     for (int i = 0; i < METRIC_COUNT; i++) out[i] = 0.f;
     if (M <= 0 || !coefs) return ERR_NULLPOINTER;
@@ -170,11 +170,11 @@ int powerMeter(Object& o, float* out, int polIdx, int polsIndependent, const flo
                 Nv = svdM;
             }
             totalSignalCount = Mv * Nv * svdCount;
-            for (int i = 0; i < Nv && i < o.modeCount; i++) {
+            for (int i = 0; i < Nv && i < M; i++) {
                 float signal = 0, noise = 0;
                 const int MGin = hgGroup(i) + 1;
                 for (int j = 0; j < Mv; j++) {
-                    const int MGout = hgGroup(j % o.modeCount) + 1;
+                    const int MGout = hgGroup(j % M) + 1;
                     float vr, vi;
                     if (!uu.empty()) {
                         // column-major n x n: element (j, i) at i * n + j
@@ -186,7 +186,7 @@ int powerMeter(Object& o, float* out, int polIdx, int polsIndependent, const flo
                         vr = vi = 0.f;
                     }
                     const float vPwr = vr * vr + vi * vi;
-                    if (i == j || i == (j - o.modeCount)) signal += vPwr;
+                    if (i == j || i == (j - M)) signal += vPwr;
                     else noise += vPwr;
                     if (MGin == MGout) totalSignalMG += vPwr / MGin;
                     else totalNoiseMG += vPwr / MGin;
@@ -457,7 +457,7 @@ float objAutoAlign(Object& o) {
     // device copy of the best coefficients so far (the other polarisation's
     // matrix half when the polarisations are not independent), taken from the
     // first evaluation as digHolo.cpp:12617-12620 does
-    const size_t coefBytes = (size_t)o.batchCount * o.polCount * o.modeCount * sizeof(float2);
+    const size_t coefBytes = (size_t)o.batchCount * o.polCount * objOutputModes(o) * sizeof(float2);
     if (o.dCoefsBackup.ensure(coefBytes) != cudaSuccess) return -FLT_MAX;
     const float2* backup = o.dCoefsBackup.as<float2>();
     bool firstRun = true;
@@ -522,7 +522,7 @@ float objAutoAlign(Object& o) {
                     if (r) return -FLT_MAX;
                     o.alignEvaluations++;
                     if (firstRun) {
-                        cudaMemcpyAsync(o.dCoefsBackup.ptr, o.dCoefs.ptr, coefBytes, cudaMemcpyDeviceToDevice, o.stream);
+                        cudaMemcpyAsync(o.dCoefsBackup.ptr, objOutputCoefs(o), coefBytes, cudaMemcpyDeviceToDevice, o.stream);
                         firstRun = false;
                     }
                     if ((!lock && P > 1) || polsIndependent) {
@@ -542,11 +542,11 @@ float objAutoAlign(Object& o) {
                                 alignmentSave(c, i, best[i]);
                                 memcpy(outBest[i], out[i], sizeof(out[i]));
                                 // keep this polarisation's coefficients as the best so far
-                                cudaMemcpy2DAsync(o.dCoefsBackup.as<float2>() + (size_t)i * o.modeCount,
-                                                  (size_t)o.polCount * o.modeCount * sizeof(float2),
-                                                  o.dCoefs.as<float2>() + (size_t)i * o.modeCount,
-                                                  (size_t)o.polCount * o.modeCount * sizeof(float2),
-                                                  (size_t)o.modeCount * sizeof(float2), o.batchCount,
+                                cudaMemcpy2DAsync(o.dCoefsBackup.as<float2>() + (size_t)i * objOutputModes(o),
+                                                  (size_t)o.polCount * objOutputModes(o) * sizeof(float2),
+                                                  objOutputCoefs(o) + (size_t)i * objOutputModes(o),
+                                                  (size_t)o.polCount * objOutputModes(o) * sizeof(float2),
+                                                  (size_t)objOutputModes(o) * sizeof(float2), o.batchCount,
                                                   cudaMemcpyDeviceToDevice, o.stream);
                                 bestPwr[i] = pwr;
                             }
@@ -590,12 +590,12 @@ float objAutoAlign(Object& o) {
             if (r) return -FLT_MAX;
             o.alignEvaluations++;
             if (firstRun) {
-                cudaMemcpyAsync(o.dCoefsBackup.ptr, o.dCoefs.ptr, coefBytes, cudaMemcpyDeviceToDevice, o.stream);
+                cudaMemcpyAsync(o.dCoefsBackup.ptr, objOutputCoefs(o), coefBytes, cudaMemcpyDeviceToDevice, o.stream);
                 firstRun = false;
             }
             r = powerMeterDB(o, outf, 1, polsIndependent, nullptr, true, true, true, mulConj);
             if (r) return -FLT_MAX;
-            cudaMemcpyAsync(o.dCoefsBackup.ptr, o.dCoefs.ptr, coefBytes, cudaMemcpyDeviceToDevice, o.stream);
+            cudaMemcpyAsync(o.dCoefsBackup.ptr, objOutputCoefs(o), coefBytes, cudaMemcpyDeviceToDevice, o.stream);
             float dErr = 0;
             for (int p = 0; p < P; p++) {
                 dErr += std::fabs(outBest[p][goalIdx] - lastErr[p]);

@@ -842,3 +842,40 @@ cudaError_t dh_launch_average_windows(const float2* in, float2* out, int batch, 
     k_average_windows<<<batch * polCount, 256, 0, s>>>(in, out, batch, avg, mode, polCount, n, cal, calCount);
     return cudaGetLastError();
 }
+
+// Coefficients in another basis (digHoloApplyBasisTransform,
+// digHolo.cpp:9469-9600): per (batch item, polarisation) out[j] =
+// sum_{i < din} T[i][j] in[i] for j < dout, T [din][dout] complex, no
+// conjugation (the reference's cgemv, no transpose, of the column-major
+// [dout x din] matrix).  One block per row; the input row staged in shared
+// memory, consecutive threads on consecutive outputs.
+__global__ void __launch_bounds__(128) k_basis_transform(const float2* __restrict__ in, float2* __restrict__ out,
+                                                         const float2* __restrict__ T, int M, int din, int dout) {
+    extern __shared__ float2 xrow[];
+    const int row = blockIdx.x;   // batch item x polarisation
+    const float2* x = in + (size_t)row * M;
+    for (int i = threadIdx.x; i < din; i += blockDim.x) xrow[i] = x[i];
+    __syncthreads();
+    for (int j = threadIdx.x; j < dout; j += blockDim.x) {
+        float ar = 0.f, ai = 0.f;
+        for (int i = 0; i < din; i++) {
+            const float2 t = T[(size_t)i * dout + j], v = xrow[i];
+            ar = fmaf(v.x, t.x, fmaf(-v.y, t.y, ar));
+            ai = fmaf(v.x, t.y, fmaf(v.y, t.x, ai));
+        }
+        out[(size_t)row * dout + j] = make_float2(ar, ai);
+    }
+}
+
+cudaError_t dh_launch_basis_transform(const float2* in, float2* out, const float2* T, int rows, int M, int din, int dout,
+                                      cudaStream_t s) {
+    if (rows <= 0 || dout <= 0) return cudaSuccess;
+    if (din < 1 || din > M) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float2) * (size_t)din;
+    if (smem > 48 * 1024) {
+        cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_basis_transform), (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_basis_transform<<<(unsigned)rows, 128, smem, s>>>(in, out, T, M, din, dout);
+    return cudaGetLastError();
+}

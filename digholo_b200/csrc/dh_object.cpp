@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstddef>
 #include <cstring>
+#include <vector>
 
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
 cudaError_t dh_launch_forward(const DhFwdParams& p, cudaStream_t s);
@@ -31,6 +32,8 @@ cudaError_t dh_launch_field_big(const DhInvParams& p, int overlapKind, void* scr
 size_t dh_inverse_smem_bytes(const DhInvParams& p);
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s);
 size_t dh_inverse_dft_smem_bytes(int w, int h, int G);
+cudaError_t dh_launch_basis_transform(const float2* in, float2* out, const float2* T, int rows, int M, int din, int dout,
+                                      cudaStream_t s);
 cudaError_t dh_launch_inverse_dft(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
 cudaError_t dh_launch_untranspose_u16(const unsigned short* in, unsigned short* out, int Nx, int Ny, int frames,
@@ -975,6 +978,101 @@ int objStageTimes(Object& o, float* out) {
     return ERR_SUCCESS;
 }
 
+// HG -> LG transform of G mode groups, T[i * M + j] (HG mode i, LG mode j),
+// block-diagonal by group (digHoloLGInit, digHolo.cpp:9909-10040, with the
+// weights of digHoloLGtoHGcoef, digHolo.cpp:9819-9907: the Beijersbergen
+// mode-converter expansion).  Group g holds HG (g - c, c) at position c and
+// LG l = g - 2r, p = (g - |l|) / 2 at position r; with (n, m) = (p, p - l)
+// for l < 0, else (l + p, p), the weight of HG (hm, hn) is
+// [t^hm] (1 + t)^n (1 - t)^m * sqrt(hm! hn! / (n! m! 2^g)) * i^(g + hm),
+// negated for odd g and l > 0; FP64, rounded once to complex64.
+static void lgTransform(int G, std::vector<float2>& T) {
+    const int M = G * (G + 1) / 2;
+    T.assign((size_t)M * M, make_float2(0.f, 0.f));
+    std::vector<double> poly, lf(2 * G + 2, 0.0);
+    for (int k = 1; k < (int)lf.size(); k++) lf[k] = lf[k - 1] + std::log((double)k);   // log k!
+    int base = 0;
+    for (int g = 0; g < G; g++) {
+        for (int r = 0; r <= g; r++) {
+            const int l = g - 2 * r, p = (g - std::abs(l)) / 2;
+            const int n = l < 0 ? p : l + p, m = l < 0 ? p - l : p;
+            // (1 + t)^n (1 - t)^m, exact in double for the group sizes here
+            poly.assign(1, 1.0);
+            for (int k = 0; k < n + m; k++) {
+                const double sgn = k < n ? 1.0 : -1.0;
+                poly.push_back(0.0);
+                for (int e = (int)poly.size() - 1; e >= 1; e--) poly[e] += sgn * poly[e - 1];
+            }
+            for (int c = 0; c <= g; c++) {
+                const int hm = g - c, hn = c;
+                const double puv = hm < (int)poly.size() ? poly[hm] : 0.0;
+                double v = puv * std::exp(0.5 * (lf[hm] + lf[hn] - lf[n] - lf[m]) - 0.5 * g * std::log(2.0));
+                if ((g & 1) && l > 0) v = -v;
+                const int q = (g + hm) & 3;   // i^q
+                const float2 w = q == 0 ? make_float2((float)v, 0.f)
+                                 : q == 1 ? make_float2(0.f, (float)v)
+                                 : q == 2 ? make_float2((float)-v, 0.f)
+                                          : make_float2(0.f, (float)-v);
+                T[(size_t)(base + c) * M + (base + r)] = w;
+            }
+        }
+        base += g + 1;
+    }
+}
+
+const float2* objOutputCoefs(const Object& o) {
+    return o.basisActive ? o.dCoefsOut.as<float2>() : o.dCoefs.as<float2>();
+}
+int objOutputModes(const Object& o) { return o.basisActive ? o.modeCountOut : o.modeCount; }
+
+// The coefficients in the configured basis (digHoloApplyBasisTransform,
+// digHolo.cpp:9469-9600): HG for type 0, an unknown type or an invalid
+// custom matrix; LG (type 1) over all modes; custom (type 2): the leading
+// min(M, in) x min(M, out) block of the [in][out] matrix, min(M, out) modes
+// out.  The device matrix is rebuilt when the type, the mode count or the
+// custom matrix changes (after the stream has drained: a batch in flight may
+// still read the previous one).
+static int applyBasis(Object& o) {
+    const int M = o.modeCount;
+    int t = o.cfg.basisType;
+    if (t < 0 || t > 2 || (t == 2 && (o.basisCustom.empty() || o.basisCustomIn <= 0 || o.basisCustomOut <= 0))) t = 0;
+    o.basisActive = 0;
+    o.modeCountOut = M;
+    if (t == 0 || M <= 0 || !o.dCoefs.ptr) return ERR_SUCCESS;
+    const int din = t == 1 ? M : std::min(M, o.basisCustomIn);
+    const int dout = t == 1 ? M : std::min(M, o.basisCustomOut);
+    if (o.basisTType != t || o.basisTModes != M || (t == 2 && o.basisTVersion != o.basisCustomVersion)) {
+        std::vector<float2> T;
+        if (t == 1) {
+            int G = 0;
+            while ((G + 1) * (G + 2) / 2 <= M) G++;
+            lgTransform(G, T);
+        } else {
+            T.resize((size_t)din * dout);
+            const float* full = o.basisCustom.data();
+            for (int i = 0; i < din; i++)
+                for (int j = 0; j < dout; j++) {
+                    const size_t src = 2 * ((size_t)i * o.basisCustomOut + j);
+                    T[(size_t)i * dout + j] = make_float2(full[src], full[src + 1]);
+                }
+        }
+        DH_CUDA(o, cudaStreamSynchronize(o.stream));
+        DH_CUDA(o, o.dBasisT.ensure(T.size() * sizeof(float2)));
+        DH_CUDA(o, cudaMemcpy(o.dBasisT.ptr, T.data(), T.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        o.basisTType = t;
+        o.basisTModes = M;
+        o.basisTVersion = o.basisCustomVersion;
+    }
+    const int rows = o.batchCount * o.polCount;
+    DH_CUDA(o, o.dCoefsOut.ensure((size_t)rows * dout * sizeof(float2)));
+    DH_CUDA(o, dh_launch_basis_transform(o.dCoefs.as<float2>(), o.dCoefsOut.as<float2>(), o.dBasisT.as<float2>(), rows,
+                                         M, din, dout, o.stream));
+    o.basisActive = t;
+    o.basisDimIn = din;
+    o.modeCountOut = dout;
+    return ERR_SUCCESS;
+}
+
 // Releases the captured batch graphs of the object.
 void objReleaseGraphs(Object& o) {
     for (auto& g : o.graphs)
@@ -1143,6 +1241,8 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     o.processedFFT = o.processedIFFT = o.processedTilt = 1;
     o.processedOverlap = o.modeCount > 0;
     o.metricsValid = 0;
+    r = applyBasis(o);
+    if (r) return r;
     (void)g;
     // the frame source of this batch, for the Fourier planes on request
     o.lastFwd = fp;
@@ -1190,6 +1290,8 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
         return fail(o, ERR_ERROR, "no-alloc path: configuration changed since the handle was prepared");
     if (o.avgCount > 1)
         return fail(o, ERR_INVALIDARGUMENT, "no-alloc path: frame averaging (avgCount > 1) needs digHoloProcessBatch");
+    if (o.cfg.basisType == 1 || (o.cfg.basisType == 2 && !o.basisCustom.empty()))
+        return fail(o, ERR_INVALIDARGUMENT, "no-alloc path: returns Hermite-Gaussian coefficients only (basis type 0)");
     const Geometry& g = o.geo;
     const int P = o.polCount;
     if ((size_t)B * P * g.w * g.h * sizeof(float2) > windowBytes)
@@ -1286,9 +1388,9 @@ int objCoefsToHost(Object& o) {
         DH_CUDA(o, cudaStreamSynchronize(o.stream));
         return objCheckStatus(o);
     }
-    const size_t n = (size_t)o.batchCount * o.polCount * o.modeCount * sizeof(float2);
+    const size_t n = (size_t)o.batchCount * o.polCount * objOutputModes(o) * sizeof(float2);
     if (!o.hCoefs.ensure(n)) return fail(o, ERR_MEMORYALLOCATION, "host coefficient buffer");
-    DH_CUDA(o, cudaMemcpyAsync(o.hCoefs.ptr, o.dCoefs.ptr, n, cudaMemcpyDeviceToHost, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.hCoefs.ptr, objOutputCoefs(o), n, cudaMemcpyDeviceToHost, o.stream));
     DH_CUDA(o, cudaStreamSynchronize(o.stream));
     return objCheckStatus(o);
 }
@@ -1324,6 +1426,10 @@ static int runStages(Object& o, int withInverse, int withOverlap) {
     if (!withInverse) ip.fieldR = nullptr;
     r = o.avgCount > 1 ? launchAveraged(o, fp, ip) : launchChunk(o, fp, ip, 0, o.batchCount);
     if (r) return r;
+    if (withOverlap) {
+        r = applyBasis(o);
+        if (r) return r;
+    }
     DH_CUDA(o, cudaStreamSynchronize(o.stream));
     return ERR_SUCCESS;
 }

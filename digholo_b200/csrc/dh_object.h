@@ -148,6 +148,16 @@ struct Object {
     int preparedValid = 0, preparedKeep32 = -1, preparedU16 = -1, batchCalVersion = 0, preparedBatchCal = -1;
     DevBuf dTwiddle, dFrames, dWindow, dFieldR, dFieldI, dField32, dStats, dCoefs;
     DevBuf dWindowAvg;                  // frame averaging: the windows of all batch x avg frames
+    // output basis (digHoloConfigSetBasisType*): the custom matrix as given
+    // ([in][out] complex), the device matrix of the active transform
+    // ([dimIn][dimOut]) with the settings it was built for, and the
+    // coefficients in that basis [batch][pol][modeCountOut]
+    std::vector<float> basisCustom;
+    int basisCustomIn = 0, basisCustomOut = 0, basisCustomVersion = 0;
+    DevBuf dBasisT, dCoefsOut;
+    int basisTType = -1, basisTModes = -1, basisTVersion = -1, basisDimIn = 0;
+    int basisActive = 0;                // 0 HG (the overlap's coefficients), 1 LG, 2 custom
+    int modeCountOut = 0;
     DevBuf dKx, dKy, dX, dY, dRef, dRefF, dTables, dHgX, dHgY, dHgScaleX, dHgScaleY, dBasisAxis, dBatchCal, dFieldsC64;
     // basis cache key
     int basisNx = 0, basisNy = 0, basisMG = 0;
@@ -236,6 +246,10 @@ int objUpdateBasis(Object& o);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
 void objReleaseGraphs(Object& o);
+// The coefficients the API returns: in the configured basis after a batch
+// (modeCountOut modes per polarisation), else the HG coefficients.
+const float2* objOutputCoefs(const Object& o);
+int objOutputModes(const Object& o);
 int objInverseAux(Object& o, const float2* window, int frameCount, float2* field32, short* scratchR, short* scratchI,
                   float* scratchStats);
 int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);

@@ -253,7 +253,12 @@ int digHoloConfigSetBasisWaist(int handleIdx, int polIdx, float waist);
 float digHoloConfigGetBasisWaist(int handleIdx, int polIdx);
 /* replaces digHolo.h:1424 */
 int digHoloConfigSetBasisTypeHG(int handleIdx);
-/* replaces digHolo.h:1464 */
+/* replaces digHolo.h:1435: coefficients returned in the Laguerre-Gaussian basis */
+int digHoloConfigSetBasisTypeLG(int handleIdx);
+/* replaces digHolo.h:1453: coefficients returned in a custom basis; transform is
+ * [modeCountIn][modeCountOut] complex (copied), HG mode i onto custom mode j */
+int digHoloConfigSetBasisTypeCustom(int handleIdx, int modeCountIn, int modeCountOut, complex64* transform);
+/* replaces digHolo.h:1464: returns the type set (0 HG, 1 LG, 2 custom) */
 int digHoloConfigSetBasisType(int handleIdx, int basisType);
 /* replaces digHolo.h:1472 */
 int digHoloConfigGetBasisType(int handleIdx);

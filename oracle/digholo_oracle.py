@@ -661,7 +661,75 @@ def process_batch(frames, cfg, quantised=True):
                 coefs[:, pol] = overlap(V.real, V.imag, Hx, Hy, sx, sy, np.ones(B), cfg.max_mg, False)
     res.update(window=windows, field_untilted=untilted, field=field, field_v=field_v,
                R=Rs, I=Is, scale=scales, coefs=coefs, stats=stats)
+    if M:
+        res["coefs_out"] = transform_coefs(coefs, cfg)
     return res
+
+
+# ---------------------------------------------------------------- basis transforms
+
+def lg_transform(G):
+    """HG -> LG transform of the modes of G groups, (M, M) complex with
+    T[i, j] the weight of HG mode i in LG mode j (digHoloLGInit,
+    digHolo.cpp:9909-10040, and digHoloLGtoHGcoef, digHolo.cpp:9819-9907,
+    the Beijersbergen mode-converter expansion).  Group g holds HG (g - c, c)
+    at position c and LG l = g - 2r, p = (g - |l|) / 2 at position r.  With
+    (n, m) = (p, p - l) for l < 0, else (l + p, p), the weight of HG (hm, hn) is
+    [t^hm] (1 + t)^n (1 - t)^m * sqrt(hm! hn! / (n! m! 2^g)) * i^(g + hm),
+    negated for odd g and l > 0.  Computed in FP64 and rounded to complex64,
+    as the reference stores it."""
+    M = G * (G + 1) // 2
+    T = np.zeros((M, M), dtype=np.complex128)
+    base = 0
+    for g in range(G):
+        for r in range(g + 1):
+            l = g - 2 * r
+            p = (g - abs(l)) // 2
+            n, m = (p, p - l) if l < 0 else (l + p, p)
+            poly = np.array([1.0])
+            for _ in range(n):
+                poly = np.convolve(poly, [1.0, 1.0])
+            for _ in range(m):
+                poly = np.convolve(poly, [1.0, -1.0])
+            for c in range(g + 1):
+                hm, hn = g - c, c
+                puv = poly[hm] if hm < poly.size else 0.0
+                b = math.sqrt(math.factorial(hm) * math.factorial(hn) / (math.factorial(n) * math.factorial(m)))
+                v = puv * b * 2.0 ** (-0.5 * g)
+                if g % 2 and l > 0:
+                    v = -v
+                T[base + c, base + r] = v * (1j ** ((g + hm) % 4))
+        base += g + 1
+    return T.astype(np.complex64).astype(np.complex128)
+
+
+def basis_matrix(cfg, M):
+    """The active transform (digHoloApplyBasisTransform, digHolo.cpp:9469-9562):
+    None for HG (type 0, an unknown type, or an invalid custom matrix), the LG
+    matrix for type 1, for type 2 the leading min(M, in) x min(M, out) block of
+    the custom [in][out] matrix."""
+    t = int(getattr(cfg, "basis_type", 0) or 0)
+    if t == 1:
+        G = int(round((math.sqrt(8 * M + 1) - 1) / 2))
+        return lg_transform(G)
+    if t == 2:
+        full = getattr(cfg, "basis_custom", None)
+        if full is None or full.size == 0:
+            return None
+        full = np.asarray(full, dtype=np.complex64).astype(np.complex128)
+        return full[:min(M, full.shape[0]), :min(M, full.shape[1])]
+    return None
+
+
+def transform_coefs(coefs, cfg):
+    """Coefficients in the configured basis: (B, P, modeCountOut), each
+    polarisation's HG coefficients times the transform (applyBasisTransform /
+    HGtoLG, digHolo.cpp:5000-5037, 9565-9600: no conjugation)."""
+    B, P, M = coefs.shape
+    T = basis_matrix(cfg, M)
+    if T is None:
+        return coefs
+    return np.einsum("bpi,ij->bpj", coefs[:, :, :T.shape[0]], T)
 
 
 def reference_unscaled_16(coefs, cfg, res):

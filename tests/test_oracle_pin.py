@@ -174,3 +174,39 @@ def test_batch_calibration_matches_live_reference(avg):
     r = api.read_outputs(L, h, 4, cp, m.value, p.value, True)
     o = O.process_batch(hol.frames, cfg, quantised=True)
     _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
+
+
+@pytest.mark.parametrize("basis", ["lg", "custom"])
+def test_basis_transform_matches_live_reference(basis):
+    """Coefficients in the Laguerre-Gaussian basis and in a custom basis
+    (digHoloConfigSetBasisTypeLG / Custom, 45 HG modes onto 30 custom modes):
+    the oracle's transform of its HG coefficients against the reference
+    build's returned coefficients (full resolution: no unscaled 16-row case)."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    import ctypes as C
+    from digholo_b200 import api
+    hol = make_case("plain_320x256_f32_1pol", 8)
+    cfg = config_for(hol, 0)
+    if basis == "lg":
+        cfg.basis_type = 1
+    else:
+        rng = np.random.default_rng(5)
+        cfg.basis_type = 2
+        cfg.basis_custom = (rng.normal(size=(50, 30)) + 1j * rng.normal(size=(50, 30))).astype(np.complex64)
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    frames = np.ascontiguousarray(hol.frames.astype(np.float32))
+    api.set_batch(L, h, frames)
+    b, m, p = C.c_int(), C.c_int(), C.c_int()
+    cp = L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    co = o["coefs_out"]
+    assert m.value == co.shape[2] and b.value == co.shape[0]
+    r = np.ctypeslib.as_array(cp, shape=(b.value * m.value * p.value * 2,)).copy().view(np.complex64).reshape(co.shape)
+    assert rel_l2(r, co) <= 2e-5
+    if basis == "lg":
+        # the LG transform is unitary: the power per frame is unchanged
+        np.testing.assert_allclose(np.sum(np.abs(co) ** 2, axis=(1, 2)), np.sum(np.abs(o["coefs"]) ** 2, axis=(1, 2)),
+                                   rtol=1e-6)
