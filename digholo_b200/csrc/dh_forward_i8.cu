@@ -448,6 +448,31 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
     const int frame0 = blockIdx.x / P;
     const int nIt = frame0 < p.frameCount ? (p.frameCount - frame0 + frameStep - 1) / frameStep : 0;
 
+    const int rowsPerFrame = (int)(p.frameStride / p.frameWidth);
+    int pre = 0;   // frame tiles issued by thread 0 before the block barrier
+    if (tid == 0) {
+        for (int s = 0; s < NA; s++) { mbarInitN(&full[s], 1); mbarInitN(&empty[s], 1); }
+        for (int g = 0; g < NG; g++) { mbarInitN(&accFull[g], 1); mbarInitN(&accEmpty[g], 1); }
+        mbarInitN(bLoad, 1);
+        mbarInitN(drain, 1);
+        *abortFlag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        // the digit table and the first NA frame tiles go out before the
+        // window tables are staged and the block synchronises: their latency
+        // overlaps the prologue (thread 0 is the TMA producer below)
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmap)) : "memory");
+        tc::fenceProxyAsync();
+        tc::mbarExpectTxTc(bLoad, 4 * BQ);
+        tc::bulkLoad(bBuf, p.dftDigits + (size_t)pol * 4 * BQ, 4 * BQ, bLoad);
+        for (; pre < NA && pre < nIt; pre++) {
+            const int frame = frame0 + pre * frameStep;
+            unsigned char* dst = aBuf + (size_t)pre * ABYTES;
+            tc::mbarExpectTxTc(&full[pre], ABYTES);
+#pragma unroll
+            for (int a = 0; a < NATOM; a++)
+                tmaLoad2D(dst + (size_t)a * H * 128, &tmap, p.cx[pol] + a * 64, frame * rowsPerFrame + p.cy[pol], &full[pre]);
+        }
+    }
     for (int e = tid; e < h * Q; e += NT) tCol[e] = p.tabCol[(size_t)pol * h * Q + e];
     for (int e = tid; e < h * w; e += NT) tAdj[e] = p.tabAdj[(size_t)pol * h * w + e];
     if (FUSE) {
@@ -466,14 +491,6 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
             hsT[P * GI + e] = ip.hgScaleY[e];
         }
     }
-    if (tid == 0) {
-        for (int s = 0; s < NA; s++) { mbarInitN(&full[s], 1); mbarInitN(&empty[s], 1); }
-        for (int g = 0; g < NG; g++) { mbarInitN(&accFull[g], 1); mbarInitN(&accEmpty[g], 1); }
-        mbarInitN(bLoad, 1);
-        mbarInitN(drain, 1);
-        *abortFlag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::sAddr(tmemSlot)),
                      "n"(TMEMCOLS)
@@ -484,17 +501,12 @@ __global__ void __launch_bounds__(64 + 128 * NG, 1) k_forward_i8(const __grid_co
     __syncthreads();
     tc::fenceAfterSync();
     const uint32_t tmem = *tmemSlot;
-    const int rowsPerFrame = (int)(p.frameStride / p.frameWidth);
 
     if (warp == 0) {
-        // ---------------- TMA producer
+        // ---------------- TMA producer (the first `pre` tiles are out already)
         if (lane == 0) {
-            const unsigned char* tab = p.dftDigits + (size_t)pol * 4 * BQ;
-            tc::fenceProxyAsync();
-            tc::mbarExpectTxTc(bLoad, 4 * BQ);
-            tc::bulkLoad(bBuf, tab, 4 * BQ, bLoad);
-            int issued = 0;
-            for (int it = 0; it < nIt; it++) {
+            int issued = pre;
+            for (int it = pre; it < nIt; it++) {
                 const int s = it % NA;
                 if (it >= NA && !tc::mbarWaitTc(&empty[s], (unsigned)(((it / NA) - 1) & 1))) {
                     flagFail(p, abortFlag);
