@@ -301,6 +301,11 @@ __device__ __forceinline__ void idft4(float2& x0, float2& x1, float2& x2, float2
     x3 = csub(d02, id13);
 }
 
+// Barrier of one unit's 64 threads (named barrier 1 + slot): after the
+// block-wide barrier that publishes the tables, the units of a block share
+// nothing, so each waits only for its own two warps.
+__device__ __forceinline__ void unitBar(int slot) { asm volatile("bar.sync %0, 64;" ::"r"(1 + slot) : "memory"); }
+
 __device__ __forceinline__ float2 shflXor2(float2 v, int m) {
     return make_float2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
@@ -455,7 +460,7 @@ __global__ void __launch_bounds__(Q_THREADS) k_inverse_lo16q(DhInvParams p) {
         rw[0] = st.maxI; rw[1] = __int_as_float(st.maxIdx);
         rw[2] = st.P; rw[3] = st.cx; rw[4] = st.cy; rw[5] = st.cyw; rw[6] = st.e4;
     }
-    __syncthreads();
+    unitBar(slot);
     {
         const float* r0 = red + slot * 16;
         const float* r1 = r0 + 8;
@@ -518,7 +523,7 @@ __global__ void __launch_bounds__(Q_THREADS) k_inverse_lo16q(DhInvParams p) {
         T[y * Q_TLD + xpix] = make_float2((float)sr, (float)si);
     }
     if (G <= 0 || !p.coefs) return;   // uniform over the block: no barrier is skipped by part of it
-    __syncthreads();
+    unitBar(slot);
 
     // 5. overlap on the int16 field (digHolo.cpp:2149-2341):
     //    U[x][n] = sum_y Hy[n][y] V[y][x], then c_mn = sum_x Hx[m][x] U[x][n]
@@ -540,7 +545,7 @@ __global__ void __launch_bounds__(Q_THREADS) k_inverse_lo16q(DhInvParams p) {
             U[xc * ULD + n] = make_float2(ur, ui);
         }
     }
-    __syncthreads();
+    unitBar(slot);
     if (!active) return;
     const float fieldScale = 1.0f / scale;
     const float* sxp = hsc + pol * G;
