@@ -210,3 +210,24 @@ def test_basis_transform_matches_live_reference(basis):
         # the LG transform is unitary: the power per frame is unchanged
         np.testing.assert_allclose(np.sum(np.abs(co) ** 2, axis=(1, 2)), np.sum(np.abs(o["coefs"]) ** 2, axis=(1, 2)),
                                    rtol=1e-6)
+
+
+def test_lg_transform_is_block_unitary():
+    """The oracle's HG -> LG matrix: block-diagonal by mode group, each block
+    unitary (to complex64 rounding), and the l = +-g modes of group g carry
+    the binomial weights sqrt(C(g, k) / 2^g) in magnitude."""
+    import math
+    G = 8
+    T = O.lg_transform(G)
+    M = G * (G + 1) // 2
+    assert T.shape == (M, M)
+    base = 0
+    for g in range(G):
+        blk = T[base:base + g + 1, base:base + g + 1]
+        np.testing.assert_allclose(blk.conj().T @ blk, np.eye(g + 1), atol=1e-6)
+        off = np.abs(T[base:base + g + 1, :]).sum() - np.abs(blk).sum()
+        assert off == 0.0
+        mag = np.abs(blk[:, 0])   # LG l = g: weights over the HG modes of the group
+        want = np.array([math.sqrt(math.comb(g, k) / 2.0 ** g) for k in range(g + 1)])
+        np.testing.assert_allclose(np.sort(mag), np.sort(want), atol=1e-6)
+        base += g + 1
