@@ -1093,10 +1093,15 @@ void objReleaseGraphs(Object& o) {
 // graph each).  At most eight graphs and eight settled argument sets are kept.
 static int launchBatchDevice(Object& o, const DhFwdParams& fp, const DhInvParams& ip) {
     const int B = o.batchCount;
+    // the default streams cannot be captured; a stream the caller is
+    // capturing already records the launches into the caller's graph
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (!o.useGraphs || o.timing || cudaStreamIsCapturing(o.stream, &cs) != cudaSuccess ||
-        cs != cudaStreamCaptureStatusNone)
+    const bool defaultStream = o.stream == nullptr || o.stream == cudaStreamLegacy || o.stream == cudaStreamPerThread;
+    if (!o.useGraphs || o.timing || defaultStream || cudaStreamIsCapturing(o.stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
         return launchChunk(o, fp, ip, 0, B);
+    }
     const int choice[4] = {o.forwardKernel, o.inverseKernel, o.overlapKernel, B};
     const unsigned long long gen = devBufGeneration();
     std::vector<unsigned char> key(sizeof(fp) + sizeof(ip) + sizeof(choice) + sizeof(gen));
@@ -1121,7 +1126,11 @@ static int launchBatchDevice(Object& o, const DhFwdParams& fp, const DhInvParams
         o.graphPending.push_back(std::move(shape));
         return launchChunk(o, fp, ip, 0, B);
     }
-    DH_CUDA(o, cudaStreamBeginCapture(o.stream, cudaStreamCaptureModeThreadLocal));
+    if (cudaStreamBeginCapture(o.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        if (++o.graphFailures >= 3) o.useGraphs = 0;
+        return launchChunk(o, fp, ip, 0, B);
+    }
     const int r = launchChunk(o, fp, ip, 0, B);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(o.stream, &graph);

@@ -72,3 +72,26 @@ def test_graph_replay_equals_direct_launches(lib, mode):
     assert lib.digHoloB200GetGraphCount(hg) == 0
     for h in (hg, hd):
         lib.digHoloDestroy(h)
+
+
+def test_default_stream_launches_directly(lib):
+    """On the legacy default stream (digHoloB200SetStream with a null
+    stream, as torch's default stream reports itself) nothing can be
+    captured: the batches launch directly, with the same results."""
+    import torch
+    B = 16
+    hol = make_case("batched_640x512_u16_2pol", B, seed=3)
+    cfg = config_for(hol, 1)
+    dev = torch.from_numpy(np.ascontiguousarray(hol.frames).view(np.int16)).cuda()
+    hd = lib.digHoloCreate()
+    hs = lib.digHoloCreate()
+    for h in (hd, hs):
+        api.configure(lib, h, cfg)
+    ref = _coefs(lib, hs, dev, B)
+    _coefs(lib, hd, dev, B)                       # first batch creates the handle's own stream
+    assert lib.digHoloB200SetStream(hd, None) == 0
+    for _ in range(3):
+        np.testing.assert_array_equal(_coefs(lib, hd, dev, B), ref)
+    assert lib.digHoloB200GetGraphCount(hd) == 0
+    for h in (hd, hs):
+        lib.digHoloDestroy(h)
