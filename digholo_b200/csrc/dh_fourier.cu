@@ -66,16 +66,21 @@ __global__ void __launch_bounds__(FT) k_fourier_rows(DhFourierParams q) {
     }
 }
 
-// CB columns of one plane: H-point forward FFT in place.
+// CB columns of one plane: H-point forward FFT in place.  With windowCols
+// only the columns sx0 .. sx0 + w - 1 of the unit's polarisation (the
+// Fourier window's) are transformed; the others are left as the rows wrote them.
 __global__ void __launch_bounds__(FT) k_fourier_cols(DhFourierParams q) {
     extern __shared__ float2 sm[];
     const DhFwdParams& f = q.f;
     const int W = 1 << f.logW, H = 1 << f.logH, Nx = W / 2 + 1;
     int CB = FBUF / H;
     if (CB < 1) CB = 1;
-    const int groups = (Nx + CB - 1) / CB;
-    const int unit = blockIdx.x / groups, c0 = (blockIdx.x % groups) * CB;
-    const int cols = Nx - c0 < CB ? Nx - c0 : CB;
+    const int ccount = q.windowCols ? f.w : Nx;
+    const int groups = (ccount + CB - 1) / CB;
+    const int unit = blockIdx.x / groups;
+    const int cbeg = q.windowCols ? f.sx0[unit % f.polCount] : 0;
+    const int c0 = cbeg + (blockIdx.x % groups) * CB;
+    const int cols = cbeg + ccount - c0 < CB ? cbeg + ccount - c0 : CB;
     float2* pl = q.plane + (size_t)unit * H * Nx;
     for (int e = threadIdx.x; e < H * cols; e += FT) {
         const int r = e / cols, c = e - r * cols;
@@ -254,12 +259,16 @@ cudaError_t dh_launch_forward_plane(const DhFourierParams& q, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     e = setSmemOnce(reinterpret_cast<const void*>(k_fourier_cols), (int)smemC);
     if (e != cudaSuccess) return e;
-    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(q);
-    k_fourier_cols<<<(unsigned)(units * ((Nx + CB - 1) / CB)), FT, smemC, s>>>(q);
+    // the window needs only its own w columns of each plane transformed
+    DhFourierParams qw = q;
+    qw.windowCols = 1;
+    (void)Nx;
+    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(qw);
+    k_fourier_cols<<<(unsigned)(units * ((f.w + CB - 1) / CB)), FT, smemC, s>>>(qw);
     const int total = units * f.h * f.w;
     int g = (total + 255) / 256;
     if (g > 148 * 16) g = 148 * 16;
-    k_window_from_plane<<<g, 256, 0, s>>>(q);
+    k_window_from_plane<<<g, 256, 0, s>>>(qw);
     return cudaGetLastError();
 }
 
@@ -280,9 +289,11 @@ cudaError_t dh_launch_fourier_full(const DhFourierParams& q, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     e = setSmemOnce(reinterpret_cast<const void*>(k_fourier_cols), (int)smemC);
     if (e != cudaSuccess) return e;
-    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(q);
-    k_fourier_cols<<<(unsigned)(units * ((Nx + CB - 1) / CB)), FT, smemC, s>>>(q);
-    k_fourier_stats<<<(unsigned)units, FT, 0, s>>>(q);
+    DhFourierParams qf = q;
+    qf.windowCols = 0;   // the whole plane
+    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(qf);
+    k_fourier_cols<<<(unsigned)(units * ((Nx + CB - 1) / CB)), FT, smemC, s>>>(qf);
+    k_fourier_stats<<<(unsigned)units, FT, 0, s>>>(qf);
     const int total = q.f.polCount * H * Nx;
     int g = (total + 255) / 256;
     if (g > 148 * 8) g = 148 * 8;

@@ -103,4 +103,5 @@ struct DhFourierParams {
     float r2;               // squared radius of the excluded disk (0: none)
     float* stats;           // out: [param][pol][frameCount + 1] (DIGHOLO_ANALYSIS layout)
     float* batchSum;        // out: [pol][W H], pixel (j, i) at j (W/2+1) + i
+    int windowCols;         // 1: column transforms of each polarisation's Fourier-window columns only
 };
