@@ -28,11 +28,6 @@ namespace {
 constexpr int FT = 256;           // threads per block
 constexpr int FBUF = 4096;        // complex elements per shared transform buffer
 
-__device__ __forceinline__ float frameSample(const DhFwdParams& f, long long idx) {
-    return f.inputU16 ? (float)static_cast<const unsigned short*>(f.frames)[idx]
-                      : static_cast<const float*>(f.frames)[idx];
-}
-
 // RB rows of one (frame, polarisation) window: packed FFT of length W/2, R2C
 // split, all W/2+1 columns written.
 __global__ void __launch_bounds__(FT) k_fourier_rows(DhFourierParams q) {
@@ -46,16 +41,28 @@ __global__ void __launch_bounds__(FT) k_fourier_rows(DhFourierParams q) {
     const int unit = blockIdx.x / groups, r0 = (blockIdx.x % groups) * RB;
     const int P = f.polCount, pol = unit % P, frame = unit / P;
     const long long base = (long long)frame * f.frameStride + (long long)f.cy[pol] * f.frameWidth + f.cx[pol];
+    // pixel pairs (2n, 2n + 1) in one load: the window's corner and the row
+    // pitch are even, and the frame buffers are 16-byte aligned
     for (int e = threadIdx.x; e < RB * N; e += FT) {
         const int r = e / N, n = e - r * N;
         const long long o = base + (long long)(r0 + r) * f.frameWidth + 2 * n;
-        sm[r * N + bitrev(n, logN)] = make_float2(frameSample(f, o), frameSample(f, o + 1));
+        float2 v;
+        if (f.inputU16) {
+            const unsigned int u = *reinterpret_cast<const unsigned int*>(static_cast<const unsigned short*>(f.frames) + o);
+            v = make_float2((float)(u & 0xFFFFu), (float)(u >> 16));
+        } else {
+            v = *reinterpret_cast<const float2*>(static_cast<const float*>(f.frames) + o);
+        }
+        sm[r * N + bitrev(n, logN)] = v;
     }
     __syncthreads();
     fft_dit(sm, RB, N, 1, logN, false, false, f.twiddle);
     float2* out = q.plane + ((size_t)unit * H + r0) * Nx;
-    for (int e = threadIdx.x; e < RB * Nx; e += FT) {
-        const int r = e / Nx, k = e - r * Nx;
+    // all W/2 + 1 columns, or with windowCols the Fourier window's w columns
+    const int kcount = q.windowCols ? f.w : Nx;
+    const int kbeg = q.windowCols ? f.sx0[pol] : 0;
+    for (int e = threadIdx.x; e < RB * kcount; e += FT) {
+        const int r = e / kcount, k = kbeg + (e - r * kcount);
         const float2 zk = sm[r * N + (k & (N - 1))];
         const float2 zc = cconj(sm[r * N + ((N - k) & (N - 1))]);
         const float2 even = cscale(cadd(zk, zc), 0.5f);
