@@ -1,10 +1,9 @@
 // Power-meter support on the GPU: gather of one coefficient matrix block and
-// its FP64 Gram matrix, whose eigenvalues (cuSOLVER zheevd, FP64) are the
-// squared singular values digHolo takes from cgesvd (digHolo.cpp:3021-3055,
-// used by digHoloPowerMeter digHolo.cpp:10980-11011).
+// its FP64 Gram matrix, whose eigenvalues (dh_eigen.cu, FP64) are the squared
+// singular values digHolo takes from cgesvd (digHolo.cpp:3021-3055, used by
+// digHoloPowerMeter digHolo.cpp:10980-11011).
 #include <cuda_runtime.h>
 #include <cuComplex.h>
-#include <cusolverDn.h>
 
 #include <cstdio>
 
@@ -84,50 +83,4 @@ cudaError_t dh_launch_gram(const float2* A, int rows, int batch, int rowsGram, v
     dim3 grid((n + 15) / 16, (n + 15) / 16);
     k_gram<<<grid, dim3(16, 16), 0, s>>>(A, rows, batch, rowsGram, static_cast<cuDoubleComplex*>(G));
     return cudaGetLastError();
-}
-
-// Eigenvalues (ascending) of the Hermitian n x n matrix G (column-major,
-// overwritten) into W.  The solver handle and workspace are created on first
-// use and grown as needed; the caller owns them.
-struct DhEigen {
-    cusolverDnHandle_t handle = nullptr;
-    void* work = nullptr;
-    int lwork = 0;
-    int* info = nullptr;
-};
-
-int dh_eigen_values(DhEigen& e, void* G, int n, double* W, cudaStream_t s) {
-    if (!e.handle) {
-        if (cusolverDnCreate(&e.handle) != CUSOLVER_STATUS_SUCCESS) return 1;
-        if (cudaMalloc(&e.info, sizeof(int)) != cudaSuccess) return 1;
-    }
-    cusolverDnSetStream(e.handle, s);
-    int lw = 0;
-    if (cusolverDnZheevd_bufferSize(e.handle, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, n,
-                                    static_cast<cuDoubleComplex*>(G), n, W, &lw) != CUSOLVER_STATUS_SUCCESS)
-        return 2;
-    if (lw > e.lwork) {
-        if (e.work) cudaFree(e.work);
-        if (cudaMalloc(&e.work, sizeof(cuDoubleComplex) * (size_t)lw) != cudaSuccess) { e.work = nullptr; e.lwork = 0; return 3; }
-        e.lwork = lw;
-    }
-    if (cusolverDnZheevd(e.handle, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, n, static_cast<cuDoubleComplex*>(G), n,
-                         W, static_cast<cuDoubleComplex*>(e.work), e.lwork, e.info) != CUSOLVER_STATUS_SUCCESS)
-        return 4;
-    return 0;
-}
-
-void dh_eigen_release(DhEigen& e) {
-    if (e.handle) cusolverDnDestroy(e.handle);
-    if (e.work) cudaFree(e.work);
-    if (e.info) cudaFree(e.info);
-    e = DhEigen();
-}
-
-DhEigen* dh_eigen_create() { return new DhEigen(); }
-void dh_eigen_destroy(DhEigen* e) {
-    if (e) {
-        dh_eigen_release(*e);
-        delete e;
-    }
 }

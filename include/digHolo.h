@@ -404,6 +404,14 @@ float digHoloB200AutoAlignAdjoint(int handleIdx);
  * power meter) the last digHoloAutoAlign call made. */
 int digHoloB200GetAutoAlignEvaluations(int handleIdx);
 
+/* No counterpart in the reference (its power meter calls LAPACK cgesvd).
+ * Eigenvalues of one Hermitian n x n matrix, FP64, with the GPU solver
+ * behind MDL: G (host) column-major complex double (re, im interleaved),
+ * W (host) n eigenvalues ascending; with vecs non-null (host, 2 n complex
+ * double) the unit eigenvectors of the smallest and the largest eigenvalue.
+ * n up to 2048.  Runs on the current device and waits for it. */
+int digHoloB200EigenHermitian(int n, const double* G, double* W, double* vecs);
+
 /* No counterpart in the reference.  The batch path for callers that cannot
  * allocate device memory while they process frames (a real-time acquisition
  * callback must not block in cudaMalloc/cudaFree, which can synchronise the
@@ -416,8 +424,14 @@ int digHoloB200GetAutoAlignEvaluations(int handleIdx);
  * for its configuration (process one batch with digHoloProcessBatch or
  * digHoloB200ProcessBatchDevice first; that call allocates).  Sizes with
  * frameCount*polCount*w*h*8 bytes above 8 MiB are refused with
- * DIGHOLO_ERROR_INVALIDDIMENSION.  The first call on a device looks up the
- * scratch address (cudaGetSymbolAddress): make it before any stream capture.
+ * DIGHOLO_ERROR_INVALIDDIMENSION.  Where the preparing batch sized a scratch
+ * of the handle (the Fourier planes of windows 256 pixels wide and more, the
+ * band buffers of large full-resolution fields), a frameCount above that
+ * batch's is refused with DIGHOLO_ERROR_MEMORYALLOCATION, not allocated.
+ * The call makes the handle's device current and leaves it so; the first
+ * call on a device looks up the scratch address there
+ * (cudaGetSymbolAddress; with CUDA's lazy module loading the 8 MiB array is
+ * placed in device memory at that moment): make it before any stream capture.
  * Calls share the scratch; calls whose GPU work overlaps race on it.
  * Returns without waiting for the GPU (see digHoloB200Synchronize). */
 int digHoloB200ProcessBatchNoAlloc(int handleIdx, const void* frames, int frameCount, int framesAreUint16,
