@@ -48,22 +48,32 @@ typedef float complex64[2];
 // batch with digHoloProcessBatch or digHoloB200ProcessBatchDevice first (that
 // call allocates).  frameCount * polCount * w * h * 8 bytes must not exceed
 // the 8 MiB scratch (e.g. 2048 dual-polarisation frames with 16x16 IFFT
-// windows).  The first call on a device looks up the scratch address with
-// cudaGetSymbolAddress; make that first call before any stream capture.
-// All calls share the one scratch array and it keeps the last call's
-// contents (the forward kernel overwrites every element it reads back, so
-// nothing needs clearing); calls whose GPU work overlaps race on it.
+// windows), and frameCount must not exceed the batch that call prepared
+// where that batch sized a scratch of the handle (the Fourier planes of
+// 256-pixel and wider windows, the band buffers of large full-resolution
+// fields): larger calls return DIGHOLO_ERROR_MEMORYALLOCATION instead of
+// allocating.  The call makes the handle's device current (and leaves it
+// current); the first call on a device then looks up the scratch address on
+// that device with cudaGetSymbolAddress (with CUDA's lazy module loading that
+// lookup is also when the 8 MiB array is placed in device memory), so make
+// that first call before any stream capture.  All calls share the one scratch array and it keeps the
+// last call's contents (the forward kernel overwrites every element it reads
+// back, so nothing needs clearing); calls whose GPU work overlaps race on it.
 int digHoloB200ProcessBatchNoAlloc(int handleIdx, const void* frames, int frameCount, int framesAreUint16,
                                    complex64* coefs, short* fieldR, short* fieldI, float* stats) {
     dh::Object* o = dhObjectForHandle(handleIdx);
     if (!o) return dh::ERR_INVALIDHANDLE;
     if (!frames || !fieldR || !fieldI || !stats) return dh::ERR_NULLPOINTER;
     if (frameCount < 1) return dh::ERR_INVALIDDIMENSION;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return dh::ERR_ERROR;
+    // the handle's device (set by its first batch; calls on one handle are
+    // serialised by the caller): the scratch address is looked up and cached
+    // on that device, whichever device the calling thread had current
+    const int dev = o->device;
     void* scratch = nullptr;
-    {
+    if (dev >= kMaxDevices) return dh::ERR_ERROR;
+    if (dev >= 0) {
+        cudaError_t e = cudaSetDevice(dev);
+        if (e != cudaSuccess) return dh::ERR_ERROR;
         std::lock_guard<std::mutex> g(gSetupLock);
         if (!gScratch[dev]) {
             // the array's name is a host-side stand-in; the kernels need its device address
@@ -77,6 +87,7 @@ int digHoloB200ProcessBatchNoAlloc(int handleIdx, const void* frames, int frameC
         }
         scratch = gScratch[dev];
     }
+    // an unprepared handle (no device yet, scratch null) is refused there
     return dh::objProcessNoAlloc(*o, frames, frameCount, framesAreUint16 ? 1 : 0, static_cast<float2*>(scratch),
                                  DH_NOALLOC_WINDOW_BYTES, reinterpret_cast<float2*>(coefs), fieldR, fieldI, stats);
 }

@@ -740,7 +740,7 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
 
 // Forward stage: the TMA-fed persistent kernel where the shape and the
 // alignment allow it, else the register kernel, else the generic one.
-static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
+static cudaError_t launchForward(Object& o, const DhFwdParams& fp, bool mayAlloc = true) {
     const int mode = o.forwardKernel;
     cudaError_t fe = cudaErrorNotSupported;
     if (mode == 0 || mode == 4) {
@@ -768,6 +768,7 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp) {
         const size_t Nx = (size_t)(1 << fp.logW) / 2 + 1;
         const size_t frames = (size_t)std::max(o.batchCount * std::max(1, o.avgCount), fp.frameOffset + fp.frameCount);
         const size_t need = frames * o.polCount * (1 << fp.logH) * Nx * sizeof(float2);
+        if (o.dFourier.bytes < need && !mayAlloc) return cudaErrorMemoryAllocation;
         fe = o.dFourier.ensure(need);
         if (fe != cudaSuccess) return fe;
         DhFourierParams q;
@@ -1288,7 +1289,7 @@ static int processBatchLocked(Object& o, int syncCoefs) {
 int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* window, size_t windowBytes,
                       float2* coefs, short* fieldR, short* fieldI, float* stats) {
     std::lock_guard<std::mutex> guard(o.lock);
-    if (o.device < 0 || !o.preparedValid)
+    if (o.device < 0 || !o.preparedValid || !window)
         return fail(o, ERR_ERROR, "no-alloc path: process one batch with this configuration first (that call allocates)");
     cudaSetDevice(o.device);
     Config a = o.cfg, b = o.preparedCfg;
@@ -1335,8 +1336,13 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     ip.statsStride = B + 1;
     ip.coefs = o.cfg.maxMG > 0 ? coefs : nullptr;
     if (!ip.coefs) ip.maxMG = 0;
-    cudaError_t fe = launchForward(o, fp);
+    cudaError_t fe = launchForward(o, fp, false);
+    if (fe == cudaErrorMemoryAllocation)
+        return fail(o, ERR_MEMORYALLOCATION, "no-alloc path: the Fourier-plane buffer was sized for a smaller batch");
     if (fe != cudaSuccess) return failCuda(o, fe, "no-alloc forward kernel launch");
+    // the full-plane forward wrote this call's planes over the last batch's:
+    // a later Fourier-plane request recomputes them from that batch's frames
+    if (o.lastForwardKernel == 5) o.fourierValid = 0;
     fe = launchInverse(o, ip, false);
     if (fe == cudaErrorMemoryAllocation)
         return fail(o, ERR_MEMORYALLOCATION, "no-alloc path: the band scratch was sized for a smaller batch");

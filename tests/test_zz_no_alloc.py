@@ -9,7 +9,15 @@ static 8 MiB device array, and the caller passes the frames and every output
 buffer.  This file runs last (pytest collects it after the others) and
 checks the entry point twice in a row against digHoloB200ProcessBatchDevice,
 with the coefficient tolerance of the parity tests (relative L2 <= 5e-5) and
-identical int16 fields.
+identical int16 fields: once with 16x16 low-resolution fields, once with
+large fields (2048x2048 frames, 512x512 windows: the full-plane forward and
+the band inverse, whose scratch buffers the preparing batch sized).  Free
+device memory is read before and after every call but the first (the first
+call on a device looks up the static scratch array there, and CUDA's lazy
+module loading places the 8 MiB array in device memory at that moment): an
+allocation by the entry point would show.
+A call with more frames than the preparing batch on the large-field
+configuration is refused (DIGHOLO_ERROR_MEMORYALLOCATION), not allocated.
 """
 import ctypes as C
 
@@ -27,12 +35,16 @@ class _DeviceArray:
         self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False), "version": 2}
 
 
-def test_no_alloc_matches_device_entry_point():
+CASES = [("batched_640x512_u16_2pol", 32, 1, 16), ("largefield_2048_u16_2pol", 4, 0, 2)]
+
+
+@pytest.mark.parametrize("workload,frames,mode,smaller", CASES)
+def test_no_alloc_matches_device_entry_point(workload, frames, mode, smaller):
     import torch
     import digholo_b200
     L = digholo_b200.load()
-    hol = make_case("batched_640x512_u16_2pol", 32)
-    cfg = config_for(hol, 1)
+    hol = make_case(workload, frames)
+    cfg = config_for(hol, mode)
     frames = torch.from_numpy(np.ascontiguousarray(hol.frames).view(np.int16)).cuda()
     h = L.digHoloCreate()
     api.configure(L, h, cfg)
@@ -43,7 +55,8 @@ def test_no_alloc_matches_device_entry_point():
     assert L.digHoloB200Synchronize(h) == 0
     b, m, p = C.c_int(), C.c_int(), C.c_int()
     dptr = L.digHoloB200GetCoefsDevice(h, C.byref(b), C.byref(m), C.byref(p))
-    assert dptr and m.value == 120 and p.value == 2
+    G = hol.max_mg
+    assert dptr and m.value == G * (G + 1) // 2 and p.value == 2
     M, P = m.value, p.value
     # the regular entry point leaves the coefficients on the GPU; view them through the CUDA array interface
     dev_view = _DeviceArray(C.cast(dptr, C.c_void_p).value, (B, P * M, 2), "<f4")
@@ -52,22 +65,43 @@ def test_no_alloc_matches_device_entry_point():
     L.digHoloB200GetGeometry(h, geo)
     nx, ny = geo[4], geo[5]
     ref_out = api.read_outputs(L, h, B, want_fields=True)
-    for call in range(2):
-        coefs = torch.full((B, P * M, 2), float("nan"), dtype=torch.float32, device="cuda")
-        fr = torch.full((B, P, ny, nx), 7, dtype=torch.int16, device="cuda")
-        fi = torch.full((B, P, ny, nx), 7, dtype=torch.int16, device="cuda")
-        stats = torch.zeros((7, P, B + 1), dtype=torch.float32, device="cuda")
-        rc = L.digHoloB200ProcessBatchNoAlloc(h, frames.data_ptr(), B, 1, coefs.data_ptr(), fr.data_ptr(),
+    want_all = ref_coefs.cpu().numpy().view(np.complex64).reshape(B, P * M)
+    # the full batch twice, then a smaller one (the leading frames)
+    for call, n in enumerate((B, B, smaller)):
+        coefs = torch.full((n, P * M, 2), float("nan"), dtype=torch.float32, device="cuda")
+        fr = torch.full((n, P, ny, nx), 7, dtype=torch.int16, device="cuda")
+        fi = torch.full((n, P, ny, nx), 7, dtype=torch.int16, device="cuda")
+        stats = torch.zeros((7, P, n + 1), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        rc = L.digHoloB200ProcessBatchNoAlloc(h, frames.data_ptr(), n, 1, coefs.data_ptr(), fr.data_ptr(),
                                               fi.data_ptr(), stats.data_ptr())
         assert rc == 0, L.digHoloB200GetLastError(h)
         assert L.digHoloB200Synchronize(h) == 0
-        got = coefs.cpu().numpy().view(np.complex64).reshape(B, P * M)
-        want = ref_coefs.cpu().numpy().view(np.complex64).reshape(B, P * M)
+        if call > 0:
+            assert torch.cuda.mem_get_info()[0] >= free0      # nothing was allocated
+        got = coefs.cpu().numpy().view(np.complex64).reshape(n, P * M)
         assert np.isfinite(got).all()
-        assert rel_l2(got, want) <= 5e-5
-        np.testing.assert_array_equal(fr.cpu().numpy(), ref_out["R"])
-        np.testing.assert_array_equal(fi.cpu().numpy(), ref_out["I"])
-        np.testing.assert_allclose(stats[3, :, :B].cpu().numpy(), ref_out["scale"], rtol=1e-6)
+        assert rel_l2(got, want_all[:n]) <= 5e-5
+        np.testing.assert_array_equal(fr.cpu().numpy(), ref_out["R"][:n])
+        np.testing.assert_array_equal(fi.cpu().numpy(), ref_out["I"][:n])
+        np.testing.assert_allclose(stats[3, :, :n].cpu().numpy(), ref_out["scale"][:, :n], rtol=1e-6)
+    if mode == 0:
+        # more frames than the preparing batch: its plane and band buffers are
+        # too small, and the call is refused instead of growing them
+        big = torch.cat([frames, frames])
+        n = big.shape[0]
+        coefs = torch.zeros((n, P * M, 2), dtype=torch.float32, device="cuda")
+        fr = torch.zeros((n, P, ny, nx), dtype=torch.int16, device="cuda")
+        fi = torch.zeros((n, P, ny, nx), dtype=torch.int16, device="cuda")
+        stats = torch.zeros((7, P, n + 1), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        rc = L.digHoloB200ProcessBatchNoAlloc(h, big.data_ptr(), n, 1, coefs.data_ptr(), fr.data_ptr(),
+                                              fi.data_ptr(), stats.data_ptr())
+        assert rc == 9, rc  # DIGHOLO_ERROR_MEMORYALLOCATION
+        assert L.digHoloB200Synchronize(h) == 0
+        assert torch.cuda.mem_get_info()[0] >= free0
     # sizes beyond the scratch are refused with an error, not processed
     big = 1 << 20
     rc = L.digHoloB200ProcessBatchNoAlloc(h, frames.data_ptr(), big, 1, coefs.data_ptr(), fr.data_ptr(),
