@@ -319,7 +319,7 @@ static float windowRadiusRec(const Config& c, int P) {
 // fitToQuadratic (digHolo.cpp:3146-3252): Gauss-Newton fit of y = a x^2 + b x + c
 // from B0, with the normal equations of the 3-parameter linear least squares
 // solved directly; returns the vertex -b / 2a (NaN if the data are not finite).
-static float fitToQuadratic(const float* x, const float* y, int n, float* B, const float* B0, float tol, float maxIter) {
+float fitToQuadratic(const float* x, const float* y, int n, float* B, const float* B0, float tol, float maxIter) {
     double a = B0[0], b = B0[1], c = B0[2];
     float resid = 0.f, lastResid = 0.f;
     int iter = 0;
@@ -372,10 +372,12 @@ static float fitToQuadratic(const float* x, const float* y, int n, float* B, con
 }
 
 
-// AutoAlign (digHolo.cpp:12237-12982), single wavelength.  TWEAK refines
-// the current settings with the reference's coordinate search; FULL and
-// ESTIMATE start from the current settings too (the snap estimate, which
-// needs the full Fourier plane of every frame, is not built on this path).
+int objAutoAlignSnap(Object& o, float steps[4]);
+
+// AutoAlign (digHolo.cpp:12237-12982), single wavelength.  FULL and
+// ESTIMATE start with the parameter estimate (objAutoAlignSnap, dh_snap.cpp);
+// ESTIMATE then scores the estimate, FULL and TWEAK refine the settings with
+// the reference's coordinate search.
 float objAutoAlign(Object& o) {
     Config& c = o.cfg;
     const int P = c.polCount;
@@ -387,12 +389,34 @@ float objAutoAlign(Object& o) {
     if (c.autoAlignFourierWindowRadius) {
         c.apertureSize = c.autoAlignTilt ? windowRadiusMax(c.pixelSize, c.wavelengthCentre) : windowRadiusRec(c, P);
     }
+    // FULL (0) and ESTIMATE (2): the parameter estimate first, which also
+    // sets the step sizes of the search (digHolo.cpp:12301-12314)
+    const int mode = c.autoAlignMode;
+    float snapSteps[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool snapped = mode == 0 || mode == 2 || maxMG <= 0;
+    if (snapped) {
+        if (objAutoAlignSnap(o, snapSteps)) return -FLT_MAX;
+        if (mode == 2 || maxMG <= 0) {
+            // the estimate scored by a final overlap and power meter
+            // (digHolo.cpp:11925-11953, 12962-12980); this build scores it
+            // on the configured FFT window
+            if (maxMG <= 0) return -FLT_MAX;
+            if (objProcessBatch(o, 0) || objCalcMetrics(o)) return -FLT_MAX;
+            return o.autoAlignMetrics[goalIdx0 >= 0 && goalIdx0 < METRIC_COUNT ? goalIdx0 : 0][0];
+        }
+    }
     // step sizes (digHolo.cpp:12298-12313)
     float tiltStep = c.apertureSize * 0.1f;
     float centreStep = c.waist[0] * 0.1f;
     float defocusStep = 0.4f;
     for (int i = 0; i < P; i++) defocusStep = std::max(defocusStep, std::fabs(c.zern[i][ZERN_DEFOCUS]) * 0.1f);
     float waistStep = c.waist[0] * 0.1f;
+    if (snapped) {
+        tiltStep = snapSteps[0];
+        centreStep = snapSteps[1];
+        defocusStep = snapSteps[2];
+        waistStep = snapSteps[3];
+    }
     if (maxMG <= 0) return -FLT_MAX;
 
     float LIMS[6][2];

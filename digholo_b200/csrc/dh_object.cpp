@@ -354,18 +354,14 @@ static int stageFrames(Object& o, int f0, int f1, DhFwdParams& fp, int async) {
     return ERR_SUCCESS;
 }
 
-// Frame-independent factors of the forward stage for the register kernel,
-// evaluated with the float32 arithmetic of digHoloCopyWindow
-// (digHolo.cpp:1955-2035): per polarisation, the R2C split twiddles
-// [w], the column-sum twiddles [h][H/h] and the window factors [h][w].
-static void forwardTables(const Object& o, std::vector<float>& split, std::vector<float>& col,
-                          std::vector<float>& adj) {
-    const Config& c = o.useSnaps ? o.ifftSnap : o.cfg;
-    const Geometry& g = o.geo;
-    const int P = o.polCount, w = g.w, h = g.h, W = g.W, H = g.H;
-    const int Q = H / h;
-    split.assign((size_t)P * w * 2, 0.f);
-    col.assign((size_t)P * h * Q * 2, 0.f);
+// Window factors of digHoloCopyWindow (digHolo.cpp:1955-2035) per
+// polarisation, [pol][h][w] complex: the hard mask dr^2 <= kr^2 around the
+// tilt, the inverse pixel sinc, the normalisation 1/sqrt(W H . ifft length)
+// and the beam-centre phase exp(i (kx bcx + ky bcy)), in the reference's
+// float32 arithmetic.  `c` places the window and the mask, `live` gives the
+// beam centre (the two differ while AutoAlign replays stage snapshots).
+void windowFactors(const Config& c, const Config& live, const Geometry& g, int P, std::vector<float>& adj) {
+    const int w = g.w, h = g.h, W = g.W, H = g.H;
     adj.assign((size_t)P * h * w * 2, 0.f);
     const float lam = c.wavelengthCentre;
     const float k0 = 2 * PI_F / lam;
@@ -379,28 +375,16 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
     auto xcscD = [](float x) { return x == 0.f ? 1.0f : (float)((double)x / sin((double)x)); };
     for (int p = 0; p < P; p++) {
         const int sx0 = g.SX[p] - W / 2;
-        for (int cc = 0; cc < w; cc++) {
-            const double a = -2.0 * PI_D * (double)(sx0 + cc) / (double)W;
-            split[((size_t)p * w + cc) * 2] = (float)cos(a);
-            split[((size_t)p * w + cc) * 2 + 1] = (float)sin(a);
-        }
         const int cx0 = (g.cx[p] + W / 2) - c.frameWidth / 2;
         const int cy0 = (g.cy[p] + H / 2) - c.frameHeight / 2;
-        // the beam-centre phase follows the live configuration; the window
-        // selection and the mask may come from a snapshot
-        const float bcx = o.cfg.beamCentreX[p] - (cx0) * c.pixelSize;
-        const float bcy = o.cfg.beamCentreY[p] - (cy0) * c.pixelSize;
+        const float bcx = live.beamCentreX[p] - (cx0) * c.pixelSize;
+        const float bcy = live.beamCentreY[p] - (cy0) * c.pixelSize;
         const float kx0 = k0 * sinf(c.zern[p][ZERN_TILTX] * UNIT_ANGLE);
         const float ky0 = k0 * sinf(c.zern[p][ZERN_TILTY] * UNIT_ANGLE);
         for (int j = 0; j < h; j++) {
             const int jSY = j + g.SY[p];
             int row = (jSY + H / 2) % H;
             if (row < 0) row += H;
-            for (int b = 0; b < Q; b++) {
-                const double a = -2.0 * PI_D * (double)((row * b) % H) / (double)H;
-                col[(((size_t)p * h + j) * Q + b) * 2] = (float)cos(a);
-                col[(((size_t)p * h + j) * Q + b) * 2 + 1] = (float)sin(a);
-            }
             const float ky = g.ky[row];
             const float shift = jSY < 0 ? kyShift : (jSY > H ? -kyShift : 0.0f);
             for (int cc = 0; cc < w; cc++) {
@@ -421,6 +405,41 @@ static void forwardTables(const Object& o, std::vector<float>& split, std::vecto
             }
         }
     }
+}
+
+// Frame-independent factors of the forward stage for the register kernel,
+// evaluated with the float32 arithmetic of digHoloCopyWindow
+// (digHolo.cpp:1955-2035): per polarisation, the R2C split twiddles
+// [w], the column-sum twiddles [h][H/h] and the window factors [h][w].
+static void forwardTables(const Object& o, std::vector<float>& split, std::vector<float>& col,
+                          std::vector<float>& adj) {
+    const Config& c = o.useSnaps ? o.ifftSnap : o.cfg;
+    const Geometry& g = o.geo;
+    const int P = o.polCount, w = g.w, h = g.h, W = g.W, H = g.H;
+    const int Q = H / h;
+    split.assign((size_t)P * w * 2, 0.f);
+    col.assign((size_t)P * h * Q * 2, 0.f);
+    for (int p = 0; p < P; p++) {
+        const int sx0 = g.SX[p] - W / 2;
+        for (int cc = 0; cc < w; cc++) {
+            const double a = -2.0 * PI_D * (double)(sx0 + cc) / (double)W;
+            split[((size_t)p * w + cc) * 2] = (float)cos(a);
+            split[((size_t)p * w + cc) * 2 + 1] = (float)sin(a);
+        }
+        for (int j = 0; j < h; j++) {
+            const int jSY = j + g.SY[p];
+            int row = (jSY + H / 2) % H;
+            if (row < 0) row += H;
+            for (int b = 0; b < Q; b++) {
+                const double a = -2.0 * PI_D * (double)((row * b) % H) / (double)H;
+                col[(((size_t)p * h + j) * Q + b) * 2] = (float)cos(a);
+                col[(((size_t)p * h + j) * Q + b) * 2 + 1] = (float)sin(a);
+            }
+        }
+    }
+    // the beam-centre phase follows the live configuration; the window
+    // selection and the mask may come from a snapshot
+    windowFactors(c, o.cfg, g, P, adj);
 }
 
 // Byte digits of the tensor-core row DFT (k_forward_i8): for every kept kx

@@ -178,6 +178,7 @@ struct Object {
     std::vector<float> hKx, hKy;
     int digitsValid = 0;
     DevBuf dBigScratch;                 // band kernels: partial statistics and coefficients, prepared Hx
+    DevBuf dSnap[16];                   // AutoAlign parameter estimate: planes, sums, fields, tables
     DevBuf dTransRaw, dTransFrames;     // transposed uint16 input: raw host copy, converted frames
     // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums
     DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab;
@@ -263,6 +264,7 @@ void fftWindowGeometry(const Config& c, int polCount, Geometry& g);
 void ifftWindowGeometry(const Config& c, int polCount, Geometry& g);
 void referenceWave(const Config& c, int polCount, const Geometry& g, std::vector<short>& out,
                    std::vector<float>* outF = nullptr);
+void windowFactors(const Config& c, const Config& live, const Geometry& g, int polCount, std::vector<float>& adj);
 bool isPow2(int v);
 int ilog2(int v);
 

@@ -26,6 +26,9 @@ It restates, step by step, the work of digHoloProcessBatch
   apply_tilt          -conj(A.ref) and int16 rounding digHolo.cpp:2701-2837
   hg_basis            int16 HG modes and scales       digHolo.cpp:1269-1484, 10543-10645
   overlap             separable HG overlap            digHolo.cpp:2149-2341, 9756-9815
+  auto_align_snap     AutoAlign parameter estimate    digHolo.cpp:11517-11970
+  auto_focus          its focus search                digHolo.cpp:11181-11499
+  dct2_redft          FFTW REDFT10 / REDFT01 (2D)     digHolo.cpp:7393-7420
 
 Two flavours are produced by :func:`process_batch`:
 
@@ -776,3 +779,343 @@ def power_meter(coefs, pol_independent=False, goal_uses_svd=True):
     return {"il": il, "mdl": mdl, "il_frob": il_frob,
             "il_db": 10 * math.log10(il), "mdl_db": 10 * math.log10(mdl),
             "il_frob_db": 10 * math.log10(il_frob)}
+
+
+# ---------------------------------------------------------------- AutoAlign snap (parameter estimate)
+
+def dct2_redft(a, kind):
+    """2D FFTW REDFT10 (kind 2, DCT-II) or REDFT01 (kind 3, DCT-III),
+    unnormalised, as FFTW defines them: along the last axis, then the first,
+    FP64 inside, float32 out (the digHoloDCTPlan / digHoloIDCTPlan pair,
+    digHolo.cpp:7393-7420).
+      REDFT10: Y_k = 2 sum_j X_j cos(pi (j + 1/2) k / n)
+      REDFT01: Y_k = X_0 + 2 sum_{j>=1} X_j cos(pi j (k + 1/2) / n)
+    """
+    x = np.asarray(a, dtype=np.float64)
+
+    def mat(n):
+        k = np.arange(n)[:, None]
+        j = np.arange(n)[None, :]
+        if kind == 2:
+            return 2.0 * np.cos(np.pi * ((2 * j + 1) * k % (4 * n)) / (2.0 * n))
+        m = np.cos(np.pi * ((j * (2 * k + 1)) % (4 * n)) / (2.0 * n)) * 2.0
+        m[:, 0] = 1.0
+        return m
+    y = x @ mat(x.shape[1]).T
+    y = mat(x.shape[0]) @ y
+    return y.astype(F32)
+
+
+def snap_filter(out, k0, aperture_rad, pixel_size):
+    """The Gaussian filter of the snap's correlation (digHolo.cpp:11611-11643)
+    applied as the reference applies it: in blocks of 8 floats per row of
+    8 floor(Nx/8) columns, stepping through the (H, Nx) array without its row
+    stride, so flat position f gets the factor of row f // (8 floor(Nx/8)) and
+    column f % (8 floor(Nx/8)), and the last H floats are left as they are."""
+    H, Nx = out.shape
+    nb = 8 * (Nx // 8)
+    aperturek = F32(k0 * F32(aperture_rad))
+    wx = F32((1.0 * math.pi / float(aperturek)) * math.sqrt(2.0))
+    wy = F32((2.0 * math.pi / float(aperturek)) * math.sqrt(2.0))
+    wx2 = F32(-1.0 / (float(wx) * float(wx)))
+    wy2 = F32(-1.0 / (float(wy) * float(wy)))
+    ps = F32(pixel_size)
+    ps2 = F32(ps * ps)
+    flat = out.reshape(-1).copy()
+    n = H * nb
+    f = np.arange(n)
+    j = (f // nb).astype(np.int64)
+    i = (f % nb).astype(F32)
+    x = (i * ps).astype(F32)
+    xw2 = ((x * x).astype(F32) * wx2).astype(F32)
+    y2 = (F32(1.0) * (j * j).astype(F32) * ps2).astype(F32)
+    yw2 = (y2 * wy2).astype(F32)
+    g = np.exp((xw2 + yw2).astype(F32).astype(np.float64)).astype(F32)
+    flat[:n] = (flat[:n] * g).astype(F32)
+    return flat.reshape(H, Nx)
+
+
+def snap_tilt(S, kx, ky, k0, aperture_rad, pixel_size):
+    """Tilt estimate of one polarisation (digHolo.cpp:11601-11691): DCT-II of
+    the batch-summed Fourier intensity S (H, Nx), the Gaussian filter, DCT-III,
+    then the maximum over pixels with kx^2 + ky^2 > (2 k0 aperture)^2 (first
+    in row-major order on ties); returns (tiltX, tiltY) in degrees and the
+    correlation map."""
+    H, Nx = S.shape
+    out = dct2_redft(np.asarray(S, dtype=F32), 2)
+    out = snap_filter(out, k0, aperture_rad, pixel_size)
+    out2 = dct2_redft(out, 3)
+    aperturek = F32(k0 * F32(aperture_rad))
+    ad = F32(aperturek * F32(2))
+    ad = F32(ad * ad)
+    xs = kx[:Nx].astype(F32)
+    ys = ky[:H].astype(F32)
+    kr = ((xs * xs)[None, :] + (ys * ys)[:, None]).astype(F32)
+    cand = np.where(kr > ad, out2, -np.inf)
+    flat = int(np.argmax(cand))          # first maximum in row-major order
+    j, i = divmod(flat, Nx)
+    tx = F32(F32(np.arcsin(F32(xs[i] / k0))) / UNIT_ANGLE)
+    ty = F32(F32(np.arcsin(F32(ys[j] / k0))) / UNIT_ANGLE)
+    return tx, ty, out2
+
+
+def windowed_fourier_aeff(F, kx, ky, cx, cy, radius):
+    """Effective area of the batch-summed Fourier intensity inside the disk
+    of `radius` around (cx, cy) (digHoloFieldAnalysis with a negative window
+    radius, removeZeroOrder1D set: rows 0 and H/2, column 0 and the columns
+    from 8 floor(Nx/8) on excluded), intensity |F|^2 / (Nx H)."""
+    B, Ny, Nx = F.shape
+    xs = kx[:Nx].astype(F32)
+    ys = ky[:Ny].astype(F32)
+    dx = (xs - F32(cx)).astype(F32)
+    dy = (ys - F32(cy)).astype(F32)
+    rr = ((dx * dx)[None, :] + (dy * dy)[:, None]).astype(F32)
+    w2 = F32(F32(radius) * F32(radius))
+    mask = rr <= w2
+    nxr = 8 * (Nx // 8)
+    mask[:, nxr:] = False
+    mask[:, 0] = False
+    mask[0, :] = False
+    mask[Ny // 2, :] = False
+    S = ((np.abs(F) ** 2) * mask[None]).sum(axis=0) / (Nx * Ny)
+    P = S.sum()
+    E4 = (S ** 2).sum()
+    dA = abs(float(kx[2] - kx[1])) * abs(float(ky[2] - ky[1]))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return dA * P * P / E4
+
+
+def aeff_to_mfd(aeff, groups):
+    """AeffToMFD (digHolo.cpp:2887-2900)."""
+    if not groups:
+        return F32(0)
+    A = F32(float(aeff) / (15.1059697707643 * groups + 6.65360122093789))
+    return F32(2 * float(F32(np.sqrt(F32(A / PI_F)))) / 0.223008930683135)
+
+
+def focus_estimate(w_camera, w_fourier):
+    """FocusEstimate (digHolo.cpp:12017-12050)."""
+    if not (w_camera > 0 and w_fourier > 0):
+        return F32(0)
+    ratio = F32(F32(w_fourier) / F32(w_camera))
+    a, b = F32(0.25), F32(PI_F / F32(2))
+    with np.errstate(invalid="ignore"):
+        r = F32(F32(2) * F32(b * F32(np.sqrt(F32(F32(F32(1) - a) / F32(ratio - a)) - F32(1)))))
+    if not (r > 0) or np.isnan(r):
+        return F32(0)
+    return r
+
+
+def fit_quadratic(x, y, B0, tol=1e-6, max_iter=1000):
+    """fitToQuadratic (digHolo.cpp:3146-3255): Gauss-Newton steps of
+    y = a x^2 + b x + c solved by least squares; the residual accumulates
+    over the iterations as in the reference.  Returns (x of the extremum,
+    B)."""
+    a, b, c = (F32(v) for v in B0)
+    x = np.asarray(x, dtype=F32)
+    y = np.asarray(y, dtype=F32)
+    resid = F32(0)
+    last = F32(0)
+    it = 0
+    B = [a, b, c]
+    while True:
+        J = np.stack([(x * x).astype(F32), x, np.ones_like(x)], axis=1)
+        r = (y - ((a * x * x).astype(F32) + (b * x).astype(F32) + c).astype(F32)).astype(F32)
+        if np.isnan(J).any() or np.isnan(r).any():
+            return float("nan"), B
+        resid = F32(resid + F32((r.astype(F32) * r.astype(F32)).sum(dtype=F32)))
+        d = np.linalg.lstsq(J.astype(np.float64), r.astype(np.float64), rcond=None)[0].astype(F32)
+        a, b, c = F32(a + d[0]), F32(b + d[1]), F32(c + d[2])
+        B = [a, b, c]
+        it += 1
+        done = abs(float(resid - last)) < tol or it > max_iter
+        last = resid
+        mx = F32(-b / F32(2 * a))
+        if done:
+            return float(mx), B
+
+
+def _untilted_fields(frames, cfg):
+    res = process_batch(frames, _no_basis(cfg), quantised=True)
+    return res
+
+
+def _no_basis(cfg):
+    import copy
+    c = copy.deepcopy(cfg)
+    c.max_mg = 0
+    return c
+
+
+def auto_focus(res, cfg, scale):
+    """digHoloAutoFocus (digHolo.cpp:11181-11499): per defocus trial, the
+    tilt-removed field V = -conj(A . ref) (float, before int16 rounding) is
+    transformed back (unnormalised backward DFT of the field plane) and the
+    effective area of its batch-summed intensity scored; up to 25 trials,
+    the first two at +-scale, then a 0.25-scale ladder from the better one,
+    from the fifth on the minimum of a quadratic fitted to the four smallest
+    effective areas.  Returns the defocus with the smallest effective area
+    per polarisation."""
+    import copy
+    P = cfg.pol_count
+    W, H = res["W"], res["H"]
+    kx, ky = res["kx"], res["ky"]
+    xax, yax = res["x"], res["y"]
+    dA = F32(abs(float(kx[2] - kx[1])) * abs(float(ky[2] - ky[1])))
+    E = res["field_untilted"]
+    step_count, fit_count = 25, 5
+    scale = [max(F32(s), F32(1.0)) for s in scale]
+    defoc = np.zeros((P, step_count + 3), dtype=F32)
+    aeffs = np.zeros((P, step_count + 3), dtype=F32)
+    s0 = list(scale)
+    for st in range(0, step_count, 2):
+        for p in range(P):
+            defoc[p, st] = s0[p]
+            defoc[p, st + 1] = -s0[p]
+            s0[p] = F32(s0[p] + F32(scale[p] * F32(0.25)))
+    best_aeff = [np.inf] * P
+    best = [F32(0)] * P
+    converged = [False] * P
+    B0 = [[F32(0)] * 3 for _ in range(P)]
+    Bf = [[F32(0)] * 3 for _ in range(P)]
+    for st in range(step_count):
+        c = copy.deepcopy(cfg)
+        for p in range(P):
+            c.defocus[p] = F32(defoc[p, st])
+        total = True
+        for p in range(P):
+            refx, refy = reference_wave(c, p, xax, yax, W, H, res["SX"], res["SY"], kx[1] - kx[0], ky[1] - ky[0], True)
+            V, _, _ = apply_tilt(E[:, p], refx, refy, np.ones(E.shape[0]), True)
+            V = V.astype(np.complex64)
+            Fo = np.fft.ifft2(V) * (V.shape[-1] * V.shape[-2])
+            S = (np.abs(Fo) ** 2).sum(axis=0)
+            v2 = float(S.sum())
+            v4 = float((S ** 2).sum())
+            a = F32(float(dA) * (v2 * v2) / v4)
+            aeffs[p, st] = a
+            if a < best_aeff[p]:
+                best_aeff[p] = a
+                best[p] = F32(defoc[p, st])
+            if st == 1:
+                if aeffs[p, 1] < aeffs[p, 0]:
+                    sc, base = F32(defoc[p, 1] - defoc[p, 0]), defoc[p, 1]
+                else:
+                    sc, base = F32(defoc[p, 0] - defoc[p, 1]), defoc[p, 0]
+                idx = 1
+                for i in range(2, step_count, 2):
+                    defoc[p, i] = F32(base + F32(F32(idx * 0.25) * sc))
+                    defoc[p, i + 1] = F32(base - F32(F32(idx * 0.25) * sc))
+                    idx += 1
+            if st >= fit_count - 1:
+                if st == fit_count - 1:
+                    B0[p] = [F32(1e7), F32(1e7), F32(sum(float(aeffs[p, i]) for i in range(st)) / (st + 1))]
+                xs = defoc[p, :st + 1].copy()
+                ys = aeffs[p, :st + 1].copy()
+                # sortIt (digHolo.cpp:11161-11179): ascending effective area, stable
+                order = np.argsort(ys, kind="stable")
+                xs, ys = xs[order], ys[order]
+                mx, Bf[p] = fit_quadratic(xs[:fit_count - 1], ys[:fit_count - 1], B0[p])
+                B0[p] = list(Bf[p])
+                if st + 1 < step_count - 1:
+                    if not np.isnan(mx):
+                        defoc[p, st + 1] = F32(mx)
+                if abs(mx - float(best[p])) < 0.01:
+                    converged[p] = True
+            total = total and converged[p]
+        if total:
+            break
+    return best
+
+
+def auto_align_snap(frames, cfg, align_tilt=1, align_defocus=1, align_centre=1, align_waist=1,
+                    align_radius=1, pols_independent=0):
+    """digHoloAutoAlignSnap (digHolo.cpp:11517-11970) with the aperture rule
+    AutoAlign applies before it (digHolo.cpp:12286-12299).  Returns the
+    estimated configuration (a new Config) and the search step sizes."""
+    import copy
+    c = copy.deepcopy(cfg)
+    P = c.pol_count
+    fw, fh = c.frame_width, c.frame_height
+    ps = F32(c.pixel_size)
+    lam = F32(c.wavelength)
+    if align_radius:
+        if align_tilt:
+            wc = (-2.0 + math.sqrt(68.0)) / 16.0
+            wmax = F32(float(lam) / (2.0 * float(ps)))
+            c.window_radius_deg = F32(F32(F32(wc) * wmax) / UNIT_ANGLE)
+        else:
+            c.window_radius_deg = F32(min(F32(np.sqrt(F32(F32(t[0] * t[0]) + F32(t[1] * t[1])))) for t in c.tilt_deg[:P]) / F32(3))
+    for p in range(P):
+        if align_centre:
+            c.beam_centre[p] = [F32((-(P - 1) * (fw / 4.0) + (p * fw / 2.0)) * float(ps)), F32(0)]
+        if align_tilt:
+            c.tilt_deg[p] = [F32(0), F32(0)]
+        if align_defocus:
+            c.defocus[p] = F32(0)
+    c.fft_window = (fw // P, fh)
+    W, H, cxs, cys = fft_windows(c)
+    kx, ky = k_axes(W, H, ps)
+    Fp = r2c_windows(frames, c, W, H, cxs, cys)
+    k0 = F32(F32(2) * PI_F / lam)
+    fa = [fourier_analysis(Fp[:, p], kx, ky, lam, c.window_radius_deg) for p in range(P)]
+    waistF = [F32(0)] * P
+    tilts = {}
+    for pas in range(1 + (1 if align_radius else 0)):
+        for p in range(P):
+            ap = F32(c.window_radius_deg * UNIT_ANGLE)
+            tx, ty, _ = snap_tilt(fa[p]["batchsum"].astype(F32), kx, ky, k0, ap, ps)
+            tilts[(pas, p)] = (tx, ty)
+            if align_radius:
+                apmax = F32(F32(np.sqrt(F32(F32(tx * tx) + F32(ty * ty)))) / F32(3))
+                if apmax < c.window_radius_deg:
+                    c.window_radius_deg = apmax
+                    fa = [fourier_analysis(Fp[:, q], kx, ky, lam, c.window_radius_deg) for q in range(P)]
+            if align_tilt:
+                c.tilt_deg[p] = [tx, ty]
+            wcx = F32(k0 * F32(c.tilt_deg[p][0] * UNIT_ANGLE))
+            wcy = F32(k0 * F32(c.tilt_deg[p][1] * UNIT_ANGLE))
+            wr = F32(k0 * F32(np.sin(F32(c.window_radius_deg * UNIT_ANGLE))))
+            aeff = windowed_fourier_aeff(Fp[:, p], kx, ky, wcx, wcy, wr)
+            west = aeff_to_mfd(aeff, c.max_mg)
+            waistF[p] = F32(PI_F / west) if west else F32(np.inf)
+    # camera plane (digHolo.cpp:11791-11902)
+    max_focus = F32(0.25)
+    est = [F32(0)] * P
+    attempts = 0
+    valid = False
+    res = None
+    while (not valid or attempts == 0) and attempts < 10:
+        valid = True
+        res = _untilted_fields(frames, c)
+        B = res["field_untilted"].shape[0]
+        for p in range(P):
+            off = F32(((2 * p - 1) * float(ps) * fw / 4.0) * (P - 1))
+            st = res["stats"][p]
+            comx = F32(F32(st["comx"][B]) + off)
+            comy = F32(st["comy"][B])
+            aeff = F32(st["aeff"][B])
+            west = F32(aeff_to_mfd(aeff, c.max_mg) * F32(0.5))
+            est[p] = focus_estimate(west, waistF[p])
+            if np.isnan(comx) or np.isnan(comy) or np.isnan(aeff):
+                valid = False
+                c.window_radius_deg = F32(c.window_radius_deg * F32(0.9))
+            if valid:
+                if align_centre:
+                    c.beam_centre[p] = [comx, comy]
+                if align_waist:
+                    c.waist[p] = west
+                if align_defocus:
+                    c.defocus[p] = F32(0)
+                max_focus = max(max_focus, abs(est[p]))
+            attempts += 1
+    if align_defocus:
+        # the fields of the last camera-plane pass: the Fourier planes of the
+        # windows placed at the reset centres, the beam-centre phase of that pass
+        best = auto_focus(res, c, est)
+        for p in range(P):
+            c.defocus[p] = best[p]
+            max_focus = max(max_focus, abs(best[p]))
+    steps = {"tilt": F32(c.window_radius_deg * F32(0.1)), "centre": F32(c.waist[0] * F32(0.1)),
+             "defocus": F32(F32(0.1) * max_focus), "waist": F32(c.waist[0] * F32(0.1))}
+    c.fft_window = cfg.fft_window
+    return c, steps, {"tilts": tilts, "waist_fourier": waistF, "focus_estimate": est}

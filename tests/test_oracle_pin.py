@@ -231,3 +231,44 @@ def test_lg_transform_is_block_unitary():
         want = np.array([math.sqrt(math.comb(g, k) / 2.0 ** g) for k in range(g + 1)])
         np.testing.assert_allclose(np.sort(mag), np.sort(want), atol=1e-6)
         base += g + 1
+
+
+def test_snap_estimate_matches_live_reference():
+    """The oracle's AutoAlign parameter estimate (auto_align_snap, restating
+    digHoloAutoAlignSnap digHolo.cpp:11517-11970 and digHoloAutoFocus
+    digHolo.cpp:11181-11499) against the reference's ESTIMATE mode from a
+    cold start (beam centres and tilts 0, waist 400 um), without the
+    window-radius rule, low-resolution fields, single-threaded reference.
+    Tilts equal, beam centres within 1 nm, waist within 1e-4 relative,
+    first polarisation's defocus within 1e-3 (the second's is not compared:
+    the reference's focus search reads unwritten memory for it past its
+    22nd trial, digHolo.cpp:11434)."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    import ctypes as C
+    from digholo_b200 import api, synth
+    B = 16
+    kw = dict(synth.WORKLOADS["align_640x512_f32_2pol"])
+    kw.update(frame_count=B, coefs=synth.transfer_coefs(B, 2, kw["max_mg"], 1004))
+    hol = synth.generate(**kw)
+    cfg = config_for(hol, 1)
+    for p in range(2):
+        cfg.beam_centre[p] = [O.F32(0), O.F32(0)]
+        cfg.tilt_deg[p] = [O.F32(0), O.F32(0)]
+        cfg.waist[p] = O.F32(400e-6)
+    fr = np.ascontiguousarray(hol.frames.astype(np.float32))
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    api.configure(L, h, cfg)
+    L.digHoloConfigSetThreadCount(h, 1)
+    L.digHoloSetBatch(h, B, fr.ctypes.data_as(C.POINTER(C.c_float)))
+    L.digHoloConfigSetAutoAlignMode(h, 2)
+    L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
+    L.digHoloAutoAlign(h)
+    c, steps, info = O.auto_align_snap(fr, cfg, align_radius=0)
+    for p in range(2):
+        for ax in range(2):
+            assert L.digHoloConfigGetTilt(h, ax, p) == pytest.approx(float(c.tilt_deg[p][ax]), abs=1e-6)
+            assert abs(L.digHoloConfigGetBeamCentre(h, ax, p) - float(c.beam_centre[p][ax])) <= 1e-9
+    assert abs(L.digHoloConfigGetBasisWaist(h, 0) - float(c.waist[0])) <= 1e-4 * float(c.waist[0])
+    assert abs(L.digHoloConfigGetDefocus(h, 0) - float(c.defocus[0])) <= 1e-3
