@@ -29,8 +29,13 @@ enum { G_TX = 0, G_TY = 1, G_DEF = 2, G_CX = 3, G_CY = 4, G_WAIST = 5 };
 // grad12[pol * 6 + k], k in {tiltX, tiltY, defocus, beamCentreX, beamCentreY,
 // waist} (config units: degrees, dioptre, m, m); parameters tied by the
 // polarisation locks carry the sum on polarisation 0 and zero on 1.
-// ilOut = 10 log10(S).
-int objAlignGradient(Object& o, float* grad12, float* ilOut) {
+// metric 0: IL = 10 log10(S), S = sum |c|^2 (valueOut = IL); metric 1: MDL
+// in dB from the extreme eigenvalues of the batch Gram matrix
+// (valueOut = MDL), its gradient through the eigenvalue derivatives
+// d lambda = u^H dG u (objMdlWeights).
+int objAlignGradient(Object& o, float* grad12, float* ilOut) { return objAlignGradientMetric(o, 0, grad12, ilOut); }
+
+int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
     Config& c = o.cfg;
     if (c.maxMG <= 0) return fail(o, ERR_ERROR, "adjoint AutoAlign needs a modal basis (maxMG > 0)");
     using Clock = std::chrono::steady_clock;
@@ -123,6 +128,13 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
         gp.waist[p] = wv == 0 ? 400e-6f : wv;
     }
     gp.piOverLambda = (float)(PI_DA / c.wavelengthCentre);
+    double mdlDb = 0.0;
+    if (metric == 1) {
+        DH_CUDA(o, o.dGradWeights.ensure((size_t)units * M * sizeof(float2)));
+        r = objMdlWeights(o, o.dGradWeights.as<float2>(), &mdlDb);
+        if (r) return fail(o, r, "MDL gradient: eigenvalues of the batch Gram matrix");
+        gp.weights = o.dGradWeights.as<float2>();
+    }
     DH_CUDA(o, o.dGradOut.ensure((size_t)units * 7 * sizeof(float)));
     gp.out = o.dGradOut.as<float>();
     DH_CUDA(o, dh_launch_align_grad(gp, o.stream));
@@ -145,8 +157,9 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
         for (int k = 0; k < 6; k++) acc[u % P][k] += part[(size_t)u * 7 + k];
         S += part[(size_t)u * 7 + 6];
     }
-    // d IL / d theta = 10 / ln 10 * dS / S, dS = 2 Re sum conj(c) dc
-    const double f = (S > 0) ? 20.0 / std::log(10.0) / S : 0.0;
+    // d IL / d theta = 10 / ln 10 * dS / S, dS = 2 Re sum conj(c) dc;
+    // d MDL / d theta = 20 / ln 10 * Re sum W dc
+    const double f = metric == 1 ? 20.0 / std::log(10.0) : ((S > 0) ? 20.0 / std::log(10.0) / S : 0.0);
     for (int p = 0; p < 2; p++)
         for (int k = 0; k < 6; k++) grad12[p * 6 + k] = p < P ? (float)(f * acc[p][k]) : 0.f;
     if (P > 1) {
@@ -155,7 +168,7 @@ int objAlignGradient(Object& o, float* grad12, float* ilOut) {
         if (c.polLockDefocus) tie(G_DEF);
         if (c.polLockBasisWaist) tie(G_WAIST);
     }
-    if (ilOut) *ilOut = (float)(10.0 * std::log10(S > 0 ? S : 1e-300));
+    if (ilOut) *ilOut = metric == 1 ? (float)mdlDb : (float)(10.0 * std::log10(S > 0 ? S : 1e-300));
     return ERR_SUCCESS;
 }
 
@@ -246,17 +259,20 @@ float objAutoAlignAdjoint(Object& o) {
         for (int i = 0; i < n; i++) setParam(c, prm[i], zz[i] * prm[i].scale);
         if (c.polLockBasisWaist && P > 1) c.waist[1] = c.waist[0];
     };
-    // f = -IL (minimised) and its gradient in step coordinates
+    // f = -metric (IL, then MDL for goal MDL; minimised) and its gradient in
+    // step coordinates
+    int metric = 0;
     auto evalF = [&](const std::vector<double>& zz, double& f, std::vector<double>& gg) -> int {
         apply(zz);
         float g12[12], il = 0.f;
-        const int r = objAlignGradient(o, g12, &il);
+        const int r = objAlignGradientMetric(o, metric, g12, &il);
         o.alignEvaluations++;
         if (r) return r;
         f = -(double)il;
         for (int i = 0; i < n; i++) gg[i] = -(double)g12[prm[i].pol * 6 + prm[i].kind] * prm[i].scale;
         if (c.verbosity >= 2) {
-            fprintf(stderr, "digholo_b200: adjoint AutoAlign evaluation %d: IL %.5f dB, z =", o.alignEvaluations, il);
+            fprintf(stderr, "digholo_b200: adjoint AutoAlign evaluation %d: %s %.5f dB, z =", o.alignEvaluations,
+                    metric ? "MDL" : "IL", il);
             for (int i = 0; i < n; i++) fprintf(stderr, " %.4f", zz[i]);
             fprintf(stderr, "\n");
         }
@@ -265,110 +281,147 @@ float objAutoAlignAdjoint(Object& o) {
     // The FFT window stays where the first evaluation put it; the Fourier
     // window selection and mask are held during a round (the gradient
     // assumes them fixed) and re-selected at the reached point between rounds.
+    // Within a round the tilts move at most about one Fourier-plane pixel
+    // (lambda / (W pixel) radians) from the round's start: beyond that the
+    // selection the round holds is no longer the one the tilt implies, and
+    // the held-window objective stops describing the batch path.  The best
+    // point seen with freshly selected windows is the result.
     o.useSnaps = 1;
     o.fftSnap = o.ifftSnap = c;
-    double f = 0.0;
-    if (n == 0 || evalF(z, f, gz)) {
-        objCalcMetrics(o);
-        return o.autoAlignMetrics[METRIC_IL][0];
-    }
-    // inverse Hessian estimate, initially a scaled identity (first step of unit length)
-    std::vector<double> Hi((size_t)n * n, 0.0);
-    double gn = 0.0;
-    for (double v : gz) gn += v * v;
-    gn = std::sqrt(gn);
-    for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
-    const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.1);   // dB
-    const int maxIter = 60, maxRounds = 4;
-    int quiet = 0, round = 0;
-    bool firstUpdate = true;
-    double lastRoundEnd = f;   // objective at the end of the previous round (before re-selection)
-    std::vector<double> d(n), s(n), y(n), Hy(n);
-    for (int it = 0; it < maxIter; it++) {
-        double slope = 0.0;
-        for (int i = 0; i < n; i++) {
-            double v = 0.0;
-            for (int j = 0; j < n; j++) v -= Hi[(size_t)i * n + j] * gz[j];
-            d[i] = v;
-            slope += v * gz[i];
+    const double tiltTrust = std::max(0.5, (double)(c.wavelengthCentre / (o.geo.W * c.pixelSize)) / UNIT_ANGLE_A / tiltStep);
+    std::vector<char> isTilt(n, 0);
+    for (int i = 0; i < n; i++) isTilt[i] = prm[i].kind == G_TX || prm[i].kind == G_TY;
+    // goal MDL: as the reference's search (digHolo.cpp:12458-12467), a pass
+    // on IL first, then one on the goal
+    const int passes = c.autoAlignGoalIdx == METRIC_MDL ? 2 : 1;
+    for (int pass = 0; pass < passes; pass++) {
+        metric = pass ? METRIC_MDL : METRIC_IL;
+        double f = 0.0;
+        if (n == 0 || evalF(z, f, gz)) {
+            objCalcMetrics(o);
+            return o.autoAlignMetrics[METRIC_IL][0];
         }
-        if (slope >= 0) {   // not a descent direction: restart from the gradient
-            for (int i = 0; i < n; i++) {
-                for (int j = 0; j < n; j++) Hi[(size_t)i * n + j] = (i == j) ? 1.0 / std::max(gn, 1e-12) : 0.0;
-                d[i] = -gz[i] / std::max(gn, 1e-12);
-            }
-            slope = 0.0;
-            for (int i = 0; i < n; i++) slope += d[i] * gz[i];
-        }
-        double t = 1.0, ft = 0.0;
-        bool accepted = false;
-        for (int ls = 0; ls < 6; ls++) {
-            for (int i = 0; i < n; i++) zt[i] = z[i] + t * d[i];
-            if (evalF(zt, ft, gt)) return -FLT_MAX;
-            if (ft <= f + 1e-4 * t * slope) { accepted = true; break; }
-            // minimiser of the quadratic through f, slope and ft, kept in [0.1 t, 0.5 t]
-            const double tq = -slope * t * t / (2.0 * (ft - f - slope * t));
-            t = std::min(0.5 * t, std::max(0.1 * t, tq));
-        }
-        if (!accepted) { apply(z); break; }
-        double sy = 0.0;
-        for (int i = 0; i < n; i++) {
-            s[i] = zt[i] - z[i];
-            y[i] = gt[i] - gz[i];
-            sy += s[i] * y[i];
-        }
-        const double df = f - ft;
-        z = zt;
-        gz = gt;
-        f = ft;
-        gn = 0.0;
+        std::vector<double> zc = z, zBest = z;   // round start (trust box centre), best re-selected point
+        double fBest = f;
+        // inverse Hessian estimate, initially a scaled identity (first step of unit length)
+        std::vector<double> Hi((size_t)n * n, 0.0);
+        double gn = 0.0;
         for (double v : gz) gn += v * v;
         gn = std::sqrt(gn);
-        if (sy > 1e-12) {
-            if (firstUpdate) {
-                // scale the initial estimate by s.y / y.y before the first update
-                double yy = 0.0;
-                for (int i = 0; i < n; i++) yy += y[i] * y[i];
-                for (size_t i = 0; i < Hi.size(); i++) Hi[i] = 0.0;
-                for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = sy / yy;
-                firstUpdate = false;
-            }
-            // BFGS update of the inverse Hessian
-            double yHy = 0.0;
+        for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
+        const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.1);   // dB
+        const int maxIter = 80, maxRounds = 8;
+        int quiet = 0, round = 0;
+        bool firstUpdate = true;
+        double lastRoundEnd = f;   // objective at the end of the previous round (before re-selection)
+        std::vector<double> d(n), s(n), y(n), Hy(n);
+        for (int it = 0; it < maxIter; it++) {
+            double slope = 0.0;
             for (int i = 0; i < n; i++) {
                 double v = 0.0;
-                for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * y[j];
-                Hy[i] = v;
-                yHy += y[i] * v;
+                for (int j = 0; j < n; j++) v -= Hi[(size_t)i * n + j] * gz[j];
+                d[i] = v;
+                slope += v * gz[i];
             }
-            const double rho = 1.0 / sy;
-            for (int i = 0; i < n; i++)
-                for (int j = 0; j < n; j++)
-                    Hi[(size_t)i * n + j] += (1.0 + yHy * rho) * rho * s[i] * s[j] - rho * (Hy[i] * s[j] + s[i] * Hy[j]);
+            if (slope >= 0) {   // not a descent direction: restart from the gradient
+                for (int i = 0; i < n; i++) {
+                    for (int j = 0; j < n; j++) Hi[(size_t)i * n + j] = (i == j) ? 1.0 / std::max(gn, 1e-12) : 0.0;
+                    d[i] = -gz[i] / std::max(gn, 1e-12);
+                }
+                slope = 0.0;
+                for (int i = 0; i < n; i++) slope += d[i] * gz[i];
+            }
+            double t = 1.0, ft = 0.0;
+            bool accepted = false;
+            bool boxed = false;
+            for (int ls = 0; ls < 6; ls++) {
+                boxed = false;
+                for (int i = 0; i < n; i++) {
+                    zt[i] = z[i] + t * d[i];
+                    if (isTilt[i] && std::fabs(zt[i] - zc[i]) > tiltTrust) {
+                        zt[i] = zc[i] + (zt[i] > zc[i] ? tiltTrust : -tiltTrust);
+                        boxed = true;
+                    }
+                }
+                if (evalF(zt, ft, gt)) return -FLT_MAX;
+                if (ft <= f + 1e-4 * t * slope) { accepted = true; break; }
+                // minimiser of the quadratic through f, slope and ft, kept in [0.1 t, 0.5 t]
+                const double tq = -slope * t * t / (2.0 * (ft - f - slope * t));
+                t = std::min(0.5 * t, std::max(0.1 * t, tq));
+            }
+            if (!accepted) { apply(z); break; }
+            double sy = 0.0;
+            for (int i = 0; i < n; i++) {
+                s[i] = zt[i] - z[i];
+                y[i] = gt[i] - gz[i];
+                sy += s[i] * y[i];
+            }
+            const double df = f - ft;
+            z = zt;
+            gz = gt;
+            f = ft;
+            gn = 0.0;
+            for (double v : gz) gn += v * v;
+            gn = std::sqrt(gn);
+            if (sy > 1e-12) {
+                if (firstUpdate) {
+                    // scale the initial estimate by s.y / y.y before the first update
+                    double yy = 0.0;
+                    for (int i = 0; i < n; i++) yy += y[i] * y[i];
+                    for (size_t i = 0; i < Hi.size(); i++) Hi[i] = 0.0;
+                    for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = sy / yy;
+                    firstUpdate = false;
+                }
+                // BFGS update of the inverse Hessian
+                double yHy = 0.0;
+                for (int i = 0; i < n; i++) {
+                    double v = 0.0;
+                    for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * y[j];
+                    Hy[i] = v;
+                    yHy += y[i] * v;
+                }
+                const double rho = 1.0 / sy;
+                for (int i = 0; i < n; i++)
+                    for (int j = 0; j < n; j++)
+                        Hi[(size_t)i * n + j] += (1.0 + yHy * rho) * rho * s[i] * s[j] - rho * (Hy[i] * s[j] + s[i] * Hy[j]);
+            }
+            // converged: a step below the tolerance and a predicted gain of the
+            // next quasi-Newton step (g' H^-1 g / 2) below it too, or two small steps
+            double decrement = 0.0;
+            for (int i = 0; i < n; i++) {
+                double v = 0.0;
+                for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * gz[j];
+                decrement += 0.5 * v * gz[i];
+            }
+            quiet = (df < tol) ? quiet + 1 : 0;
+            if ((quiet >= 1 && decrement < tol) || quiet >= 2 || boxed) {
+                // converged with these windows, or at the edge of the round's
+                // tilt box: re-select the windows at the reached point, unless
+                // the last re-selection and its round gained too little
+                const double gain = lastRoundEnd - f;
+                if (++round >= maxRounds || (round > 1 && gain < tol && !boxed)) break;
+                lastRoundEnd = f;
+                const float ap = o.ifftSnap.apertureSize;
+                o.ifftSnap = c;
+                o.ifftSnap.apertureSize = ap;
+                if (evalF(z, f, gz)) return -FLT_MAX;
+                if (f < fBest) { fBest = f; zBest = z; }
+                zc = z;
+                quiet = 0;
+            }
         }
-        // converged: a step below the tolerance and a predicted gain of the
-        // next quasi-Newton step (g' H^-1 g / 2) below it too, or two small steps
-        double decrement = 0.0;
-        for (int i = 0; i < n; i++) {
-            double v = 0.0;
-            for (int j = 0; j < n; j++) v += Hi[(size_t)i * n + j] * gz[j];
-            decrement += 0.5 * v * gz[i];
-        }
-        quiet = (df < tol) ? quiet + 1 : 0;
-        if ((quiet >= 1 && decrement < tol) || quiet >= 2) {
-            // converged with these windows: re-select them at the reached point
-            // unless the last re-selection and its round gained too little
-            const double gain = lastRoundEnd - f;
-            if (++round >= maxRounds || (round > 1 && gain < tol)) break;
-            lastRoundEnd = f;
+        // the reached point with its windows re-selected, against the best
+        // re-selected point of the pass
+        {
             const float ap = o.ifftSnap.apertureSize;
             o.ifftSnap = c;
             o.ifftSnap.apertureSize = ap;
-            if (evalF(z, f, gz)) return -FLT_MAX;
-            quiet = 0;
+            double fz = 0.0;
+            if (evalF(z, fz, gz)) return -FLT_MAX;
+            if (fz > fBest) z = zBest;
         }
+        apply(z);
     }
-    apply(z);
     // final pass and the metrics of the reached configuration, with the
     // Fourier window re-selected there and the FFT window still where the
     // search found it (the reference's search moves the FFT window only at

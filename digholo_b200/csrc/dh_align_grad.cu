@@ -68,8 +68,9 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
 
     float spow = 0.f;   // captured power of this field
     for (int mode = tid; mode < M; mode += blockDim.x) {
-        const float2 c = p.coefs[(size_t)frame * P * M + (size_t)pol * M + mode];
-        cc[mode] = make_float2(c.x, -c.y);
+        const size_t ci = (size_t)frame * P * M + (size_t)pol * M + mode;
+        const float2 c = p.coefs[ci];
+        cc[mode] = p.weights ? p.weights[ci] : make_float2(c.x, -c.y);
         spow = fmaf(c.x, c.x, fmaf(c.y, c.y, spow));
     }
     // ladder derivatives of the modes with respect to the waist
@@ -143,6 +144,57 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
         for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 7 + tid];
         p.out[(size_t)unit * 7 + tid] = t;
     }
+}
+
+// Weights of an eigenvalue's derivative.  For an eigenpair (lambda, u) of
+// the Gram matrix of the block A (rows = modes of pol0 [and pol1], columns
+// = frames; column-major A[b rows + j]), d lambda = 2 Re sum_jb w_jb dA_jb
+// with w_jb = conj(p_j) q_b and (p, q) = (u, A^H u) for the mode-space Gram
+// A A^H, (A u, u) for the frame-space Gram A^H A.  W[b][pol M + m] +=
+// alpha w_jb, row j < M of pol0, j >= M of pol1.  One thread per (j, b).
+__global__ void k_mdl_weights(const float2* __restrict__ A, int rows, int batch, int rowsGram,
+                              const double2* __restrict__ u, double alpha, int pol0, int pol1, int polCount, int M,
+                              float2* __restrict__ W) {
+    const int total = rows * batch;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int b = e / rows, j = e - b * rows;
+        double2 pj, qb;
+        if (rowsGram) {
+            pj = u[j];
+            double re = 0.0, im = 0.0;   // (A^H u)_b = sum_i conj(A_ib) u_i
+            for (int i = 0; i < rows; i++) {
+                const float2 a = A[(size_t)b * rows + i];
+                re += (double)a.x * u[i].x + (double)a.y * u[i].y;
+                im += (double)a.x * u[i].y - (double)a.y * u[i].x;
+            }
+            qb = make_double2(re, im);
+        } else {
+            double re = 0.0, im = 0.0;   // (A u)_j = sum_c A_jc u_c
+            for (int c = 0; c < batch; c++) {
+                const float2 a = A[(size_t)c * rows + j];
+                re += (double)a.x * u[c].x - (double)a.y * u[c].y;
+                im += (double)a.x * u[c].y + (double)a.y * u[c].x;
+            }
+            pj = make_double2(re, im);
+            qb = u[b];
+        }
+        // conj(p_j) q_b
+        const double wr = pj.x * qb.x + pj.y * qb.y, wi = pj.x * qb.y - pj.y * qb.x;
+        const int pol = j < M ? pol0 : pol1, m = j < M ? j : j - M;
+        float2* wp = W + (size_t)b * polCount * M + (size_t)pol * M + m;
+        wp->x += (float)(alpha * wr);
+        wp->y += (float)(alpha * wi);
+    }
+}
+
+cudaError_t dh_launch_mdl_weights(const float2* A, int rows, int batch, int rowsGram, const double2* u, double alpha,
+                                  int pol0, int pol1, int polCount, int M, float2* W, cudaStream_t s) {
+    const int total = rows * batch;
+    int blocks = (total + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    if (blocks < 1) blocks = 1;
+    k_mdl_weights<<<blocks, 256, 0, s>>>(A, rows, batch, rowsGram, u, alpha, pol0, pol1, polCount, M, W);
+    return cudaGetLastError();
 }
 
 cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const float* kyw, int w, int h, int polCount, int units,

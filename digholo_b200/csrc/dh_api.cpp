@@ -779,6 +779,14 @@ int digHoloB200AutoAlignGradient(int h, float* grad12, float* il) {
     if (!grad12) return dh::ERR_NULLPOINTER;
     return dh::objAlignGradient(*o, grad12, il);
 }
+// Gradient of a metric (0 IL, 1 MDL, both in dB) with the layout of
+// digHoloB200AutoAlignGradient; *value = the metric at the current settings.
+int digHoloB200AutoAlignGradientMetric(int h, int metricIdx, float* grad12, float* value) {
+    OBJ_OR(h, dh::ERR_INVALIDHANDLE);
+    if (!grad12) return dh::ERR_NULLPOINTER;
+    if (metricIdx != 0 && metricIdx != 1) return dh::ERR_INVALIDARGUMENT;
+    return dh::objAlignGradientMetric(*o, metricIdx, grad12, value);
+}
 // Holds the FFT window and the Fourier-window selection and mask at the
 // current settings (enable = 1) while the beam-centre phase, the reference
 // wave and the basis keep following the configuration; 0 releases them.

@@ -21,7 +21,10 @@ cudaError_t dh_launch_gather_block(const float2* src0, const float2* src1, int p
                                    int rows, int batch, float2* A, cudaStream_t s);
 cudaError_t dh_launch_gram(const float2* A, int rows, int batch, int rowsGram, void* G, cudaStream_t s);
 int dh_eigen_values(DhEigen& e, void* G, int n, double* W, cudaStream_t s);
+int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs, cudaStream_t s);
 DhEigen* dh_eigen_create();
+cudaError_t dh_launch_mdl_weights(const float2* A, int rows, int batch, int rowsGram, const double2* u, double alpha,
+                                  int pol0, int pol1, int polCount, int M, float2* W, cudaStream_t s);
 
 namespace dh {
 
@@ -62,6 +65,68 @@ static int blockSingular2(Object& o, const Block& blk, std::vector<double>& s2) 
     if (cudaStreamSynchronize(o.stream) != cudaSuccess) return ERR_ERROR;
     for (double& v : s2) v = v < 0 ? 0 : v;
     std::sort(s2.begin(), s2.end(), [](double a, double b) { return a > b; });
+    return ERR_SUCCESS;
+}
+
+// MDL of the batch (the power meter's SVD path, digHolo.cpp:11012-11062,
+// over all polarisations: blocks as powerMeter forms them) and the weights
+// of its gradient: W[frame][pol M + mode] such that
+//   d MDL_dB = 20 / ln 10 * Re sum W dc,
+// W = w_min / lambda_min - w_max / lambda_max, w of an eigenpair of the
+// block Gram matrix as dh_launch_mdl_weights forms it (lambda_min and
+// lambda_max the extremes over all blocks, from the FP64 eigensolver with
+// their eigenvectors).  Coefficients in the HG basis (the overlap's).
+int objMdlWeights(Object& o, float2* W, double* mdlDb) {
+    const int B = o.batchCount, P = o.polCount, M = o.modeCount;
+    const float2* coefs = o.dCoefs.as<float2>();
+    if (M <= 0 || !coefs || B < 1) return ERR_NULLPOINTER;
+    const bool indep = o.cfg.autoAlignPolIndependence || P == 1;
+    std::vector<Block> blocks;
+    if (P == 1) blocks.push_back({coefs, coefs, 0, 0, M});
+    else if (indep) { blocks.push_back({coefs, coefs, 0, 0, M}); blocks.push_back({coefs, coefs, 1, 1, M}); }
+    else blocks.push_back({coefs, coefs, 0, 1, 2 * M});
+    const int rows = blocks[0].rows, K = (int)blocks.size();
+    const int rowsGram = rows <= B;
+    const int n = rowsGram ? rows : B;
+    const size_t aElems = (size_t)rows * B;
+    if (o.dMetricA.ensure((size_t)K * aElems * sizeof(float2)) != cudaSuccess) return ERR_MEMORYALLOCATION;
+    const size_t gBytes = (size_t)K * n * n * 16, wBytes = (size_t)K * n * sizeof(double), vBytes = (size_t)K * 2 * n * 16;
+    if (o.dMetricG.ensure(gBytes + wBytes + vBytes) != cudaSuccess) return ERR_MEMORYALLOCATION;
+    char* gb = o.dMetricG.as<char>();
+    double* dW = reinterpret_cast<double*>(gb + gBytes);
+    double2* dV = reinterpret_cast<double2*>(gb + gBytes + wBytes);
+    if (!o.eigen) o.eigen = dh_eigen_create();
+    std::vector<double> ev((size_t)K * n);
+    for (int k = 0; k < K; k++) {
+        float2* A = o.dMetricA.as<float2>() + (size_t)k * aElems;
+        const Block& bl = blocks[k];
+        if (dh_launch_gather_block(bl.src0, bl.src1, bl.pol0, bl.pol1, P, M, rows, B, A, o.stream) != cudaSuccess) return ERR_ERROR;
+        void* Gk = gb + (size_t)k * n * n * 16;
+        if (dh_launch_gram(A, rows, B, rowsGram, Gk, o.stream) != cudaSuccess) return ERR_ERROR;
+        if (dh_eigen_solve(*o.eigen, Gk, n, 1, dW + (size_t)k * n, dV + (size_t)k * 2 * n, o.stream)) return ERR_ERROR;
+    }
+    if (cudaMemcpyAsync(ev.data(), dW, ev.size() * sizeof(double), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess)
+        return ERR_ERROR;
+    if (cudaStreamSynchronize(o.stream) != cudaSuccess) return ERR_ERROR;
+    int kmin = 0, kmax = 0;
+    double lmin = DBL_MAX, lmax = -DBL_MAX;
+    for (int k = 0; k < K; k++) {
+        const double a = std::max(0.0, ev[(size_t)k * n]), b = std::max(0.0, ev[(size_t)k * n + n - 1]);
+        if (a < lmin) { lmin = a; kmin = k; }
+        if (b > lmax) { lmax = b; kmax = k; }
+    }
+    if (mdlDb) *mdlDb = (lmin > 0 && lmax > 0) ? 10.0 * std::log10(lmin / lmax) : -DBL_MAX;
+    if (cudaMemsetAsync(W, 0, (size_t)B * P * M * sizeof(float2), o.stream) != cudaSuccess) return ERR_ERROR;
+    if (!(lmin > 0 && lmax > 0)) return ERR_SUCCESS;   // MDL undefined: zero gradient
+    const int sel[2] = {kmin, kmax};
+    const double alpha[2] = {1.0 / lmin, -1.0 / lmax};
+    for (int t = 0; t < 2; t++) {
+        const int k = sel[t];
+        const Block& bl = blocks[k];
+        if (dh_launch_mdl_weights(o.dMetricA.as<float2>() + (size_t)k * aElems, rows, B, rowsGram,
+                                  dV + ((size_t)k * 2 + t) * n, alpha[t], bl.pol0, bl.pol1, P, M, W, o.stream) != cudaSuccess)
+            return ERR_ERROR;
+    }
     return ERR_SUCCESS;
 }
 

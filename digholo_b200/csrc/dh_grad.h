@@ -19,8 +19,13 @@ struct DhGradParams {
     float piOverLambda;
     float waist[2];
     float* out;             // [unit][7]: tx, ty, defocus, bcx, bcy, waist, sum |c|^2
+    // optional weights [frame][pol * M + mode] in place of conj(c): the
+    // kernel then returns Re sum w dc (the MDL gradient's contraction)
+    const float2* weights;
 };
 
 cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const float* kyw, int w, int h, int polCount, int units,
                                    float2* Wx, float2* Wy, cudaStream_t s);
 cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s);
+cudaError_t dh_launch_mdl_weights(const float2* A, int rows, int batch, int rowsGram, const double2* u, double alpha,
+                                  int pol0, int pol1, int polCount, int M, float2* W, cudaStream_t s);

@@ -181,7 +181,7 @@ struct Object {
     DevBuf dSnap[16];                   // AutoAlign parameter estimate: planes, sums, fields, tables
     DevBuf dTransRaw, dTransFrames;     // transposed uint16 input: raw host copy, converted frames
     // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums
-    DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab;
+    DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab, dGradWeights;
     HostBuf hGradOut;
     DhEigen* eigen = nullptr;
     int alignEvaluations = 0;
@@ -255,6 +255,8 @@ int objInverseAux(Object& o, const float2* window, int frameCount, float2* field
                   float* scratchStats);
 int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);
 int objAlignGradient(Object& o, float* grad12, float* ilOut);
+int objAlignGradientMetric(Object& o, int metric, float* grad12, float* valueOut);
+int objMdlWeights(Object& o, float2* W, double* mdlDb);
 float objAutoAlignAdjoint(Object& o);
 int objCalcMetrics(Object& o);
 float objAutoAlign(Object& o);

@@ -90,19 +90,23 @@ class Hologram:
 
 def transfer_coefs(frame_count, pol_count, max_mg, seed, loss_db=1.0):
     """Coefficients of frames that each excite one column of a Haar-random
-    unitary times a per-mode loss uniform in [0, loss_db] dB: frame f of
-    polarisation p carries column (f mod M) of diag(d_p) U_p."""
+    unitary over the modes of all polarisations (pol_count * M square),
+    times a per-mode loss uniform in [0, loss_db] dB: frame f carries column
+    f mod (pol_count * M) of diag(d) U, whose rows split into the
+    polarisations (rows p M .. p M + M - 1 are polarisation p).  The batch
+    coefficient matrix of both polarisations together then has full rank
+    once frame_count >= pol_count * M."""
     rng = np.random.default_rng(seed)
     M = len(hg_indices(max_mg)[0])
+    N = pol_count * M
+    z = (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))) / math.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    q = q * (np.diag(r) / np.abs(np.diag(r)))[None, :]   # Haar: fix the phases of R's diagonal
+    d = 10.0 ** (-rng.uniform(0.0, loss_db, size=N) / 20.0)
+    T = d[:, None] * q
     out = np.zeros((frame_count, pol_count, M), dtype=np.complex128)
-    for p in range(pol_count):
-        z = (rng.standard_normal((M, M)) + 1j * rng.standard_normal((M, M))) / math.sqrt(2.0)
-        q, r = np.linalg.qr(z)
-        q = q * (np.diag(r) / np.abs(np.diag(r)))[None, :]   # Haar: fix the phases of R's diagonal
-        d = 10.0 ** (-rng.uniform(0.0, loss_db, size=M) / 20.0)
-        T = d[:, None] * q
-        for f in range(frame_count):
-            out[f, p] = T[:, f % M]
+    for f in range(frame_count):
+        out[f] = T[:, f % N].reshape(pol_count, M)
     return out
 
 

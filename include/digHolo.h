@@ -391,6 +391,13 @@ const char* digHoloB200GetLastError(int handleIdx);
  * GPU.  Parameters tied by the polarisation locks carry the sum on
  * polarisation 0.  *il (optional) = 10 log10(sum |c|^2). */
 int digHoloB200AutoAlignGradient(int handleIdx, float* grad12, float* il);
+/* The same for metricIdx DIGHOLO_METRIC_IL (0) or DIGHOLO_METRIC_MDL (1):
+ * MDL = 10 log10(s_min^2 / s_max^2) of the batch coefficient matrix (the
+ * power meter's blocks: both polarisations together, or each alone with
+ * AutoAlignPolIndependence), its gradient through the derivatives of the
+ * extreme eigenvalues of the FP64 Gram matrix, d lambda = u^H dG u.
+ * *value (optional) = the metric in dB.  No counterpart in the reference. */
+int digHoloB200AutoAlignGradientMetric(int handleIdx, int metricIdx, float* grad12, float* value);
 /* 1: hold the FFT window and the Fourier-window selection and mask at the
  * current settings (the beam-centre phase, reference wave and basis keep
  * following the configuration), as the gradient assumes; 0: release. */
