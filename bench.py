@@ -580,12 +580,14 @@ def largefield_leg(L, torch, device, stream, no_cpu):
 
 def autoalign_leg(L, torch, device):
     """ms per AutoAlign, plain coordinate search (digHoloAutoAlign, TWEAK) vs
-    the adjoint-driven search (digHoloB200AutoAlignAdjoint), goal IL, on 512
-    frames of 640x512 float32, two polarisations, each frame one column of a
-    Haar-random 120x120 transfer matrix with 0-1 dB per-mode loss, full
-    resolution (IFFT mode 0); the start is off by +60/-60 um in beam centre,
-    +5/-5 % in tilt, +0.2 in defocus and +15 % in waist.  Frames are device
-    resident; each search runs twice on its handle and the second is timed."""
+    the adjoint-driven search (digHoloB200AutoAlignAdjoint), goal IL and goal
+    MDL, on 512 frames of 640x512 float32, two polarisations, each frame one
+    column of a Haar-random 240x240 transfer matrix over both polarisations'
+    120 modes with 0-1 dB per-mode loss, full resolution (IFFT mode 0).  The
+    start is off the true alignment by seeded uniform draws: beam centre
+    +-60 um, tilt +-5 % of the Nyquist angle, defocus +-0.5, waist +-15 %.
+    Frames are device resident; each search runs twice on its handle and
+    the second is timed."""
     import ctypes as C
     import numpy as np
     from digholo_b200 import api, synth
@@ -594,6 +596,8 @@ def autoalign_leg(L, torch, device):
     kw["coefs"] = synth.transfer_coefs(B, 2, kw["max_mg"], 1004)
     hol = synth.generate(**kw)
     frames = torch.from_numpy(np.ascontiguousarray(hol.frames)).to(device)
+    rng = np.random.default_rng(4004)
+    dtilt = synth.carrier_to_tilt_degrees(0.05)
 
     class Cfg:
         pass
@@ -603,37 +607,45 @@ def autoalign_leg(L, torch, device):
     cfg.pol_count, cfg.fft_window, cfg.window_radius_deg = 2, hol.window, hol.radius_deg
     cfg.resolution_mode, cfg.max_mg, cfg.fill_factor = 0, hol.max_mg, 1
     cfg.pol_lock_tilt, cfg.pol_lock_defocus, cfg.pol_lock_waist = 0, 0, 1
-    cfg.beam_centre = [[bc[0] + 60e-6, bc[1] - 60e-6] for bc in hol.beam_centres]
-    cfg.tilt_deg = [[t[0] * 1.05, t[1] * 0.95] for t in hol.tilts_deg]
-    cfg.waist = [hol.waist * 1.15] * 2
-    cfg.defocus = [0.2, 0.2]
-    out = {}
-    for name in ("plain", "adjoint"):
-        h = L.digHoloCreate()
-        ms = None
-        for run in range(2):
-            api.configure(L, h, cfg)
-            L.digHoloSetBatch(h, B, C.cast(C.c_void_p(frames.data_ptr()), C.POINTER(C.c_float)))
-            b, m, p = C.c_int(), C.c_int(), C.c_int()
-            L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
-            L.digHoloConfigSetAutoAlignMode(h, 1)
-            L.digHoloConfigSetAutoAlignGoalIdx(h, 0)
-            L.digHoloConfigSetAutoAlignTol(h, 0.01)
-            L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
-            L.digHoloB200Synchronize(h)
-            t = time.perf_counter()
-            if name == "plain":
-                L.digHoloAutoAlign(h)
-            else:
-                L.digHoloB200AutoAlignAdjoint(h)
-            L.digHoloB200Synchronize(h)
-            ms = (time.perf_counter() - t) * 1e3
-        out[name] = {"ms": ms, "il_db": L.digHoloAutoAlignGetMetric(h, 0), "mdl_db": L.digHoloAutoAlignGetMetric(h, 1),
-                     "evaluations": L.digHoloB200GetAutoAlignEvaluations(h)}
-        L.digHoloDestroy(h)
-    return {"metric": "ms per AutoAlign (goal IL), host wall clock around the call", "workload":
-            "align_640x512_f32_2pol_mode0: 512 frames, Haar 120x120 transfer, perturbed start",
-            "plain": out["plain"], "adjoint": out["adjoint"], "adjoint_over_plain": out["adjoint"]["ms"] / out["plain"]["ms"]}
+    cfg.beam_centre = [[bc[0] + rng.uniform(-60e-6, 60e-6), bc[1] + rng.uniform(-60e-6, 60e-6)]
+                       for bc in hol.beam_centres]
+    cfg.tilt_deg = [[t[0] + rng.uniform(-dtilt, dtilt), t[1] + rng.uniform(-dtilt, dtilt)] for t in hol.tilts_deg]
+    cfg.defocus = [rng.uniform(-0.5, 0.5), rng.uniform(-0.5, 0.5)]
+    cfg.waist = [hol.waist * (1.0 + rng.uniform(-0.15, 0.15))] * 2
+    out = {"metric": "ms per AutoAlign, host wall clock around the call",
+           "workload": "align_640x512_f32_2pol_mode0: 512 frames, Haar 240x240 transfer over both polarisations, "
+                       "perturbed start (centre +-60 um, tilt +-5% Nyquist, defocus +-0.5, waist +-15%)"}
+    for goal, gname in ((0, "goal_il"), (1, "goal_mdl")):
+        res = {}
+        for name in ("plain", "adjoint"):
+            h = L.digHoloCreate()
+            ms = None
+            for run in range(2):
+                api.configure(L, h, cfg)
+                L.digHoloSetBatch(h, B, C.cast(C.c_void_p(frames.data_ptr()), C.POINTER(C.c_float)))
+                b, m, p = C.c_int(), C.c_int(), C.c_int()
+                L.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
+                L.digHoloConfigSetAutoAlignMode(h, 1)
+                L.digHoloConfigSetAutoAlignGoalIdx(h, goal)
+                L.digHoloConfigSetAutoAlignTol(h, 0.01)
+                L.digHoloConfigSetAutoAlignFourierWindowRadius(h, 0)
+                L.digHoloB200Synchronize(h)
+                t = time.perf_counter()
+                if name == "plain":
+                    L.digHoloAutoAlign(h)
+                else:
+                    L.digHoloB200AutoAlignAdjoint(h)
+                L.digHoloB200Synchronize(h)
+                ms = (time.perf_counter() - t) * 1e3
+            res[name] = {"ms": ms, "il_db": L.digHoloAutoAlignGetMetric(h, 0),
+                         "mdl_db": L.digHoloAutoAlignGetMetric(h, 1),
+                         "evaluations": L.digHoloB200GetAutoAlignEvaluations(h)}
+            L.digHoloDestroy(h)
+        key = "il_db" if goal == 0 else "mdl_db"
+        res["adjoint_over_plain"] = res["adjoint"]["ms"] / res["plain"]["ms"]
+        res["goal_delta_db"] = res["adjoint"][key] - res["plain"][key]
+        out[gname] = res
+    return out
 
 
 def H_FRAME(cfg):

@@ -17,11 +17,18 @@
  *
  * The digHoloB200* functions at the end have no counterpart in the
  * reference: they serve callers whose frames are already in device memory.
+ *
+ * The library also exports every reference entry point under its
+ * C++-mangled name (e.g. _Z13digHoloCreatev for digHoloCreate), as the
+ * reference's Linux build names them (digHolo.h:148-156), so programs
+ * compiled with g++ against the reference's header link and run unchanged.
+ * Defining DIGHOLO_CXX_LINKAGE before including this header in C++ declares
+ * the functions with C++ linkage, i.e. under those names.
  */
 #ifndef DIGHOLO_B200_H
 #define DIGHOLO_B200_H
 
-#ifdef __cplusplus
+#if defined(__cplusplus) && !defined(DIGHOLO_CXX_LINKAGE)
 extern "C" {
 #endif
 
@@ -444,7 +451,7 @@ int digHoloB200EigenHermitian(int n, const double* G, double* W, double* vecs);
 int digHoloB200ProcessBatchNoAlloc(int handleIdx, const void* frames, int frameCount, int framesAreUint16,
                                    complex64* coefs, short* fieldR, short* fieldI, float* stats);
 
-#ifdef __cplusplus
+#if defined(__cplusplus) && !defined(DIGHOLO_CXX_LINKAGE)
 }
 #endif
 

@@ -138,3 +138,51 @@ def test_no_cpu_fallback(lib):
     b, m, p = C.c_int(), C.c_int(), C.c_int()
     assert not lib.digHoloProcessBatch(h, C.byref(b), C.byref(m), C.byref(p))
     assert b"CUDA" in lib.digHoloB200GetLastError(h)
+
+
+def _mangled_aliases():
+    path = os.path.join(ROOT, "digholo_b200", "csrc", "_build", "mangled.ld")
+    out = {}
+    for line in open(path):
+        m = re.match(r"(\S+) = (\w+);", line.strip())
+        if m:
+            out[m.group(2)] = m.group(1)
+    return out
+
+
+def test_cxx_mangled_aliases_exported():
+    """Every reference entry point is exported under its C++-mangled name
+    too (the reference's Linux exports are mangled: EXT_C is empty there,
+    digHolo.h:148-156), as an alias of the C-linkage function."""
+    import digholo_b200
+    raw = C.CDLL(digholo_b200.LIB_PATH)
+    aliases = _mangled_aliases()
+    ref_names = [n for n in _declared() if not n.startswith("digHoloB200")]
+    assert sorted(aliases) == sorted(ref_names)
+    missing = [m for m in aliases.values() if not hasattr(raw, m)]
+    assert not missing, missing
+
+
+def test_cxx_mangled_names_match_reference_build():
+    """The mangled names equal the reference build's own exports for every
+    entry point both libraries have, and calls through them behave like the
+    C names (a g++-built caller of the reference relinks unchanged)."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    import digholo_b200
+    from digholo_b200 import abi
+    table = ref_lib._symbol_map()
+    aliases = _mangled_aliases()
+    shared = [n for n in table if n in aliases]
+    assert len(shared) >= 100
+    assert {n: table[n] for n in shared} == {n: aliases[n] for n in shared}
+    raw = C.CDLL(digholo_b200.LIB_PATH)
+    M = abi.bind(raw, resolver=table.get)
+    h = M.digHoloCreate()
+    assert h >= 0
+    assert M.digHoloConfigSetFrameDimensions(h, 640, 512) == 0
+    w, hh = C.c_int(), C.c_int()
+    assert M.digHoloConfigGetFrameDimensions(h, C.byref(w), C.byref(hh)) == 0
+    assert (w.value, hh.value) == (640, 512)
+    assert M.digHoloConfigSetPolCount(h, 2) == 0 and M.digHoloConfigGetPolCount(h) == 2
+    assert M.digHoloDestroy(h) == 0
