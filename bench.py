@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--inverse-kernel", type=int, default=0,
                     help="digHoloB200SetInverseKernel choice (0 automatic; 3 forward and inverse fused into "
                          "one launch where they can be)")
+    ap.add_argument("--no-c3", action="store_true",
+                    help="skip the uneven-batch measurement (200 batches of 1-4096 frames, two frame sizes)")
     ap.add_argument("--no-largefield", action="store_true",
                     help="skip the large-field measurement (2048x2048 frames, 512x512 fields, 465 modes)")
     return ap.parse_args()
@@ -476,6 +478,13 @@ def main():
         except Exception as exc:
             large = {"unavailable": str(exc)}
 
+    c3 = None
+    if not args.no_c3:
+        try:
+            c3 = c3_leg(L, torch, device, stream)
+        except Exception as exc:
+            c3 = {"unavailable": str(exc)}
+
     align = None
     if not args.no_autoalign:
         try:
@@ -506,6 +515,7 @@ def main():
         "cpu_baseline": cpu,
         "autoalign": align,
         "largefield": large,
+        "uneven_batches": c3,
     }
     print(json.dumps(line))
     L.digHoloDestroy(h)
@@ -574,6 +584,97 @@ def largefield_leg(L, torch, device, stream, no_cpu):
         except Exception as exc:
             out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % exc}
     del batches
+    torch.cuda.empty_cache()
+    return out
+
+
+def c3_leg(L, torch, device, stream):
+    """Uneven streamed batches: 200 batches, frame counts log-uniform in
+    [1, 4096], frames 320x256 or 1280x1024 float32 (two polarisations, 12-bit
+    values of the synth.py hologram model, carrier (0.25, 0.2) Nyquist),
+    maxMG from {6, 9, 15}, FFT windows from {64, 128, 256} (1280x1024) or
+    {32, 64} (320x256: a 16-pixel window is smaller than the Fourier window
+    of this carrier), low-resolution fields.  The frames come from two
+    device-resident pools of 4096 frames (21.5 GB and 1.3 GB); batch k uses
+    the first n_k frames of its pool.  The sequence runs with the built-in
+    kernel choice (FFTW plan mode ESTIMATE) and with tuned kernel plans
+    (MEASURE; an untimed pass plans every shape first); CUDA events on the
+    handles' stream around the whole sequence."""
+    import ctypes as C
+    import numpy as np
+    from digholo_b200 import api, synth
+    rng = np.random.default_rng(3003)
+    pools, cfgs = {}, {}
+    for fw, fh in ((320, 256), (1280, 1024)):
+        hol = synth.generate(frame_count=1, frame_width=fw, frame_height=fh, pol_count=2, max_mg=9, waist=fw * 0.4e-6,
+                             snr_db=30, window=(fw // 5, fw // 5), dtype="float32", seed=3004)
+
+        class G:
+            pass
+        g = G()
+        g.frame_width, g.frame_height, g.pol_count, g.max_mg = fw, fh, 2, 9
+        g.pixel_size, g.beam_centre, g.waist = hol.pixel_size, hol.beam_centres, [hol.waist] * 2
+        g.snr_db, g.taper = 30, False
+        pools[fw] = torch_frames(g, 4096, 3005 + fw, device).float()
+        cfgs[fw] = hol
+    torch.cuda.synchronize()
+    batches = []
+    for k in range(200):
+        fw = 1280 if rng.random() < 0.5 else 320
+        n = int(min(4096, max(1, round(float(np.exp(rng.uniform(0.0, np.log(4096))))))))
+        mg = int(rng.choice([6, 9, 15]))
+        win = int(rng.choice([64, 128, 256] if fw == 1280 else [32, 64]))
+        batches.append((fw, n, mg, win))
+    total = sum(b[1] for b in batches)
+
+    def configure(h, fw, mg, win):
+        hol = cfgs[fw]
+        L.digHoloConfigSetFrameDimensions(h, fw, 1024 if fw == 1280 else 256)
+        L.digHoloConfigSetFramePixelSize(h, float(hol.pixel_size))
+        L.digHoloConfigSetWavelengthCentre(h, float(hol.wavelength))
+        L.digHoloConfigSetPolCount(h, 2)
+        L.digHoloConfigSetfftWindowSize(h, win, win)
+        L.digHoloConfigSetFourierWindowRadius(h, float(hol.radius_deg))
+        L.digHoloConfigSetIFFTResolutionMode(h, 1)
+        L.digHoloConfigSetBasisGroupCount(h, mg)
+        for p in range(2):
+            L.digHoloConfigSetBasisWaist(h, p, float(win * 2.5e-6))
+            L.digHoloConfigSetBeamCentre(h, 0, p, float(hol.beam_centres[p][0]))
+            L.digHoloConfigSetBeamCentre(h, 1, p, float(hol.beam_centres[p][1]))
+            L.digHoloConfigSetTilt(h, 0, p, float(hol.tilts_deg[p][0]))
+            L.digHoloConfigSetTilt(h, 1, p, float(hol.tilts_deg[p][1]))
+
+    def run(plan, timed):
+        hs = {fw: L.digHoloCreate() for fw in pools}
+        for h in hs.values():
+            L.digHoloB200SetStream(h, C.c_void_p(stream.cuda_stream))
+            L.digHoloConfigSetFFTWPlanMode(h, plan)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for fw, n, mg, win in batches:
+            h = hs[fw]
+            configure(h, fw, mg, win)
+            L.digHoloSetBatch(h, n, C.cast(C.c_void_p(pools[fw].data_ptr()), C.POINTER(C.c_float)))
+            if L.digHoloB200ProcessBatchDevice(h) != 0:
+                raise RuntimeError("C3 batch failed: %s" % L.digHoloB200GetLastError(h))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        for h in hs.values():
+            L.digHoloDestroy(h)
+        return e0.elapsed_time(e1)
+    run(0, False)                        # warm: buffers, bases, tensor maps
+    ms_default = run(0, True)
+    runs0 = L.digHoloB200GetKernelPlanRuns()
+    run(1, False)                        # plans every shape (untimed)
+    plans = L.digHoloB200GetKernelPlanRuns() - runs0
+    ms_planned = run(1, True)
+    out = {"metric": "frames/s over the whole sequence, device-resident frames",
+           "batches": len(batches), "frames": total, "shapes_planned": plans,
+           "default": {"ms": ms_default, "value": total / (ms_default / 1e3), "unit": "frames/s"},
+           "planned": {"ms": ms_planned, "value": total / (ms_planned / 1e3), "unit": "frames/s"},
+           "planned_over_default": ms_default / ms_planned}
+    del pools
     torch.cuda.empty_cache()
     return out
 

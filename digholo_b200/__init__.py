@@ -58,6 +58,8 @@ def _bind_extensions(lib, out):
         "digHoloB200AutoAlignAdjoint": (_C.c_float, [_C.c_int]),
         "digHoloB200AutoAlignGradientMetric": (_C.c_int, [_C.c_int, _C.c_int, P(_C.c_float), P(_C.c_float)]),
         "digHoloB200FreezeWindow": (_C.c_int, [_C.c_int, _C.c_int]),
+        "digHoloB200GetKernelPlan": (_C.c_int, [_C.c_int, P(_C.c_int), P(_C.c_int), P(_C.c_float)]),
+        "digHoloB200GetKernelPlanRuns": (_C.c_int, []),
         "digHoloB200EigenHermitian": (_C.c_int, [_C.c_int, P(_C.c_double), P(_C.c_double), P(_C.c_double)]),
         "digHoloB200ProcessBatchNoAlloc": (_C.c_int, [_C.c_int, _C.c_void_p, _C.c_int, _C.c_int, _C.c_void_p,
                                                      _C.c_void_p, _C.c_void_p, _C.c_void_p]),

@@ -373,7 +373,9 @@ int digHoloConfigGetThreadCount(int h) { OBJ_OR(h, 0); return o->cfg.threadCount
 // digHolo.h:1924-1937
 int digHoloConfigSetVerbosity(int h, int v) { OBJ_OR(h, dh::ERR_INVALIDHANDLE); o->cfg.verbosity = v; return 0; }
 int digHoloConfigGetVerbosity(int h) { OBJ_OR(h, 0); return o->cfg.verbosity; }
-// digHolo.h:1808-1818: FFTW planning mode has no meaning on this build; stored only
+// digHolo.h:1808-1818: planning mode 0 (estimate) uses the built-in kernel
+// choice; 1-3 (measure, patient, exhaustive) tune the forward and inverse
+// kernels by timing on the first batch of each shape (dh_object.cpp)
 int digHoloConfigSetFFTWPlanMode(int h, int m) {
     OBJ_OR(h, dh::ERR_INVALIDHANDLE);
     if (m < 0 || m >= 4) return dh::ERR_INVALIDARGUMENT;
@@ -381,6 +383,16 @@ int digHoloConfigSetFFTWPlanMode(int h, int m) {
     return dh::ERR_SUCCESS;
 }
 int digHoloConfigGetFFTWPlanMode(int h) { OBJ_OR(h, 0); return o->cfg.fftwPlanMode; }
+// digHolo.h:1825 and 1835: the kernel plans play the part of FFTW's wisdom
+int digHoloFFTWWisdomForget() { return dh::planForget(); }
+int digHoloFFTWWisdomFilename(const char* filename) { return dh::planFilename(filename); }
+int digHoloB200GetKernelPlan(int h, int* fwd, int* inv, float* ms) {
+    OBJ_OR(h, 0);
+    std::lock_guard<std::mutex> guard(o->lock);
+    if (!o->preparedValid) return 0;
+    return dh::objPlanLookup(*o, fwd, inv, ms);
+}
+int digHoloB200GetKernelPlanRuns() { return dh::planRuns(); }
 
 // AutoAlign switches (digHolo.h:938-1136)
 #define DH_FLAG(NAME, FIELD)                                                                           \

@@ -11,7 +11,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
+#include <cfloat>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
 #include <vector>
 
 size_t dh_forward_smem_bytes(int logW, int logH, int colChunk);
@@ -1220,11 +1226,176 @@ int objProcessBatch(Object& o, int syncCoefs) {
     return processBatchLocked(o, syncCoefs);
 }
 
+// ------------------------------------------------------------------ kernel planner
+// The counterpart of the reference's FFTW planning (digHoloConfigSetFFTWPlanMode,
+// digHolo.h:1808; FFTW_MEASURE and up time candidate plans, digHolo.cpp:7439-7531,
+// and keep them as wisdom, digHolo.cpp:7424-7437): with plan mode 1-3 and
+// automatic kernel choices, the first batch of each shape (frame and window
+// sizes, polarisations, pixel type, frame source, resolution mode, mode
+// groups, batch size rounded up to a power of two up to 512, overlap choice)
+// is also run through every forward x inverse kernel pair that supports it,
+// each timed with CUDA events on up to 512 of its frames (best of 1, 3 or 5
+// runs for MEASURE, PATIENT, EXHAUSTIVE), and the fastest pair is used for
+// every later batch of that shape.  The table is process-wide like FFTW's wisdom; with a wisdom file
+// named (digHoloFFTWWisdomFilename) it is loaded from it before the first
+// lookup and written back after every new entry.
+
+namespace {
+struct PlanEntry {
+    int fwd, inv;
+    float ms;
+};
+std::mutex gPlanLock;
+std::map<std::string, PlanEntry> gPlans;
+std::string gPlanFile;
+bool gPlanLoaded = true;
+int gPlanRuns = 0;
+const char* kPlanHeader = "digholo_b200 kernel plans v1";
+
+void planLoadLocked() {
+    if (gPlanLoaded) return;
+    gPlanLoaded = true;
+    std::ifstream f(gPlanFile);
+    std::string line;
+    if (!f || !std::getline(f, line) || line != kPlanHeader) return;
+    while (std::getline(f, line)) {
+        const size_t t = line.find('\t');
+        if (t == std::string::npos) continue;
+        std::istringstream v(line.substr(t + 1));
+        PlanEntry e;
+        if (v >> e.fwd >> e.inv >> e.ms) gPlans[line.substr(0, t)] = e;
+    }
+}
+
+void planSaveLocked() {
+    if (gPlanFile.empty()) return;
+    std::ofstream f(gPlanFile, std::ios::trunc);
+    if (!f) return;
+    f << kPlanHeader << "\n";
+    for (const auto& kv : gPlans) f << kv.first << "\t" << kv.second.fwd << " " << kv.second.inv << " " << kv.second.ms << "\n";
+}
+
+std::string planKey(const Object& o) {
+    const Geometry& g = o.geo;
+    int bucket = 1;   // batch sizes by powers of two up to the planner's 512-frame trials
+    while (bucket < o.batchCount && bucket < 512) bucket <<= 1;
+    char k[256];
+    snprintf(k, sizeof(k), "%d %d %d %d %d %d %d %d %d %d %d %d %d", o.cfg.frameWidth, o.cfg.frameHeight, o.polCount,
+             o.framesU16, o.framesOnDevice, g.W, g.H, g.w, g.h, o.cfg.resolutionIdx, o.cfg.maxMG, bucket, o.overlapKernel);
+    return k;
+}
+}  // namespace
+
+int planForget() {
+    std::lock_guard<std::mutex> g(gPlanLock);
+    gPlans.clear();
+    return ERR_SUCCESS;
+}
+int planFilename(const char* filename) {
+    std::lock_guard<std::mutex> g(gPlanLock);
+    gPlanFile = filename ? filename : "";
+    gPlanLoaded = gPlanFile.empty();
+    return ERR_SUCCESS;
+}
+int planRuns() {
+    std::lock_guard<std::mutex> g(gPlanLock);
+    return gPlanRuns;
+}
+
+// The tuned pair for the handle's current shape (after a batch was prepared): 1 if there is one.
+int objPlanLookup(Object& o, int* fwd, int* inv, float* ms) {
+    std::lock_guard<std::mutex> g(gPlanLock);
+    planLoadLocked();
+    auto it = gPlans.find(planKey(o));
+    if (it == gPlans.end()) return 0;
+    if (fwd) *fwd = it->second.fwd;
+    if (inv) *inv = it->second.inv;
+    if (ms) *ms = it->second.ms;
+    return 1;
+}
+
+// Times every forward x inverse pair on (up to 512 frames of) the batch just
+// processed (frames as staged for it: fp) and records the fastest; the
+// winner then runs once more over the whole batch so that the batch's
+// outputs are its.
+static int planBatch(Object& o, const DhFwdParams& fp, const DhInvParams& ip) {
+    const int B = o.batchCount, BT = std::min(B, 512);
+    const int saveF = o.forwardKernel, saveI = o.inverseKernel, saveT = o.timing;
+    const std::string saveErr = o.lastError;
+    const int reps = o.cfg.fftwPlanMode >= 3 ? 5 : (o.cfg.fftwPlanMode == 2 ? 3 : 1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DH_CUDA(o, cudaEventCreate(&e0));
+    DH_CUDA(o, cudaEventCreate(&e1));
+    PlanEntry best{0, 0, FLT_MAX};
+    static const int fwds[] = {4, 3, 2, 5, 1};
+    static const int invs[] = {0, 1, 2, 3};
+    o.timing = 0;
+    o.quietErrors = 1;
+    for (int f : fwds) {
+        for (int i : invs) {
+            if (i == 3 && f != 4) continue;                         // fused only with the tensor-core forward
+            if (i == 2 && o.cfg.resolutionIdx != 0) continue;       // bands: full resolution
+            o.forwardKernel = f;
+            o.inverseKernel = i;
+            int r = launchChunk(o, fp, ip, 0, BT);
+            cudaError_t ce = cudaStreamSynchronize(o.stream);
+            if (r || ce != cudaSuccess || objCheckStatus(o)) { cudaGetLastError(); continue; }
+            float ms = FLT_MAX;
+            for (int k = 0; k < reps && r == 0; k++) {
+                cudaEventRecord(e0, o.stream);
+                r = launchChunk(o, fp, ip, 0, BT);
+                cudaEventRecord(e1, o.stream);
+                if (cudaEventSynchronize(e1) != cudaSuccess) r = ERR_ERROR;
+                float t = 0.f;
+                if (r == 0 && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) ms = std::min(ms, t);
+            }
+            cudaGetLastError();
+            if (r == 0 && ms < best.ms) best = PlanEntry{f, i, ms};
+        }
+    }
+    o.quietErrors = 0;
+    o.timing = saveT;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int r = ERR_SUCCESS;
+    if (best.ms < FLT_MAX) {
+        o.forwardKernel = best.fwd;
+        o.inverseKernel = best.inv;
+        r = launchChunk(o, fp, ip, 0, B);
+        std::lock_guard<std::mutex> g(gPlanLock);
+        planLoadLocked();
+        gPlans[planKey(o)] = best;
+        gPlanRuns++;
+        planSaveLocked();
+    }
+    o.forwardKernel = saveF;
+    o.inverseKernel = saveI;
+    o.lastError = saveErr;
+    return r;
+}
+
 static int processBatchLocked(Object& o, int syncCoefs) {
     int r = prepare(o);
     if (r) return r;
     r = updateBasis(o);
     if (r) return r;
+    // kernel planner: the tuned kernel pair for this shape, or a tuning run
+    // after this batch (plan modes above ESTIMATE, automatic kernel choices)
+    struct ChoiceRestore {
+        Object& o; int f, i; bool active;
+        ~ChoiceRestore() { if (active) { o.forwardKernel = f; o.inverseKernel = i; } }
+    } choiceRestore{o, o.forwardKernel, o.inverseKernel, false};
+    bool planNeeded = false;
+    if (o.cfg.fftwPlanMode > 0 && o.forwardKernel == 0 && o.inverseKernel == 0 && o.avgCount <= 1 && !o.useSnaps) {
+        int pf = 0, pi = 0;
+        if (objPlanLookup(o, &pf, &pi, nullptr)) {
+            o.forwardKernel = pf;
+            o.inverseKernel = pi;
+            choiceRestore.active = true;
+        } else {
+            planNeeded = true;
+        }
+    }
     const Geometry& g = o.geo;
     const int B = o.batchCount, P = o.polCount;
     if (o.modeCount > 0) DH_CUDA(o, o.dCoefs.ensure((size_t)B * P * o.modeCount * sizeof(float2)));
@@ -1298,6 +1469,14 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     }
     o.lastFwdValid = 1;
     o.fourierValid = 0;
+    if (planNeeded) {
+        DhFwdParams pfp = o.lastFwd;
+        pfp.frameCount = B;
+        r = planBatch(o, pfp, ip);
+        if (r) return r;
+        r = applyBasis(o);
+        if (r) return r;
+    }
     if (syncCoefs) return objCoefsToHost(o);
     return ERR_SUCCESS;
 }

@@ -201,6 +201,7 @@ struct Object {
     // shape allows, 1 FP32 CUDA cores; and the one that ran last (1 FP32, 2 tensor)
     int overlapKernel = 0;
     int lastOverlapKernel = 0;
+    int quietErrors = 0;                // kernel planner trials: launch failures are expected, not printed
     int* hStatus = nullptr;             // host-mapped failure flag written by the kernels
     int* dStatus = nullptr;             // its device address
 
@@ -224,8 +225,10 @@ inline int fail(Object& o, int code, const char* what) {
 inline int failCuda(Object& o, cudaError_t e, const char* where) {
     std::string m = std::string(where) + ": " + cudaGetErrorString(e);
     o.lastError = m;
-    fprintf(stderr, "digholo_b200: %s\n", m.c_str());
-    fflush(stderr);
+    if (!o.quietErrors) {
+        fprintf(stderr, "digholo_b200: %s\n", m.c_str());
+        fflush(stderr);
+    }
     return ERR_ERROR;
 }
 #define DH_CUDA(o, call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return failCuda(o, e_, #call); } while (0)
@@ -247,6 +250,12 @@ int objUpdateBasis(Object& o);
 int objProcessForAlign(Object& o);
 int objCheckStatus(Object& o);
 void objReleaseGraphs(Object& o);
+// Kernel planner (plan modes above ESTIMATE): process-wide table of tuned
+// kernel choices, saved to and loaded from the wisdom file.
+int planForget();
+int planFilename(const char* filename);
+int planRuns();
+int objPlanLookup(Object& o, int* forwardKernel, int* inverseKernel, float* ms);
 // The coefficients the API returns: in the configured basis after a batch
 // (modeCountOut modes per polarisation), else the HG coefficients.
 const float2* objOutputCoefs(const Object& o);

@@ -306,6 +306,12 @@ int digHoloConfigGetThreadCount(int handleIdx);
 int digHoloConfigSetFFTWPlanMode(int handleIdx, int planningMode);
 /* replaces digHolo.h:1818 */
 int digHoloConfigGetFFTWPlanMode(int handleIdx);
+/* replaces digHolo.h:1825: forgets the tuned kernel plans (the wisdom of
+ * plan modes 1-3), not the wisdom file */
+int digHoloFFTWWisdomForget();
+/* replaces digHolo.h:1835: the file the tuned kernel plans are loaded from
+ * (before the next lookup) and saved to (after every new plan) */
+int digHoloFFTWWisdomFilename(const char* filename);
 /* replaces digHolo.h:1924 */
 int digHoloConfigSetVerbosity(int handleIdx, int verbosity);
 /* replaces digHolo.h:1937 */
@@ -417,6 +423,14 @@ float digHoloB200AutoAlignAdjoint(int handleIdx);
 /* Number of batch evaluations (window selection, tilt removal, overlap and
  * power meter) the last digHoloAutoAlign call made. */
 int digHoloB200GetAutoAlignEvaluations(int handleIdx);
+
+/* No counterpart in the reference.  The kernel plan tuned for the handle's
+ * current shape (plan modes 1-3, see digHoloConfigSetFFTWPlanMode): returns 1
+ * and the forward / inverse kernel choices (as digHoloB200SetForwardKernel /
+ * SetInverseKernel number them) and the batch time in ms, or 0 when the shape
+ * has no plan.  digHoloB200GetKernelPlanRuns: tuning runs in this process. */
+int digHoloB200GetKernelPlan(int handleIdx, int* forwardKernel, int* inverseKernel, float* ms);
+int digHoloB200GetKernelPlanRuns();
 
 /* No counterpart in the reference (its power meter calls LAPACK cgesvd).
  * Eigenvalues of one Hermitian n x n matrix, FP64, with the GPU solver
