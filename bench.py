@@ -61,6 +61,10 @@ def parse():
                          "one launch where they can be)")
     ap.add_argument("--no-c3", action="store_true",
                     help="skip the uneven-batch measurement (200 batches of 1-4096 frames, two frame sizes)")
+    ap.add_argument("--largefield-only", action="store_true",
+                    help="run only the large-field measurement and print its JSON (for profiling)")
+    ap.add_argument("--largefield-frames", type=int, default=256,
+                    help="frames per batch of the large-field measurement")
     ap.add_argument("--no-largefield", action="store_true",
                     help="skip the large-field measurement (2048x2048 frames, 512x512 fields, 465 modes)")
     return ap.parse_args()
@@ -331,6 +335,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import digholo_b200
     L = digholo_b200.load()
+    if args.largefield_only:
+        stream = torch.cuda.Stream(device)
+        torch.cuda.set_stream(stream)
+        print(json.dumps(largefield_leg(L, torch, device, stream, True, args.largefield_frames)))
+        return 0
     cfg = workload_config(args.mode, args.frames)
     B = args.frames
     P, W, H = cfg.pol_count, cfg.fft_window[0], cfg.fft_window[1]
@@ -524,7 +533,7 @@ def main():
     return 0
 
 
-def largefield_leg(L, torch, device, stream, no_cpu):
+def largefield_leg(L, torch, device, stream, no_cpu, frames=256):
     """frames/s on the large-field workload: 256 frames of 2048x2048 uint16,
     two polarisations, FFT window 512x512, full resolution (IFFT mode 0,
     the reference's default: 512x512 fields by the band kernels), maxMG 30
@@ -535,7 +544,7 @@ def largefield_leg(L, torch, device, stream, no_cpu):
     import ctypes as C
     import numpy as np
     from digholo_b200 import api
-    B, steps, warmup = 256, 5, 3
+    B, steps, warmup = frames, 5, 3
     cfg = workload_config(0, B, "largefield_2048_u16_2pol")
     batches = [torch_frames(cfg, B, 5000 + i, device) for i in range(2)]
     torch.cuda.synchronize()
