@@ -22,6 +22,10 @@
 
 using namespace dh;
 
+bool dh_plane_window64_fits(const DhFourierParams& q);
+cudaError_t dh_launch_plane_rows512(const DhFourierParams& q, int compact, cudaStream_t s);
+cudaError_t dh_launch_plane_window64(const DhFourierParams& q, cudaStream_t s);
+
 
 namespace {
 
@@ -270,7 +274,18 @@ cudaError_t dh_launch_forward_plane(const DhFourierParams& q, cudaStream_t s) {
     DhFourierParams qw = q;
     qw.windowCols = 1;
     (void)Nx;
-    k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(qw);
+    // 512-pixel rows: the register row kernel; with 64-row windows its
+    // compact output feeds the pruned column kernel (dh_plane.cu)
+    const bool fits64 = dh_plane_window64_fits(qw);
+    e = dh_launch_plane_rows512(qw, fits64 ? 1 : 0, s);
+    if (e == cudaSuccess) {
+        if (fits64) return dh_launch_plane_window64(qw, s);
+    } else if (e != cudaErrorNotSupported) {
+        return e;
+    } else {
+        cudaGetLastError();
+        k_fourier_rows<<<(unsigned)(units * (H / RB)), FT, smemR, s>>>(qw);
+    }
     k_fourier_cols<<<(unsigned)(units * ((f.w + CB - 1) / CB)), FT, smemC, s>>>(qw);
     const int total = units * f.h * f.w;
     int g = (total + 255) / 256;

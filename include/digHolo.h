@@ -363,8 +363,10 @@ int digHoloB200GetGeometry(int handleIdx, int* out10);
  * and alignment allow, else the register kernel, else the generic one),
  * 1 generic shared-memory kernel, 2 register kernel, 3 TMA-fed kernel only,
  * 4 tensor-core row-DFT kernel only (uint16 frames, 128-row FFT windows 64
- * or 128 wide, 16- or 32-pixel IFFT windows), 5 full R2C planes (rows, then
- * columns, then the window; automatic for windows 256 pixels wide or more);
+ * or 128 wide, 16- or 32-pixel IFFT windows), 5 R2C planes (rows, then
+ * columns, then the window; automatic for windows 256 pixels wide or more;
+ * 512-pixel rows by a register transform and, for 64-row IFFT windows, only
+ * the window's columns and rows computed);
  * the batch fails where the chosen kernel does not apply. */
 int digHoloB200SetForwardKernel(int handleIdx, int kernel);
 /* Forward kernel the last batch ran: 1 generic, 2 register, 3 TMA-fed,
