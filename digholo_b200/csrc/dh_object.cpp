@@ -28,6 +28,9 @@ cudaError_t dh_launch_forward_i8(const DhFwdParams& p, cudaStream_t s);
 cudaError_t dh_launch_forward_i8_fused(const DhFwdParams& p, const DhInvParams& ip, cudaStream_t s);
 cudaError_t dh_launch_fourier_full(const DhFourierParams& q, cudaStream_t s);
 cudaError_t dh_launch_forward_plane(const DhFourierParams& q, cudaStream_t s);
+size_t dh_field_band64_scratch_bytes(const DhInvParams& p, int overlapKind);
+cudaError_t dh_launch_field_band64(const DhInvParams& p, int overlapKind, void* scratch, size_t scratchBytes,
+                                   int* overlapUsed, cudaStream_t s);
 int dh_forward_i8_npad(int w);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
@@ -813,6 +816,25 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp, bool mayAlloc
 // Full-resolution fields by bands of 64 rows (any field size); its scratch
 // grows here unless the caller may not allocate.
 static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) {
+    // 512-wide fields with IFFT windows up to 64 x 64: 64-point sub-transforms
+    // and the exact integer overlap (dh_band64.cu)
+    const size_t need64 = dh_field_band64_scratch_bytes(ip, o.overlapKernel);
+    if (need64 > 0) {
+        if (o.dBigScratch.bytes < need64) {
+            if (!mayAlloc) return cudaErrorMemoryAllocation;
+            cudaError_t e = o.dBigScratch.ensure(need64);
+            if (e != cudaSuccess) return e;
+        }
+        int used = 0;
+        cudaError_t e = dh_launch_field_band64(ip, o.overlapKernel, o.dBigScratch.ptr, o.dBigScratch.bytes, &used, o.stream);
+        if (e == cudaSuccess) {
+            o.lastInverseKernel = 7;
+            o.lastOverlapKernel = used;
+            return e;
+        }
+        if (e != cudaErrorNotSupported) return e;
+        cudaGetLastError();
+    }
     const size_t need = dh_field_big_scratch_bytes(ip, o.overlapKernel);
     if (need == 0) return cudaErrorNotSupported;
     if (o.dBigScratch.bytes < need) {

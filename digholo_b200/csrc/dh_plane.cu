@@ -9,7 +9,8 @@
 // 512 pixels is the complex sequence z[n] = f[2n] + i f[2n+1] of 256 points,
 // transformed as 16 x 16 in registers: each thread takes z[16 n1 + t], a
 // 16-point DFT over n1, the twiddle exp(-2 pi i t k1 / 256), one exchange
-// through shared memory (padded rows), a 16-point DFT over n2; then the R2C
+// through the row's own shared buffer (XOR-swizzled, warp barriers only), a
+// 16-point DFT over n2; then the R2C
 // split of the kept kx columns only.  Frame rows arrive by 16-byte loads.
 //
 // k_plane_window64: the column stage for 64x64 IFFT windows, only the 64
@@ -90,14 +91,14 @@ __device__ __forceinline__ void dft8(float2 (&v)[8]) {
 
 constexpr int RR = 16;           // rows per block
 constexpr int RN = 256;          // complex points per row (W = 512)
-constexpr int EXS = 17;          // padded exchange row
 
 // compact = 1: the kept columns only, rows of w values ([unit][H][w]);
-// compact = 0: the plane's layout ([unit][H][W/2 + 1]).
+// compact = 0: the plane's layout ([unit][H][W/2 + 1]).  A row's 16 threads
+// are 16 lanes of one warp, so its exchange needs only warp barriers; the
+// exchange reuses the row's buffer, value (k1, t) at 16 k1 + (t ^ k1).
 __global__ void __launch_bounds__(256) k_plane_rows512(DhFourierParams q, int compact) {
     extern __shared__ float2 sp[];
-    float2* A = sp;                          // [RR][RN] z, then X
-    float2* E = sp + RR * RN;                // [RR][16][EXS] exchange
+    float2* A = sp;                          // [RR][RN] z, the exchange, then X
     const DhFwdParams& f = q.f;
     const int H = 1 << f.logH, Nx = RN + 1;
     const int groups = H / RR;
@@ -105,48 +106,62 @@ __global__ void __launch_bounds__(256) k_plane_rows512(DhFourierParams q, int co
     const int P = f.polCount, pol = unit % P, frame = unit / P;
     const long long base = (long long)frame * f.frameStride + (long long)(f.cy[pol] + r0) * f.frameWidth + f.cx[pol];
     const int tid = threadIdx.x;
-    // rows in by 16-byte loads (8 uint16 or 4 float pixels each)
+    // rows in by 16-byte loads (8 uint16 or 4 float pixels each), all issued
+    // before the first shared-memory store
     if (f.inputU16) {
         const unsigned short* fr = static_cast<const unsigned short*>(f.frames);
-        for (int e = tid; e < RR * 64; e += 256) {
-            const int r = e >> 6, c = e & 63;
-            const uint4 u = __ldg(reinterpret_cast<const uint4*>(fr + base + (long long)r * f.frameWidth + 8 * c));
-            float2* d = A + r * RN + 4 * c;
-            d[0] = make_float2((float)(u.x & 0xFFFFu), (float)(u.x >> 16));
-            d[1] = make_float2((float)(u.y & 0xFFFFu), (float)(u.y >> 16));
-            d[2] = make_float2((float)(u.z & 0xFFFFu), (float)(u.z >> 16));
-            d[3] = make_float2((float)(u.w & 0xFFFFu), (float)(u.w >> 16));
+        uint4 u[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int e = tid + 256 * i, rr = e >> 6, c = e & 63;
+            u[i] = __ldg(reinterpret_cast<const uint4*>(fr + base + (long long)rr * f.frameWidth + 8 * c));
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int e = tid + 256 * i, rr = e >> 6, c = e & 63;
+            float4* d = reinterpret_cast<float4*>(A + rr * RN + 4 * c);
+            d[0] = make_float4((float)(u[i].x & 0xFFFFu), (float)(u[i].x >> 16), (float)(u[i].y & 0xFFFFu),
+                               (float)(u[i].y >> 16));
+            d[1] = make_float4((float)(u[i].z & 0xFFFFu), (float)(u[i].z >> 16), (float)(u[i].w & 0xFFFFu),
+                               (float)(u[i].w >> 16));
         }
     } else {
         const float* fr = static_cast<const float*>(f.frames);
-        for (int e = tid; e < RR * 128; e += 256) {
-            const int r = e >> 7, c = e & 127;
-            const float4 u = __ldg(reinterpret_cast<const float4*>(fr + base + (long long)r * f.frameWidth + 4 * c));
-            float2* d = A + r * RN + 2 * c;
-            d[0] = make_float2(u.x, u.y);
-            d[1] = make_float2(u.z, u.w);
+        float4 u[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int e = tid + 256 * i, rr = e >> 7, c = e & 127;
+            u[i] = __ldg(reinterpret_cast<const float4*>(fr + base + (long long)rr * f.frameWidth + 4 * c));
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int e = tid + 256 * i, rr = e >> 7, c = e & 127;
+            *reinterpret_cast<float4*>(A + rr * RN + 2 * c) = u[i];
         }
     }
     __syncthreads();
     const int r = tid >> 4, t = tid & 15;
+    float2* Ar = A + r * RN;
     float2 v[16];
     // first pass: n = 16 n1 + t, DFT over n1, twiddle exp(-2 pi i t k1 / 256)
 #pragma unroll
-    for (int n1 = 0; n1 < 16; n1++) v[n1] = A[r * RN + 16 * n1 + t];
+    for (int n1 = 0; n1 < 16; n1++) v[n1] = Ar[16 * n1 + t];
     dft16(v);
+    __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 16; k1++) {
         float2 y = at16(v, k1);
         if (k1 && t) y = cmul(y, __ldg(&f.twiddle[(t * k1) << (TW_LOG - 8)]));
-        E[(r * 16 + k1) * EXS + t] = y;
+        Ar[16 * k1 + (t ^ k1)] = y;
     }
-    __syncthreads();
+    __syncwarp();
     // second pass: thread t now holds k1 = t, DFT over n2; X[t + 16 k2]
 #pragma unroll
-    for (int n2 = 0; n2 < 16; n2++) v[n2] = E[(r * 16 + t) * EXS + n2];
+    for (int n2 = 0; n2 < 16; n2++) v[n2] = Ar[16 * t + (n2 ^ t)];
     dft16(v);
+    __syncwarp();
 #pragma unroll
-    for (int k2 = 0; k2 < 16; k2++) A[r * RN + t + 16 * k2] = at16(v, k2);
+    for (int k2 = 0; k2 < 16; k2++) Ar[t + 16 * k2] = at16(v, k2);
     __syncthreads();
     // R2C split of the kept columns: F[k] = (Z[k] + conj Z[N-k]) / 2 - i e^{-2 pi i k / 512} (Z[k] - conj Z[N-k]) / 2
     const int kcount = q.windowCols ? f.w : Nx;
@@ -275,7 +290,7 @@ cudaError_t dh_launch_plane_rows512(const DhFourierParams& q, int compact, cudaS
     }
     const int units = f.frameCount * f.polCount;
     if (units <= 0) return cudaSuccess;
-    const size_t smem = sizeof(float2) * ((size_t)RR * RN + (size_t)RR * 16 * EXS);
+    const size_t smem = sizeof(float2) * (size_t)RR * RN;
     cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_plane_rows512), (int)smem);
     if (e != cudaSuccess) return e;
     k_plane_rows512<<<(unsigned)(units * ((1 << f.logH) / RR)), 256, smem, s>>>(q, compact);

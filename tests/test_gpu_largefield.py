@@ -2,7 +2,7 @@
 window 512 x 512 (IFFT window 64 x 64), maxMG 30 (465 modes), waist 600 um,
 20 dB SNR, 1/(group + 1) amplitude taper; both IFFT resolution modes, a few
 frames.  In mode 0 the 512 x 512 fields take the band kernels, with the
-overlap in split-BF16 on the tensor cores and in FP32 on the CUDA cores,
+overlap exact in integers on the tensor cores and in FP32 on the CUDA cores,
 each scored against the FP64 overlap of the same int16 fields (the quantised
 oracle) with the worst mode group printed.  Tolerances as in
 test_gpu_parity: int16 fields within 2 LSB of the quantised oracle, field
@@ -52,7 +52,8 @@ def test_largefield_vs_oracle_and_reference(lib, hol, mode, overlap):
     kern, used = lib.digHoloB200GetInverseKernel(h), lib.digHoloB200GetOverlapKernel(h)
     lib.digHoloDestroy(h)
     if mode == 0:
-        assert kern == 4 and used == (2 if overlap == 0 else 1)
+        # tensor cores: the 64-point band kernel with the exact integer overlap
+        assert (kern, used) == ((7, 3) if overlap == 0 else (4, 1))
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert g["R"].shape == o["R"].shape
     assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
@@ -60,7 +61,7 @@ def test_largefield_vs_oracle_and_reference(lib, hol, mode, overlap):
     err = rel_l2(g["coefs"], o["coefs"])
     per = _per_group(g["coefs"], o["coefs"], cfg.max_mg)
     print("mode %d %s overlap: coefficient rel L2 %.2e, worst mode group %.2e (group %d)"
-          % (mode, "split-BF16" if used == 2 else "FP32", err, per.max(), int(per.argmax())))
+          % (mode, {2: "split-BF16", 3: "integer"}.get(used, "FP32"), err, per.max(), int(per.argmax())))
     assert err <= (1e-4 if used == 2 else 5e-5)
     if ref_lib.available():
         L = ref_lib.load()
