@@ -61,6 +61,9 @@ def _bind_extensions(lib, out):
         "digHoloB200GetKernelPlan": (_C.c_int, [_C.c_int, P(_C.c_int), P(_C.c_int), P(_C.c_float)]),
         "digHoloB200GetKernelPlanRuns": (_C.c_int, []),
         "digHoloB200EigenHermitian": (_C.c_int, [_C.c_int, P(_C.c_double), P(_C.c_double), P(_C.c_double)]),
+        "digHoloB200FrameSimulatorDevice": (_C.c_int, [_C.c_int, _C.c_int, _C.c_int, _C.c_float, _C.c_int] +
+                                            [P(_C.c_float)] * 6 + [_C.c_int] + [P(_C.c_float)] * 4 +
+                                            [_C.c_int, _C.c_int, P(_C.c_float), _C.c_int, _C.c_void_p, _C.c_void_p]),
         "digHoloB200ProcessBatchNoAlloc": (_C.c_int, [_C.c_int, _C.c_void_p, _C.c_int, _C.c_int, _C.c_void_p,
                                                      _C.c_void_p, _C.c_void_p, _C.c_void_p]),
     }

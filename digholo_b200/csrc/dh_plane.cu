@@ -92,91 +92,107 @@ __device__ __forceinline__ void dft8(float2 (&v)[8]) {
 constexpr int RR = 16;           // rows per block
 constexpr int RN = 256;          // complex points per row (W = 512)
 
+constexpr int NG = 4;            // row groups per block, the next one's pixels prefetched into registers
+
+// Loads of row group g (16 rows of one unit): 16-byte loads, 8 uint16 or 4
+// float pixels each, into registers.
+template <bool U16>
+struct RowRaw {
+    static constexpr int N = U16 ? 4 : 8;
+    uint4 u[N];
+    __device__ __forceinline__ void load(const DhFwdParams& f, int unit, int r0, int tid) {
+        const int P = f.polCount, pol = unit % P, frame = unit / P;
+        const long long base = (long long)frame * f.frameStride + (long long)(f.cy[pol] + r0) * f.frameWidth + f.cx[pol];
+        const int es = U16 ? 2 : 4;
+        const unsigned char* fr = static_cast<const unsigned char*>(f.frames) + base * es;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const int e = tid + 256 * i, rr = e / (N * 16), c = e % (N * 16);
+            u[i] = __ldg(reinterpret_cast<const uint4*>(fr + ((long long)rr * f.frameWidth) * es + 16 * c));
+        }
+    }
+    // as complex pairs z[n] = f[2n] + i f[2n + 1] into rows of RN
+    __device__ __forceinline__ void store(float2* A, int tid) const {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const int e = tid + 256 * i, rr = e / (N * 16), c = e % (N * 16);
+            if (U16) {
+                float4* d = reinterpret_cast<float4*>(A + rr * RN + 4 * c);
+                d[0] = make_float4((float)(u[i].x & 0xFFFFu), (float)(u[i].x >> 16), (float)(u[i].y & 0xFFFFu),
+                                   (float)(u[i].y >> 16));
+                d[1] = make_float4((float)(u[i].z & 0xFFFFu), (float)(u[i].z >> 16), (float)(u[i].w & 0xFFFFu),
+                                   (float)(u[i].w >> 16));
+            } else {
+                *reinterpret_cast<uint4*>(A + rr * RN + 2 * c) = u[i];
+            }
+        }
+    }
+};
+
 // compact = 1: the kept columns only, rows of w values ([unit][H][w]);
-// compact = 0: the plane's layout ([unit][H][W/2 + 1]).  A row's 16 threads
-// are 16 lanes of one warp, so its exchange needs only warp barriers; the
-// exchange reuses the row's buffer, value (k1, t) at 16 k1 + (t ^ k1).
-__global__ void __launch_bounds__(256) k_plane_rows512(DhFourierParams q, int compact) {
+// compact = 0: the plane's layout ([unit][H][W/2 + 1]).  A block takes NG
+// consecutive groups of 16 rows.  A row's 16 threads are 16 lanes of one
+// warp, so its exchange needs only warp barriers; the exchange reuses the
+// row's buffer, value (k1, t) at 16 k1 + (t ^ k1).
+template <bool U16>
+__global__ void __launch_bounds__(256, 3) k_plane_rows512(DhFourierParams q, int compact) {
     extern __shared__ float2 sp[];
     float2* A = sp;                          // [RR][RN] z, the exchange, then X
     const DhFwdParams& f = q.f;
     const int H = 1 << f.logH, Nx = RN + 1;
     const int groups = H / RR;
-    const int unit = blockIdx.x / groups, r0 = (blockIdx.x % groups) * RR;
-    const int P = f.polCount, pol = unit % P, frame = unit / P;
-    const long long base = (long long)frame * f.frameStride + (long long)(f.cy[pol] + r0) * f.frameWidth + f.cx[pol];
+    const int total = f.frameCount * f.polCount * groups;
+    const int g0 = blockIdx.x * NG;
     const int tid = threadIdx.x;
-    // rows in by 16-byte loads (8 uint16 or 4 float pixels each), all issued
-    // before the first shared-memory store
-    if (f.inputU16) {
-        const unsigned short* fr = static_cast<const unsigned short*>(f.frames);
-        uint4 u[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int e = tid + 256 * i, rr = e >> 6, c = e & 63;
-            u[i] = __ldg(reinterpret_cast<const uint4*>(fr + base + (long long)rr * f.frameWidth + 8 * c));
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int e = tid + 256 * i, rr = e >> 6, c = e & 63;
-            float4* d = reinterpret_cast<float4*>(A + rr * RN + 4 * c);
-            d[0] = make_float4((float)(u[i].x & 0xFFFFu), (float)(u[i].x >> 16), (float)(u[i].y & 0xFFFFu),
-                               (float)(u[i].y >> 16));
-            d[1] = make_float4((float)(u[i].z & 0xFFFFu), (float)(u[i].z >> 16), (float)(u[i].w & 0xFFFFu),
-                               (float)(u[i].w >> 16));
-        }
-    } else {
-        const float* fr = static_cast<const float*>(f.frames);
-        float4 u[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int e = tid + 256 * i, rr = e >> 7, c = e & 127;
-            u[i] = __ldg(reinterpret_cast<const float4*>(fr + base + (long long)rr * f.frameWidth + 4 * c));
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int e = tid + 256 * i, rr = e >> 7, c = e & 127;
-            *reinterpret_cast<float4*>(A + rr * RN + 2 * c) = u[i];
-        }
-    }
-    __syncthreads();
     const int r = tid >> 4, t = tid & 15;
     float2* Ar = A + r * RN;
-    float2 v[16];
-    // first pass: n = 16 n1 + t, DFT over n1, twiddle exp(-2 pi i t k1 / 256)
+    RowRaw<U16> raw;
+    raw.load(f, g0 / groups, (g0 % groups) * RR, tid);
+    for (int gi = 0; gi < NG; gi++) {
+        const int g = g0 + gi;
+        if (g >= total) break;
+        const int unit = g / groups, r0 = (g % groups) * RR;
+        const int pol = unit % f.polCount;
+        __syncthreads();   // the previous group's split has read A
+        raw.store(A, tid);
+        if (gi + 1 < NG && g + 1 < total) raw.load(f, (g + 1) / groups, ((g + 1) % groups) * RR, tid);
+        __syncthreads();
+        float2 v[16];
+        // first pass: n = 16 n1 + t, DFT over n1, twiddle exp(-2 pi i t k1 / 256)
 #pragma unroll
-    for (int n1 = 0; n1 < 16; n1++) v[n1] = Ar[16 * n1 + t];
-    dft16(v);
-    __syncwarp();
+        for (int n1 = 0; n1 < 16; n1++) v[n1] = Ar[16 * n1 + t];
+        dft16(v);
+        __syncwarp();
 #pragma unroll
-    for (int k1 = 0; k1 < 16; k1++) {
-        float2 y = at16(v, k1);
-        if (k1 && t) y = cmul(y, __ldg(&f.twiddle[(t * k1) << (TW_LOG - 8)]));
-        Ar[16 * k1 + (t ^ k1)] = y;
-    }
-    __syncwarp();
-    // second pass: thread t now holds k1 = t, DFT over n2; X[t + 16 k2]
+        for (int k1 = 0; k1 < 16; k1++) {
+            float2 y = at16(v, k1);
+            if (k1 && t) y = cmul(y, __ldg(&f.twiddle[(t * k1) << (TW_LOG - 8)]));
+            Ar[16 * k1 + (t ^ k1)] = y;
+        }
+        __syncwarp();
+        // second pass: thread t now holds k1 = t, DFT over n2; X[t + 16 k2]
 #pragma unroll
-    for (int n2 = 0; n2 < 16; n2++) v[n2] = Ar[16 * t + (n2 ^ t)];
-    dft16(v);
-    __syncwarp();
+        for (int n2 = 0; n2 < 16; n2++) v[n2] = Ar[16 * t + (n2 ^ t)];
+        dft16(v);
+        __syncwarp();
 #pragma unroll
-    for (int k2 = 0; k2 < 16; k2++) Ar[t + 16 * k2] = at16(v, k2);
-    __syncthreads();
-    // R2C split of the kept columns: F[k] = (Z[k] + conj Z[N-k]) / 2 - i e^{-2 pi i k / 512} (Z[k] - conj Z[N-k]) / 2
-    const int kcount = q.windowCols ? f.w : Nx;
-    const int kbeg = q.windowCols ? f.sx0[pol] : 0;
-    const int pitch = compact ? kcount : Nx, o0 = compact ? kbeg : 0;
-    float2* out = q.plane + ((size_t)unit * H + r0) * pitch;
-    for (int e = tid; e < RR * kcount; e += 256) {
-        const int rr = e / kcount, k = kbeg + (e - rr * kcount);
-        const float2 zk = A[rr * RN + (k & (RN - 1))];
-        const float2 zc = cconj(A[rr * RN + ((RN - k) & (RN - 1))]);
-        const float2 even = cscale(cadd(zk, zc), 0.5f);
-        const float2 d = csub(zk, zc);
-        const float2 odd = make_float2(0.5f * d.y, -0.5f * d.x);
-        const float2 wk = __ldg(&f.twiddle[k << (TW_LOG - 9)]);
-        out[(size_t)rr * pitch + (k - o0)] = cadd(even, cmul(wk, odd));
+        for (int k2 = 0; k2 < 16; k2++) Ar[t + 16 * k2] = at16(v, k2);
+        __syncthreads();
+        // R2C split of the kept columns: F[k] = (Z[k] + conj Z[N-k]) / 2 - i e^{-2 pi i k / 512} (Z[k] - conj Z[N-k]) / 2
+        const int kcount = q.windowCols ? f.w : Nx;
+        const int kbeg = q.windowCols ? f.sx0[pol] : 0;
+        const int pitch = compact ? kcount : Nx, o0 = compact ? kbeg : 0;
+        float2* out = q.plane + ((size_t)unit * H + r0) * pitch;
+        for (int e = tid; e < RR * kcount; e += 256) {
+            const int rr = e / kcount, k = kbeg + (e - rr * kcount);
+            const float2 zk = A[rr * RN + (k & (RN - 1))];
+            const float2 zc = cconj(A[rr * RN + ((RN - k) & (RN - 1))]);
+            const float2 even = cscale(cadd(zk, zc), 0.5f);
+            const float2 d = csub(zk, zc);
+            const float2 odd = make_float2(0.5f * d.y, -0.5f * d.x);
+            const float2 wk = __ldg(&f.twiddle[k << (TW_LOG - 9)]);
+            out[(size_t)rr * pitch + (k - o0)] = cadd(even, cmul(wk, odd));
+        }
     }
 }
 
@@ -291,9 +307,12 @@ cudaError_t dh_launch_plane_rows512(const DhFourierParams& q, int compact, cudaS
     const int units = f.frameCount * f.polCount;
     if (units <= 0) return cudaSuccess;
     const size_t smem = sizeof(float2) * (size_t)RR * RN;
-    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_plane_rows512), (int)smem);
-    if (e != cudaSuccess) return e;
-    k_plane_rows512<<<(unsigned)(units * ((1 << f.logH) / RR)), 256, smem, s>>>(q, compact);
+    const unsigned blocks = (unsigned)((units * ((1 << f.logH) / RR) + NG - 1) / NG);
+    if (f.inputU16) {
+        k_plane_rows512<true><<<blocks, 256, smem, s>>>(q, compact);
+    } else {
+        k_plane_rows512<false><<<blocks, 256, smem, s>>>(q, compact);
+    }
     return cudaGetLastError();
 }
 

@@ -463,4 +463,7 @@ int objAutoAlignSnap(Object& o, float steps[4]) {
     return ERR_SUCCESS;
 }
 
+// AeffToMFD for the frame simulator's default beam waist.
+float aeffToMfdPublic(float aeff, int groups) { return aeffToMfd(aeff, groups); }
+
 }  // namespace dh

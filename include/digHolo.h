@@ -316,6 +316,23 @@ int digHoloFFTWWisdomFilename(const char* filename);
 int digHoloConfigSetVerbosity(int handleIdx, int verbosity);
 /* replaces digHolo.h:1937 */
 int digHoloConfigGetVerbosity(int handleIdx);
+/* replaces digHolo.h:2026: synthetic camera frames, computed on the GPU,
+ * returned in one host allocation ([float32 frames][uint16 frames]
+ * [parameters]) released by digHoloFrameSimulatorDestroy; null arrays take
+ * the reference's defaults and are pointed at them; wavelengthOrdering is
+ * accepted (the reference's frames do not depend on it) */
+float* digHoloFrameSimulatorCreate(int frameCount, int* frameWidth, int* frameHeight, float* pixelSize, int* polCount,
+                                   float** refTiltX, float** refTiltY, float** refDefocus, float** refWaist,
+                                   float** refBeamCentreX, float** refBeamCentreY, complex64** refAmplitude,
+                                   int* beamGroupCount, float** beamWaist, complex64** beamCoefs, float** beamCentreX,
+                                   float** beamCentreY, int* cameraPixelLevelCount, int fillFactorCorrection,
+                                   float** wavelengths, int* wavelengthCount, int wavelengthOrdering, int printToConsole,
+                                   unsigned short** pixelBuffer16, const char* fname);
+/* replaces digHolo.h:2046 */
+float* digHoloFrameSimulatorCreateSimple(int frameCount, int frameWidth, int frameHeight, float pixelSize, int polCount,
+                                         float wavelength, int printToConsole);
+/* replaces digHolo.h:2056 */
+int digHoloFrameSimulatorDestroy(float* pixelBuffer);
 
 /* ------------------------------------------------------------------------
  * Extensions with no counterpart in the reference.
@@ -441,6 +458,20 @@ int digHoloB200GetKernelPlanRuns();
  * double) the unit eigenvectors of the smallest and the largest eigenvalue.
  * n up to 2048.  Runs on the current device and waits for it. */
 int digHoloB200EigenHermitian(int n, const double* G, double* W, double* vecs);
+
+/* No counterpart in the reference.  digHoloFrameSimulatorCreate with the
+ * frames left in device memory: the same parameters by value (null arrays
+ * take the same defaults; frame sides must be multiples of 16), frames32 a
+ * device buffer of frameCount x frameHeight x frameWidth float32 (required:
+ * the intensities are formed there), frames16 an optional device uint16
+ * buffer of the same shape.  Returns a DIGHOLO_ERROR code. */
+int digHoloB200FrameSimulatorDevice(int frameCount, int frameWidth, int frameHeight, float pixelSize, int polCount,
+                                    const float* refTiltX, const float* refTiltY, const float* refDefocus,
+                                    const float* refWaist, const float* refBeamCentreX, const float* refBeamCentreY,
+                                    int beamGroupCount, const float* beamWaist, const complex64* beamCoefs,
+                                    const float* beamCentreX, const float* beamCentreY, int cameraPixelLevelCount,
+                                    int fillFactorCorrection, const float* wavelengths, int wavelengthCount,
+                                    float* frames32, unsigned short* frames16);
 
 /* No counterpart in the reference.  The batch path for callers that cannot
  * allocate device memory while they process frames (a real-time acquisition

@@ -1119,3 +1119,132 @@ def auto_align_snap(frames, cfg, align_tilt=1, align_defocus=1, align_centre=1, 
              "defocus": F32(F32(0.1) * max_focus), "waist": F32(c.waist[0] * F32(0.1))}
     c.fft_window = cfg.fft_window
     return c, steps, {"tilts": tilts, "waist_fourier": waistF, "focus_estimate": est}
+
+
+def frame_simulator(frame_count, frame_width, frame_height, pixel_size, pol_count, ref_tilt_x=None, ref_tilt_y=None,
+                    ref_defocus=None, ref_waist=None, ref_centre_x=None, ref_centre_y=None, group_count=0,
+                    beam_waist=None, beam_coefs=None, beam_centre_x=None, beam_centre_y=None, levels=16384,
+                    fill_factor=1, wavelengths=None):
+    """frameSimulatorCreate (digHolo.cpp:15930-16760) for small cases: the
+    frames (float32, quantised, and uint16) and the resolved parameters.
+
+    The reference's region axes are transposed against its frame layout: its
+    x axis (beam centre x, reference tilt x, HG index n) runs along the
+    frame's rows and its y axis along a polarisation region's columns
+    (digHolo.cpp:16371-16385 with generateModeSeparable's transpose,
+    digHolo.cpp:1610-1760).  The field is accumulated in the reference's
+    float32 order: first mode's term plus the reference wave, then every later
+    mode with nonzero coefficient power and the last mode; the fill-factor
+    sinc filter is applied in FP64 (FFTW's single-precision rounding differs
+    in the last bits); quantisation against the pre-filter maximum with
+    round-half-even (digHolo.cpp:15847-15873).  With no group count and a
+    frame count that is not triangular, the one-hot default coefficients use
+    the final mode count (the reference reads memory it never wrote there).
+    """
+    W = 16 * (frame_width // 16)
+    H = 16 * (frame_height // 16)
+    P = min(pol_count, 2)
+    ps = F32(pixel_size if pixel_size > 0 else 20e-6)
+    if levels < 2 or levels > 65536:
+        levels = 65536
+    G = group_count
+    if G <= 0:
+        m, g = 0, 1
+        while m < frame_count:
+            m += g
+            g += 1
+        G = g - 1 if m == frame_count else g
+    M = G * (G + 1) // 2
+    wl = [F32(1565e-9)] if wavelengths is None else [F32(v) for v in wavelengths]
+    k0 = F32(0)
+    for v in wl:
+        k0 = F32(k0 + F32(F32(2 * PI_F) / v))
+    k0 = F32(k0 / F32(len(wl)))
+    lam0 = F32(F32(2 * PI_F) / k0)
+    wmax = F32(lam0 / F32(2 * ps))
+    unit = F32(PI_F / F32(180))
+    tilt_max = F32(float(wmax) * (1 - 0.32037724101704079249230971981887705624103546142578125) / float(unit))
+    rows, cols = H, W // P
+    off = [F32((float(ps) * (W // P) / 2.0) * (P * p - (P - 1))) for p in range(P)]
+    pick = lambda arr, p, d: F32(arr[p]) if arr is not None else F32(d)
+    tx = [pick(ref_tilt_x, p, tilt_max) for p in range(P)]
+    ty = [pick(ref_tilt_y, p, -tilt_max) for p in range(P)]
+    df = [pick(ref_defocus, p, 0) for p in range(P)]
+    rw = [pick(ref_waist, p, 0) for p in range(P)]
+    rcx = [pick(ref_centre_x, p, off[p]) for p in range(P)]
+    rcy = [pick(ref_centre_y, p, 0) for p in range(P)]
+    bcx = [pick(beam_centre_x, p, off[p]) for p in range(P)]
+    bcy = [pick(beam_centre_y, p, 0) for p in range(P)]
+    if beam_waist is None:
+        r = F32(0.25 * min(rows, cols) * float(ps))
+        w = F32(aeff_to_mfd(F32(PI_F * r * r), G) * F32(0.5))
+        bw = [w] * P
+    else:
+        bw = [F32(v) for v in beam_waist]
+    if beam_coefs is None:
+        coefs = np.zeros((frame_count, P, M), dtype=np.complex64)
+        for f in range(min(frame_count, M)):
+            coefs[f, :, f] = 1
+    else:
+        coefs = np.asarray(beam_coefs, dtype=np.complex64).reshape(frame_count, P, M)
+    idx = hg_index(G)
+    out = np.zeros((frame_count, H, W), dtype=F32)
+    vmax = F32(0)
+    for p in range(P):
+        ax_r = (ps * (np.arange(rows) - rows // 2).astype(F32) + F32(off[p] - bcx[p])).astype(F32)
+        ax_c = (ps * (np.arange(cols) - cols // 2).astype(F32) + F32(-bcy[p])).astype(F32)
+        qr, sr = quantise_modes(hg_modes(ax_r, bw[p], G))
+        qc, sc = quantise_modes(hg_modes(ax_c, bw[p], G))
+        ref = []
+        for ax_len, ctr, kt, axis_idx in ((rows, rcx[p], tx[p], 0), (cols, rcy[p], ty[p], 1)):
+            shift = F32(off[p] - ctr) if axis_idx == 0 else F32(-ctr)
+            a = (ps * (np.arange(ax_len) - ax_len // 2).astype(F32) + shift).astype(F32)
+            kr = F32(k0 * F32(np.sin(F32(kt * unit))))
+            kf = F32(k0 * F32(F32(0.5) * df[p]))
+            r2 = (a * a).astype(F32)
+            arg = (kr * a + kf * r2).astype(F32)
+            A0 = F32(np.sqrt(F32(1.0) / F32(ax_len)))
+            A = (A0 * np.exp(-r2 / F32(rw[p] * rw[p]))).astype(F32) if rw[p] * rw[p] > 0 else np.full(ax_len, A0, F32)
+            ref.append(((A * np.cos(arg)).astype(F32), (A * np.sin(arg)).astype(F32)))
+        (rrr, rri), (rcr, rci) = ref
+        # cmul(column factor, row factor) with the real part fused
+        ref_re = (rcr[None, :].astype(np.float64) * rrr[:, None] - (rci[None, :] * rri[:, None]).astype(F32)).astype(F32)
+        ref_im = (rcr[None, :].astype(np.float64) * rri[:, None] + (rci[None, :] * rrr[:, None]).astype(F32)).astype(F32)
+        for f in range(frame_count):
+            fr = fi = None
+            for k, (m, n) in enumerate(idx):
+                c = coefs[f, p, k]
+                cR = F32(float(sc[m]) * float(sr[n]) * float(c.real))
+                cI = F32(float(sc[m]) * float(sr[n]) * float(c.imag))
+                if not (F32(cR * cR + cI * cI) > 0 or k == 0 or k == M - 1):
+                    continue
+                v = (qr[n].astype(np.int32)[:, None] * qc[m].astype(np.int32)[None, :]).astype(F32)
+                tr, ti = (v * cR).astype(F32), (v * cI).astype(F32)
+                if fr is None:
+                    fr, fi = (ref_re + tr).astype(F32), (ref_im + ti).astype(F32)
+                else:
+                    fr, fi = (tr + fr).astype(F32), (ti + fi).astype(F32)
+            I = ((fr * fr).astype(F32) + (fi * fi).astype(F32)).astype(F32)
+            out[f, :, p * cols:(p + 1) * cols] = I
+            vmax = max(vmax, F32(I.max()))
+    if fill_factor:
+        period = F32(2.0 * float(ps))
+        kfx = F32(2 * (2.0 * math.pi / float(period)) / W)
+        kfy = F32(2 * (2.0 * math.pi / float(period)) / H)
+        kx = (kfx * np.array([i if i <= W // 2 else i - W for i in range(W // 2 + 1)], dtype=F32)).astype(F32)
+        ky = (kfy * np.array([i if i <= H // 2 else i - H for i in range(H)], dtype=F32)).astype(F32)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            ax = (kx * F32(0.5) * ps).astype(F32)
+            ay = (ky * F32(0.5) * ps).astype(F32)
+            sx = np.where(kx != 0, np.sin(ax) / ax, 1).astype(F32)
+            sy = np.where(ky != 0, np.sin(ay) / ay, 1).astype(F32)
+        env = ((sy * F32(1.0 / (W * H))).astype(F32)[:, None] * sx[None, :]).astype(F32)
+        for f in range(frame_count):
+            X = np.fft.rfft2(out[f].astype(np.float64)) * env
+            out[f] = np.fft.irfft2(X, s=(H, W)) * (W * H)
+    inv = F32(F32(levels - 1) / vmax)
+    q = np.rint((out * inv).astype(F32)).astype(F32)
+    q16 = np.clip(q, 0, 65535).astype(np.uint16)
+    params = dict(W=W, H=H, P=P, G=G, M=M, tilt_x=tx, tilt_y=ty, beam_waist=bw, beam_centre_x=bcx,
+                  ref_centre_x=rcx, coefs=coefs, levels=levels, pixel_size=ps)
+    return q, q16, params

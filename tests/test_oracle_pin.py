@@ -272,3 +272,53 @@ def test_snap_estimate_matches_live_reference():
             assert abs(L.digHoloConfigGetBeamCentre(h, ax, p) - float(c.beam_centre[p][ax])) <= 1e-9
     assert abs(L.digHoloConfigGetBasisWaist(h, 0) - float(c.waist[0])) <= 1e-4 * float(c.waist[0])
     assert abs(L.digHoloConfigGetDefocus(h, 0) - float(c.defocus[0])) <= 1e-3
+
+
+def _ref_simulate(L, frames, W, H, P, G, levels, fill, coefs=None, waist=None, tiltx=None):
+    """The reference build's digHoloFrameSimulatorCreate (digHolo.cpp:16755)."""
+    import ctypes as C
+    Wc, Hc, psc, Pc, Gc, lv, wc = C.c_int(W), C.c_int(H), C.c_float(20e-6), C.c_int(P), C.c_int(G), C.c_int(levels), C.c_int(0)
+    nul = lambda: C.POINTER(C.c_float)()
+    keep = []
+
+    def arr(v):
+        if v is None:
+            return C.pointer(nul())
+        a = np.ascontiguousarray(np.asarray(v, dtype=np.complex64).view(np.float32) if np.iscomplexobj(v)
+                                 else np.asarray(v, dtype=np.float32))
+        keep.append(a)
+        return C.pointer(a.ctypes.data_as(C.POINTER(C.c_float)))
+    p16 = C.POINTER(C.c_ushort)()
+    out = L.digHoloFrameSimulatorCreate(frames, C.byref(Wc), C.byref(Hc), C.byref(psc), C.byref(Pc), arr(tiltx),
+                                        arr(None), arr(None), arr(None), arr(None), arr(None), arr(None), C.byref(Gc),
+                                        arr(waist), arr(coefs), arr(None), arr(None), C.byref(lv), fill, arr(None),
+                                        C.byref(wc), 0, 0, C.byref(p16), None)
+    n = frames * Hc.value * Wc.value
+    f32 = np.ctypeslib.as_array(out, shape=(n,)).copy().reshape(frames, Hc.value, Wc.value)
+    L.digHoloFrameSimulatorDestroy(out)
+    return f32, Gc.value
+
+
+@pytest.mark.parametrize("case", [(6, 128, 64, 2, 3, 16384, 0, False), (10, 160, 96, 2, 0, 16384, 1, False),
+                                  (5, 192, 128, 2, 5, 4096, 1, True), (4, 128, 128, 1, 6, 4096, 0, True)])
+def test_frame_simulator_matches_live_reference(case):
+    """The frame simulator restatement against the reference build: the
+    same group count, and frames equal except at no more than 1e-4 of the
+    pixels, by one camera level (float rounding of the reference's scalar
+    tables)."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    fr, W, H, P, G, levels, fill, dense = case
+    coefs = waist = tiltx = None
+    if dense:
+        rng = np.random.default_rng(3 + fr)
+        M = G * (G + 1) // 2
+        coefs = (rng.standard_normal((fr, P, M)) + 1j * rng.standard_normal((fr, P, M))).astype(np.complex64)
+        coefs[:, :, 3] = 0
+        waist, tiltx = [300e-6, 250e-6][:P], [1.5, -1.2][:P]
+    r32, Gr = _ref_simulate(ref_lib.load(), fr, W, H, P, G, levels, fill, coefs, waist, tiltx)
+    o32, o16, prm = O.frame_simulator(fr, W, H, 20e-6, P, group_count=G, levels=levels, fill_factor=fill,
+                                      beam_coefs=coefs, beam_waist=waist, ref_tilt_x=tiltx)
+    assert prm["G"] == Gr
+    d = np.abs(r32 - o32)
+    assert d.max() <= 1 and float((d > 0).mean()) <= 1e-4
