@@ -44,6 +44,7 @@ extern "C" {
 int digHoloCreate() {
     Object* o = new Object();
     o->cfg.threadCount = (int)std::thread::hardware_concurrency();
+    o->cfgBackup = o->cfg;
     std::lock_guard<std::mutex> g(gTableLock);
     gObjects.push_back(o);
     return (int)gObjects.size() - 1;

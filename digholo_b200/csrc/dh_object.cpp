@@ -147,9 +147,12 @@ void fftWindowGeometry(const Config& c, int P, Geometry& g) {
 
 // digHolo.cpp:7868-8048 (single wavelength) and 8183-8203
 void ifftWindowGeometry(const Config& c, int P, Geometry& g) {
-    const float lam = c.wavelengthCentre;
-    const float k0Max = 2 * PI_F / lam;
-    const float k0Min = k0Max;
+    // k0Max from the longest wavelength, k0Min from the shortest, as the
+    // reference names them (digHolo.cpp:7913-7914)
+    const float lamStart = c.lambdaRange[0] > 0 ? c.lambdaRange[0] : c.wavelengthCentre;
+    const float lamStop = c.lambdaRange[1] > 0 ? c.lambdaRange[1] : c.wavelengthCentre;
+    const float k0Max = 2 * PI_F / (fmaxf(lamStart, lamStop));
+    const float k0Min = 2 * PI_F / (fminf(lamStart, lamStop));
     const float dkx = g.kx[1] - g.kx[0];
     const float dky = g.ky[1] - g.ky[0];
     const float r0 = c.apertureSize * UNIT_ANGLE;
@@ -1219,9 +1222,170 @@ static int processBatchLocked(Object& o, int syncCoefs);
 // device batch.  This is the documented intent of the reference's transposing
 // converter (convert_int16tofloat32, digHolo.cpp:1206-1229), whose lane
 // permutation scrambles every other output row.
+// digHoloWavelengthUpdate (digHolo.cpp:7823-7862): a pending array replaces
+// the one in use; with none, the centre wavelength alone; an array of one
+// wavelength is replaced by the centre wavelength.
+void objWavelengthUpdate(Object& o) {
+    if (!o.wavelengthsValid && !o.wavelengthsNew.empty()) {
+        o.wavelengths = o.wavelengthsNew;
+        o.wavelengthsValid = 1;
+    } else if (o.wavelengths.empty()) {
+        o.wavelengths.assign(1, o.cfg.wavelengthCentre);
+        o.wavelengthsValid = 1;
+    }
+    if (o.wavelengths.size() == 1) o.wavelengths[0] = o.cfg.wavelengthCentre;
+}
+
+// A batch of frames at L > 1 wavelengths (digHoloProcessBatchFrequencySweep*,
+// digHolo.cpp:5046-5080; digHoloIFFTRoutine's per-frame wavenumber,
+// digHolo.cpp:8641-8700; one reference wave per wavelength,
+// digHolo.cpp:10386-10504).  Frame i belongs to wavelength i mod L
+// (wavelength the fast axis of the input) or i / (B / L) (slow axis), and
+// output o of that frame is sub L + lambda (fast) or lambda (B / L) + sub
+// (slow) (WavelengthOrderingCalc, digHolo.cpp:2656-2700).  The frames of
+// each wavelength go through the batch path as one sub-batch: the IFFT
+// window spans the first and last wavelength (digHolo.cpp:7868-8048), the
+// Fourier-window mask, its centre and the reference wave follow the
+// sub-batch's wavelength; the outputs are scattered to their positions.
+// The batch count must be a multiple of L; frame averaging is not combined
+// with it here.
+static int processSweepLocked(Object& o, int syncCoefs) {
+    int r = objInitDevice(o);
+    if (r) return r;
+    const std::vector<float> lams = o.wavelengths;
+    const int L = (int)lams.size();
+    const Config saved = o.cfg;
+    const int B = std::max(1, saved.batchCount);
+    if (!o.frames) return fail(o, ERR_NULLPOINTER, "frame buffer not set");
+    if (saved.avgCount > 1)
+        return fail(o, ERR_INVALIDARGUMENT, "multi-wavelength batches: frame averaging is not supported with them");
+    if (B % L)
+        return fail(o, ERR_INVALIDDIMENSION, "multi-wavelength batches: the batch count must be a multiple of the wavelength count");
+    const int S = B / L;
+    const bool inFast = saved.wavelengthOrdering[0] == 0, outFast = saved.wavelengthOrdering[1] == 0;
+    const size_t es = o.framesU16 ? 2 : 4;
+    const size_t frameBytes = (size_t)saved.frameWidth * saved.frameHeight * es;
+    const void* framesIn = o.frames;
+    const int onDevice = isDevicePointer(framesIn);
+    const std::vector<float> calSaved = o.batchCal;
+    const int calEnabled = o.batchCalEnabled, calCount = o.batchCalCount, calPol = o.batchCalPolCount;
+    struct Restore {
+        Object& o; Config c; const void* f; int d, t; std::vector<float> cal; int calCount;
+        ~Restore() {
+            o.cfg = c; o.frames = f; o.framesOnDevice = d; o.framesTransposed = t;
+            o.batchCal = cal; o.batchCalCount = calCount; o.batchCalVersion++;
+        }
+    } restore{o, saved, o.frames, o.framesOnDevice, o.framesTransposed, calSaved, calCount};
+    DH_CUDA(o, o.dSweepFrames.ensure((size_t)S * frameBytes));
+    int P = 0, M = 0, Mout = 0, nx = 0, ny = 0, keep32 = o.keepField32, active = 0;
+    for (int l = 0; l < L; l++) {
+        const char* src = static_cast<const char*>(framesIn) + (size_t)(inFast ? l : l * S) * frameBytes;
+        DH_CUDA(o, cudaMemcpy2DAsync(o.dSweepFrames.ptr, frameBytes, src, inFast ? (size_t)L * frameBytes : frameBytes,
+                                     frameBytes, S, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                     o.stream));
+        if (calEnabled && calCount > 0) {
+            // the batch calibration of each frame's input index
+            std::vector<float> c((size_t)calPol * S * 2);
+            for (int p = 0; p < calPol; p++)
+                for (int j = 0; j < S; j++) {
+                    const int in = inFast ? l + L * j : l * S + j;
+                    const size_t srcIdx = ((size_t)p * calCount + (in % calCount)) * 2;
+                    c[((size_t)p * S + j) * 2] = calSaved[srcIdx];
+                    c[((size_t)p * S + j) * 2 + 1] = calSaved[srcIdx + 1];
+                }
+            o.batchCal = c;
+            o.batchCalCount = S;
+            o.batchCalVersion++;
+        }
+        o.frames = o.dSweepFrames.ptr;
+        o.framesOnDevice = 1;
+        o.framesTransposed = 0;
+        o.cfg = saved;
+        o.cfg.batchCount = S;
+        o.cfg.wavelengthCentre = lams[l];
+        o.cfg.lambdaRange[0] = lams[0];
+        o.cfg.lambdaRange[1] = lams[L - 1];
+        r = processBatchLocked(o, 0);
+        if (r) return r;
+        P = o.polCount; M = o.modeCount; nx = o.geo.nx; ny = o.geo.ny;
+        active = o.basisActive; Mout = o.modeCountOut;
+        if (l == 0) {
+            DH_CUDA(o, o.dAccCoefs.ensure((size_t)B * P * std::max(1, M) * sizeof(float2)));
+            DH_CUDA(o, o.dAccCoefsOut.ensure((size_t)B * P * std::max(1, Mout) * sizeof(float2)));
+            DH_CUDA(o, o.dAccFieldR.ensure((size_t)B * P * nx * ny * sizeof(short)));
+            DH_CUDA(o, o.dAccFieldI.ensure((size_t)B * P * nx * ny * sizeof(short)));
+            if (keep32) DH_CUDA(o, o.dAccField32.ensure((size_t)B * P * nx * ny * sizeof(float2)));
+            DH_CUDA(o, o.dAccStats.ensure((size_t)ANALYSIS_COUNT * P * (B + 1) * sizeof(float)));
+        }
+        // rows of this sub-batch to their output positions
+        auto scatter = [&](void* dst, const void* srcRows, size_t rowBytes) -> cudaError_t {
+            char* d = static_cast<char*>(dst) + (size_t)(outFast ? l : l * S) * rowBytes;
+            return cudaMemcpy2DAsync(d, outFast ? (size_t)L * rowBytes : rowBytes, srcRows, rowBytes, rowBytes, S,
+                                     cudaMemcpyDeviceToDevice, o.stream);
+        };
+        if (M > 0) DH_CUDA(o, scatter(o.dAccCoefs.ptr, o.dCoefs.ptr, (size_t)P * M * sizeof(float2)));
+        if (active && Mout > 0) DH_CUDA(o, scatter(o.dAccCoefsOut.ptr, o.dCoefsOut.ptr, (size_t)P * Mout * sizeof(float2)));
+        DH_CUDA(o, scatter(o.dAccFieldR.ptr, o.dFieldR.ptr, (size_t)P * nx * ny * sizeof(short)));
+        DH_CUDA(o, scatter(o.dAccFieldI.ptr, o.dFieldI.ptr, (size_t)P * nx * ny * sizeof(short)));
+        if (keep32) DH_CUDA(o, scatter(o.dAccField32.ptr, o.dField32.ptr, (size_t)P * nx * ny * sizeof(float2)));
+        // statistics [param][pol][S + 1] -> [param][pol][B + 1]
+        const int rowsStat = ANALYSIS_COUNT * P;
+        float* accS = o.dAccStats.as<float>();
+        const float* subS = o.dStats.as<float>();
+        if (!outFast) {
+            DH_CUDA(o, cudaMemcpy2DAsync(accS + (size_t)l * S, (size_t)(B + 1) * 4, subS, (size_t)(S + 1) * 4, (size_t)S * 4,
+                                         rowsStat, cudaMemcpyDeviceToDevice, o.stream));
+        } else {
+            for (int q = 0; q < rowsStat; q++)
+                DH_CUDA(o, cudaMemcpy2DAsync(accS + (size_t)q * (B + 1) + l, (size_t)L * 4, subS + (size_t)q * (S + 1), 4, 4, S,
+                                             cudaMemcpyDeviceToDevice, o.stream));
+        }
+    }
+    // the whole batch's outputs in the handle's buffers
+    o.batchCount = B;
+    const size_t nf = (size_t)B * P * nx * ny;
+    if (M > 0) {
+        DH_CUDA(o, o.dCoefs.ensure((size_t)B * P * M * sizeof(float2)));
+        DH_CUDA(o, cudaMemcpyAsync(o.dCoefs.ptr, o.dAccCoefs.ptr, (size_t)B * P * M * sizeof(float2), cudaMemcpyDeviceToDevice, o.stream));
+    }
+    if (active && Mout > 0) {
+        DH_CUDA(o, o.dCoefsOut.ensure((size_t)B * P * Mout * sizeof(float2)));
+        DH_CUDA(o, cudaMemcpyAsync(o.dCoefsOut.ptr, o.dAccCoefsOut.ptr, (size_t)B * P * Mout * sizeof(float2), cudaMemcpyDeviceToDevice, o.stream));
+    }
+    DH_CUDA(o, o.dFieldR.ensure(nf * sizeof(short)));
+    DH_CUDA(o, o.dFieldI.ensure(nf * sizeof(short)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dFieldR.ptr, o.dAccFieldR.ptr, nf * sizeof(short), cudaMemcpyDeviceToDevice, o.stream));
+    DH_CUDA(o, cudaMemcpyAsync(o.dFieldI.ptr, o.dAccFieldI.ptr, nf * sizeof(short), cudaMemcpyDeviceToDevice, o.stream));
+    if (keep32) {
+        DH_CUDA(o, o.dField32.ensure(nf * sizeof(float2)));
+        DH_CUDA(o, cudaMemcpyAsync(o.dField32.ptr, o.dAccField32.ptr, nf * sizeof(float2), cudaMemcpyDeviceToDevice, o.stream));
+    }
+    DH_CUDA(o, o.dStats.ensure((size_t)ANALYSIS_COUNT * P * (B + 1) * sizeof(float)));
+    DH_CUDA(o, cudaMemcpyAsync(o.dStats.ptr, o.dAccStats.ptr, (size_t)ANALYSIS_COUNT * P * (B + 1) * sizeof(float),
+                               cudaMemcpyDeviceToDevice, o.stream));
+    // the tables of the last sub-batch's wavelength are not the configuration's
+    o.preparedValid = 0;
+    o.lastFwdValid = 0;
+    o.fourierValid = 0;
+    o.metricsValid = 0;
+    if (syncCoefs) return objCoefsToHost(o);
+    return ERR_SUCCESS;
+}
+
+static int processAnyLocked(Object& o, int syncCoefs) {
+    // the reference applies an enabled calibration of the frames' size
+    // (digHolo.cpp:8233-8240); applying it is not built here
+    if (o.refCalEnabled && o.refCalWidth == o.cfg.frameWidth && o.refCalHeight == o.cfg.frameHeight)
+        return fail(o, ERR_ERROR, "reference-wave calibration is set and enabled: applying it is not supported by this library");
+    objWavelengthUpdate(o);
+    if (o.wavelengths.size() > 1) return processSweepLocked(o, syncCoefs);
+    o.cfg.lambdaRange[0] = o.cfg.lambdaRange[1] = 0.f;
+    return processBatchLocked(o, syncCoefs);
+}
+
 int objProcessBatch(Object& o, int syncCoefs) {
     std::lock_guard<std::mutex> guard(o.lock);
-    if (!(o.framesTransposed && o.framesU16)) return processBatchLocked(o, syncCoefs);
+    if (!(o.framesTransposed && o.framesU16)) return processAnyLocked(o, syncCoefs);
     int r = objInitDevice(o);
     if (r) return r;
     if (!o.frames) return fail(o, ERR_NULLPOINTER, "frame buffer not set");
@@ -1245,7 +1409,7 @@ int objProcessBatch(Object& o, int syncCoefs) {
     o.frames = o.dTransFrames.ptr;
     o.framesOnDevice = 1;
     o.framesTransposed = 0;
-    return processBatchLocked(o, syncCoefs);
+    return processAnyLocked(o, syncCoefs);
 }
 
 // ------------------------------------------------------------------ kernel planner

@@ -44,6 +44,9 @@ struct Config {
     int avgCount = 1;
     int avgMode = 0;
     float wavelengthCentre = 1565e-9f;
+    // first and last wavelength of a multi-wavelength batch (0: the centre
+    // wavelength alone): the IFFT window spans the Fourier windows of both
+    float lambdaRange[2] = {0.f, 0.f};
     int wavelengthOrdering[2] = {0, 0};
     int polLockTilt = 0;
     int polLockBasisWaist = 1;
@@ -210,6 +213,22 @@ struct Object {
     HostBuf hUpload;                    // pinned staging of the per-configuration tables
     cudaEvent_t evUpload = nullptr;     // the last staged upload has left
     std::vector<float> hX, hY;
+    // wavelengths (digHoloConfigSetWavelengths*, digHolo.cpp:6578-6690):
+    // the pending array and the one in use after the next update
+    std::vector<float> wavelengthsNew, wavelengths;
+    int wavelengthsValid = 0;
+    DevBuf dSweepFrames, dAccCoefs, dAccCoefsOut, dAccFieldR, dAccFieldI, dAccField32, dAccStats;
+    // reference-wave calibration (digHoloConfigSetRefCalibration*,
+    // digHolo.cpp:5309-5540): the stored per-pixel factors [L][height][width]
+    std::vector<float> refCal;
+    int refCalWidth = 0, refCalHeight = 0, refCalCount = 0, refCalEnabled = 0;
+    // frames loaded by digHoloSetFrameBufferFromFile (owned, float32)
+    std::vector<float> ownFrames;
+    // digHoloConfigBackupSave / Load
+    Config cfgBackup;
+    int cfgBackupValid = 0;
+    float* zernRows[POLMAX] = {nullptr, nullptr};   // digHoloConfigGetZernCoefs
+    HostBuf hBasisFields;                           // digHoloBasisGetFields
     float autoAlignMetrics[METRIC_COUNT][2] = {};
     int metricsValid = 0;
     std::string lastError;
@@ -269,6 +288,8 @@ int objMdlWeights(Object& o, float2* W, double* mdlDb);
 float objAutoAlignAdjoint(Object& o);
 int objCalcMetrics(Object& o);
 float objAutoAlign(Object& o);
+// The wavelength array in use (digHoloWavelengthUpdate, digHolo.cpp:7823-7862).
+void objWavelengthUpdate(Object& o);
 
 // Geometry helpers (host, float32 emulation of the reference).
 void fftWindowGeometry(const Config& c, int polCount, Geometry& g);

@@ -68,6 +68,36 @@ __global__ void __launch_bounds__(SIM_T) k_sim_field(DhSimFieldArgs a) {
     if ((threadIdx.x & 31) == 0) atomicMax(a.maxBits, __float_as_uint(vmax));
 }
 
+// Basis fields (GetFieldsBasis, digHolo.cpp:5233-5305, through
+// generateModeSeparable without the transpose or a reference wave): field
+// [mode][pol][rows][cols] = sum over the mode's terms of (float)(int16 x
+// mode x int16 y mode) c in the same order and rounding as k_sim_field.
+__global__ void __launch_bounds__(SIM_T) k_basis_fields(DhSimFieldArgs a, float2* out) {
+    extern __shared__ float4 bfSm[];
+    DhSimMode* modes = reinterpret_cast<DhSimMode*>(bfSm);
+    const int rowBlocks = (a.rows + SIM_RB - 1) / SIM_RB;
+    const int unit = blockIdx.x / rowBlocks, r0 = (blockIdx.x % rowBlocks) * SIM_RB;
+    const int pol = unit % a.polCount;
+    const int beg = a.modeOffset[unit], cnt = a.modeOffset[unit + 1] - beg;
+    for (int e = threadIdx.x; e < cnt; e += SIM_T) modes[e] = a.modes[beg + e];
+    __syncthreads();
+    const short* hc = a.hgCol + (size_t)pol * a.G * a.cols;
+    const short* hr = a.hgRow + (size_t)pol * a.G * a.rows;
+    const int rows = min(SIM_RB, a.rows - r0);
+    for (int e = threadIdx.x; e < rows * a.cols; e += SIM_T) {
+        const int r = r0 + e / a.cols, c = e % a.cols;
+        float2 f = make_float2(0.f, 0.f);
+        for (int k = 0; k < cnt; k++) {
+            const DhSimMode md = modes[k];
+            const int prod = (int)__ldg(&hc[(size_t)md.m * a.cols + c]) * (int)__ldg(&hr[(size_t)md.n * a.rows + r]);
+            const float v = __int2float_rn(prod);
+            const float2 t = make_float2(__fmul_rn(v, md.cr), __fmul_rn(v, md.ci));
+            f = k == 0 ? t : make_float2(__fadd_rn(t.x, f.x), __fadd_rn(t.y, f.y));
+        }
+        out[((size_t)unit * a.rows + r) * a.cols + c] = f;
+    }
+}
+
 // X[ky][kx] *= (sincY[ky] norm) sincX[kx] on [frame][H][W/2+1].
 __global__ void k_sim_sinc(float2* X, int frames, int H, int Nx, const float* sincX, const float* sincY, float norm) {
     const size_t total = (size_t)frames * H * Nx;
@@ -124,6 +154,18 @@ cudaError_t dh_launch_sim_field(const DhSimFieldArgs& a, int maxModesPerUnit, cu
     if (e != cudaSuccess) return e;
     const int rowBlocks = (a.rows + SIM_RB - 1) / SIM_RB;
     k_sim_field<<<(unsigned)(units * rowBlocks), SIM_T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t dh_launch_basis_fields(const DhSimFieldArgs& a, int maxModesPerUnit, float2* out, cudaStream_t s) {
+    const int units = a.frames * a.polCount;
+    if (units <= 0) return cudaSuccess;
+    const size_t smem = sizeof(DhSimMode) * (size_t)(maxModesPerUnit > 0 ? maxModesPerUnit : 1);
+    if (smem > 200 * 1024) return cudaErrorNotSupported;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_basis_fields), (int)smem);
+    if (e != cudaSuccess) return e;
+    const int rowBlocks = (a.rows + SIM_RB - 1) / SIM_RB;
+    k_basis_fields<<<(unsigned)(units * rowBlocks), SIM_T, smem, s>>>(a, out);
     return cudaGetLastError();
 }
 

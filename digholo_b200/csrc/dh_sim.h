@@ -24,6 +24,8 @@ struct DhSimFieldArgs {
 };
 
 cudaError_t dh_launch_sim_field(const DhSimFieldArgs& a, int maxModesPerUnit, cudaStream_t s);
+// Basis fields: frames = output modes, out [mode][pol][rows][cols] complex.
+cudaError_t dh_launch_basis_fields(const DhSimFieldArgs& a, int maxModesPerUnit, float2* out, cudaStream_t s);
 cudaError_t dh_launch_sim_sinc(float2* X, int frames, int H, int Nx, const float* sincX, const float* sincY, float norm,
                                cudaStream_t s);
 cudaError_t dh_launch_sim_extend(const float2* half, float2* full, int frames, int H, int W, cudaStream_t s);

@@ -316,6 +316,70 @@ int digHoloFFTWWisdomFilename(const char* filename);
 int digHoloConfigSetVerbosity(int handleIdx, int verbosity);
 /* replaces digHolo.h:1937 */
 int digHoloConfigGetVerbosity(int handleIdx);
+/* replace digHolo.h:832, 843, 854, 886, 895: the wavelengths of the frames
+ * of a batch (taking effect at the next processing), as an array or equally
+ * spaced in frequency; an array of one wavelength means the centre
+ * wavelength; the ordering of frames (inoutIdx 0) and outputs (1): 0
+ * wavelength the fast axis, 1 the slow axis */
+int digHoloConfigSetWavelengths(int handleIdx, float* wavelengths, int wavelengthCount);
+int digHoloConfigSetWavelengthsLinearFrequency(int handleIdx, float wavelengthStart, float wavelengthStop,
+                                               int wavelengthCount);
+float* digHoloConfigGetWavelengths(int handleIdx, int* wavelengthCount);
+int digHoloConfigSetWavelengthOrdering(int handleIdx, int inoutIdx, int ordering);
+int digHoloConfigGetWavelengthOrdering(int handleIdx, int inoutIdx);
+/* replace digHolo.h:1510 and 1525: ProcessBatch of frames at several
+ * wavelengths; each wavelength's frames run as one sub-batch with its own
+ * Fourier-window mask and reference wave in the common IFFT window; the
+ * batch count must be a multiple of the wavelength count, without frame
+ * averaging */
+complex64* digHoloProcessBatchFrequencySweepLinear(int handleIdx, int* batchCount, int* modeCount, int* polCount,
+                                                   float lambdaStart, float lambdaStop, int lambdaCount);
+complex64* digHoloProcessBatchWavelengthSweepArbitrary(int handleIdx, int* batchCount, int* modeCount, int* polCount,
+                                                       float* wavelengths, int lambdaCount);
+/* replace digHolo.h:369, 384, 400, 409, 417, 437: the reference-wave
+ * calibration is stored (as the reference normalises and inverts it) and can
+ * be enabled and disabled, but applying it to the fields is not built: a
+ * batch whose frames have the calibration's size fails while it is enabled,
+ * and GetRefCalibrationFields returns NULL */
+int digHoloConfigSetRefCalibrationIntensity(int handleIdx, unsigned short* cal, int wavelengthCount, int width,
+                                            int height);
+int digHoloConfigSetRefCalibrationField(int handleIdx, complex64* cal, int wavelengthCount, int width, int height);
+int digHoloConfigSetRefCalibrationFromFile(int handleIdx, const char* fname, int wavelengthCount, int width,
+                                           int height);
+int digHoloConfigSetRefCalibrationEnabled(int handleIdx, int enabled);
+int digHoloConfigGetRefCalibrationEnabled(int handleIdx);
+complex64* digHoloConfigGetRefCalibrationFields(int handleIdx, int* wavelengthCount, int* polCount, float** x,
+                                                float** y, int* width, int* height);
+/* replaces digHolo.h:288: uint16 frames from a binary file, held by the
+ * handle (as float32) as its frame buffer */
+int digHoloSetFrameBufferFromFile(int handleIdx, const char* fname);
+/* replaces digHolo.h:624: polCount x batchCount complex64 from a file */
+int digHoloConfigSetBatchCalibrationFromFile(int handleIdx, const char* fname, int polCount, int batchCount);
+/* replaces digHolo.h:1587: the basis fields of the last batch's basis,
+ * modeCount x polCount x height x width complex64 (computed on the GPU) */
+complex64* digHoloBasisGetFields(int handleIdx, int* modeCount, int* polCount, float** x, float** y, int* width,
+                                 int* height);
+/* replaces digHolo.h:1766: the configured thread count (the GPU path has
+ * no CPU thread pool to tune) */
+int digHoloBenchmarkEstimateThreadCountOptimal(int handleIdx, float goalDuration);
+/* replace digHolo.h:1883 and 1897: the viewport bitmap renderer is not part
+ * of this library; no bitmap, zero width and height, DIGHOLO_ERROR_ERROR */
+unsigned char* digHoloGetViewport(int handleIdx, int displayMode, int forceProcessing, int* width, int* height,
+                                  char** windowString);
+int digHoloGetViewportToFile(int handleIdx, int displayMode, int forceProcessing, int* width, int* height,
+                             char** windowString, const char* filename);
+/* replace digHolo.h:1945 and 1952 */
+int digHoloConsoleRedirectToFile(char* filename);
+int digHoloConsoleRestore();
+/* replace digHolo.h:1973 and 1983 */
+int digHoloConfigBackupSave(int handleIdx);
+int digHoloConfigBackupLoad(int handleIdx);
+/* replaces digHolo.h:1990 (not for general use; does nothing here) */
+void digHoloDebugRoutine(int handleIdx);
+/* replace digHolo.h:2075 and 2084: rows of six Zernike coefficients per
+ * polarisation (tilt x, tilt y at 1, 2; defocus at 4) */
+float** digHoloConfigGetZernCoefs(int handleIdx);
+int digHoloConfigGetZernCount(int handleIdx);
 /* replaces digHolo.h:2026: synthetic camera frames, computed on the GPU,
  * returned in one host allocation ([float32 frames][uint16 frames]
  * [parameters]) released by digHoloFrameSimulatorDestroy; null arrays take

@@ -85,6 +85,26 @@ SEQUENCE = [
     ("digHoloConfigSetAutoAlignMode", (5,)),
     ("digHoloConfigSetAutoAlignGoalIdx", (1,)),
     ("digHoloConfigGetAutoAlignGoalIdx", ()),
+    ("digHoloConfigSetWavelengthsLinearFrequency", (1500e-9, 1600e-9, 0)),
+    ("digHoloConfigSetWavelengthsLinearFrequency", (1500e-9, 1600e-9, -3)),
+    ("digHoloConfigSetWavelengthsLinearFrequency", (1500e-9, 1600e-9, 5)),
+    ("digHoloConfigSetWavelengthOrdering", (0, 1)),
+    ("digHoloConfigSetWavelengthOrdering", (2, 1)),
+    ("digHoloConfigSetWavelengthOrdering", (1, 3)),
+    ("digHoloConfigGetWavelengthOrdering", (0,)),
+    ("digHoloConfigGetWavelengthOrdering", (1,)),
+    ("digHoloConfigGetWavelengthOrdering", (7,)),
+    ("digHoloConfigBackupSave", ()),
+    ("digHoloConfigBackupLoad", ()),
+    ("digHoloConfigGetZernCount", ()),
+    ("digHoloConfigSetRefCalibrationIntensity", (None, 1, 16, 16)),
+    ("digHoloConfigGetRefCalibrationEnabled", ()),
+    ("digHoloConfigSetRefCalibrationEnabled", (1,)),
+    ("digHoloConfigGetRefCalibrationEnabled", ()),
+    ("digHoloConfigSetRefCalibrationFromFile", (b"no_such_calibration.bin", 1, 16, 16)),
+    ("digHoloConfigGetRefCalibrationEnabled", ()),
+    ("digHoloConfigSetBatchCalibrationFromFile", (b"no_such_calibration.bin", 1, 4)),
+    ("digHoloSetFrameBufferFromFile", (b"no_such_frames.bin",)),
 ]
 
 
@@ -104,6 +124,23 @@ def test_config_semantics_match_reference(lib):
     ref = _run_sequence(ref_lib.load())
     diffs = [(SEQUENCE[i][0], SEQUENCE[i][1], a, b) for i, (a, b) in enumerate(zip(ours, ref)) if a != b]
     assert not diffs, diffs
+
+
+def test_wavelengths_before_processing(lib):
+    """Before any processing there is no wavelength array in use: NULL and a
+    zero count, as in the reference (digHolo.cpp:5056-5068); the setters'
+    return codes are compared in the sequence above."""
+    out = []
+    libs = [lib] + ([ref_lib.load()] if ref_lib.available() else [])
+    for L in libs:
+        h = L.digHoloCreate()
+        assert L.digHoloConfigSetWavelengthsLinearFrequency(h, 1500e-9, 1600e-9, 7) == 0
+        n = C.c_int(5)
+        p = L.digHoloConfigGetWavelengths(h, C.byref(n))
+        out.append((bool(p), n.value))
+        if L is lib:
+            L.digHoloDestroy(h)   # the reference's Destroy faults after this sequence; its handle is left
+    assert all(v == (False, 0) for v in out)
 
 
 def test_invalid_handle_returns(lib):
