@@ -37,6 +37,13 @@ Object* get(int h) {
 
 dh::Object* dhObjectForHandle(int h) { return get(h); }
 
+// Handles created so far (destroyed ones included), for the settings-file
+// runner, which uses handle 0 when one exists (digHolo.cpp:16774-16782).
+extern "C" int dhHandleCount() {
+    std::lock_guard<std::mutex> g(gTableLock);
+    return (int)gObjects.size();
+}
+
 extern "C" {
 
 // ------------------------------------------------------------ handles

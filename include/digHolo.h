@@ -350,6 +350,11 @@ int digHoloConfigSetRefCalibrationEnabled(int handleIdx, int enabled);
 int digHoloConfigGetRefCalibrationEnabled(int handleIdx);
 complex64* digHoloConfigGetRefCalibrationFields(int handleIdx, int* wavelengthCount, int* polCount, float** x,
                                                 float** y, int* width, int* height);
+/* replaces digHolo.h:1962: one batch described by a settings file (tab-
+ * separated names and values, the reference's names), its outputs written
+ * to the files the settings name; digholo_b200/digholo_run runs it for each
+ * file named on its command line */
+int digHoloRunBatchFromConfigFile(char* filename);
 /* replaces digHolo.h:288: uint16 frames from a binary file, held by the
  * handle (as float32) as its frame buffer */
 int digHoloSetFrameBufferFromFile(int handleIdx, const char* fname);
