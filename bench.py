@@ -549,8 +549,8 @@ def largefield_leg(L, torch, device, stream, no_cpu, frames=256):
     batches = [torch_frames(cfg, B, 5000 + i, device) for i in range(2)]
     torch.cuda.synchronize()
     out = {"metric": "frames/s (FFT->window->IFFT->tilt->HG overlap), device-resident frames",
-           "workload": "largefield_2048_u16_2pol_mode0: 256 frames 2048x2048 uint16, 2 pol, window 512x512, "
-                       "maxMG 30 (465 modes)", "steps": steps, "warmup": warmup}
+           "workload": "largefield_2048_u16_2pol_mode0: %d frames 2048x2048 uint16, 2 pol, window 512x512, "
+                       "maxMG 30 (465 modes)" % B, "steps": steps, "warmup": warmup}
     for name, ov in (("split_bf16", 0), ("fp32", 1)):
         h = L.digHoloCreate()
         api.configure(L, h, cfg)
@@ -588,8 +588,8 @@ def largefield_leg(L, torch, device, stream, no_cpu, frames=256):
             threads = os.cpu_count() or 1
             fps, calls, el = reference_run(cfg, sample, 8.0, threads)
             out["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "reference",
-                                   "sample": "4 of the 256 frames, digHoloProcessBatch repeated for %.1f s (%d calls)"
-                                             % (el, calls)}
+                                   "sample": "4 of the %d frames, digHoloProcessBatch repeated for %.1f s (%d calls)"
+                                             % (B, el, calls)}
         except Exception as exc:
             out["cpu_baseline"] = {"value": None, "sample": "unavailable: %s" % exc}
     del batches
