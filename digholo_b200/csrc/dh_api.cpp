@@ -77,6 +77,9 @@ int digHoloDestroy(int h) {
             for (auto e : o->evCopy) if (e) cudaEventDestroy(e);
             if (o->copyStream2) cudaStreamDestroy(o->copyStream2);
             for (auto e : o->evCopy2) if (e) cudaEventDestroy(e);
+            if (o->d2hStream) cudaStreamDestroy(o->d2hStream);
+            for (auto e : o->evChunk) if (e) cudaEventDestroy(e);
+            if (o->evD2H) cudaEventDestroy(o->evD2H);
             if (o->evStart) cudaEventDestroy(o->evStart);
             if (o->evStop) cudaEventDestroy(o->evStop);
             if (o->hStatus) cudaFreeHost(o->hStatus);

@@ -382,11 +382,8 @@ extern "C" complex64* digHoloProcessBatchWavelengthSweepArbitrary(int h, int* ba
 // digHolo.h:369-437 / digHolo.cpp:5309-5540.  The factors are stored as the
 // reference forms them: from an intensity, sqrt(1 / (I / max I)); from a
 // field, the componentwise (1 / (re / max|E|), -1 / (im / max|E|)); NaN or
-// infinite factors become 0.  Applying them to the reconstructed fields
-// (through an FFT of the calibration frames, the Fourier window at zero
-// tilt and an IFFT, digHolo.cpp:6729-6830, 8253-8285) is not built: a batch
-// with an enabled calibration of the frame's size fails with an error
-// instead of returning uncalibrated fields.
+// infinite factors become 0.  Their reconstructed planes multiply the IFFT
+// output of each frame of the calibration's size (dh_refcal.cpp).
 namespace {
 int refCalStore(Object& o, const unsigned short* i16, const float* c64, int count, int w, int h) {
     if (!i16 && !c64) { o.refCalEnabled = 0; return dh::ERR_NULLPOINTER; }
@@ -423,6 +420,9 @@ int refCalStore(Object& o, const unsigned short* i16, const float* c64, int coun
     o.refCalHeight = h;
     o.refCalCount = count;
     o.refCalEnabled = 1;
+    o.refCalGen++;
+    if (o.device >= 0) cudaSetDevice(o.device);
+    o.refCalPlanes.clear();   // frees device planes (cudaFree waits for kernels using them)
     return dh::ERR_SUCCESS;
 }
 }  // namespace
@@ -485,11 +485,26 @@ extern "C" int digHoloConfigGetRefCalibrationEnabled(int h) {
     Object* o = dhObjectForHandle(h);
     return o ? o->refCalEnabled : 0;
 }
-// The calibration as applied to the reconstructed fields: not built (see
-// above), so there is none to return.
+// The calibration as applied to the reconstructed fields (digHolo.cpp:4912-4924):
+// [item][pol][height][width] with the field's axes, for the geometry of the
+// last batch; null until a batch with an applicable calibration ran.
 extern "C" complex64* digHoloConfigGetRefCalibrationFields(int h, int* wavelengthCount, int* polCount, float** x,
                                                            float** y, int* width, int* height) {
-    (void)h;
-    *wavelengthCount = 0; *polCount = 0; *x = nullptr; *y = nullptr; *width = 0; *height = 0;
-    return nullptr;
+    if (wavelengthCount) *wavelengthCount = 0;
+    if (polCount) *polCount = 0;
+    if (x) *x = nullptr;
+    if (y) *y = nullptr;
+    if (width) *width = 0;
+    if (height) *height = 0;
+    Object* o = dhObjectForHandle(h);
+    if (!o) return nullptr;
+    std::lock_guard<std::mutex> g(o->lock);
+    if (dh::objRefCalFieldsToHost(*o) != dh::ERR_SUCCESS) return nullptr;
+    if (wavelengthCount) *wavelengthCount = o->refCalCount;
+    if (polCount) *polCount = o->polCount;
+    if (x) *x = o->hRefCalX.data();
+    if (y) *y = o->hRefCalY.data();
+    if (width) *width = o->geo.nx;
+    if (height) *height = o->geo.ny;
+    return reinterpret_cast<complex64*>(o->hRefCalFields.ptr);
 }

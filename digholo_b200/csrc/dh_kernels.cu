@@ -173,6 +173,12 @@ __device__ Stat6 blockReduceStat(Stat6 s, Stat6* scratch) {
 }  // namespace
 
 // One block per (frame, polarisation).
+// field x calibration with the reference's complex product, real part fused
+// (cmul, digHolo.cpp:885-892)
+__device__ __forceinline__ float2 calMul(float2 a, float2 c) {
+    return make_float2(__fmaf_rn(a.x, c.x, -__fmul_rn(a.y, c.y)), __fmaf_rn(a.x, c.y, __fmul_rn(a.y, c.x)));
+}
+
 __global__ void __launch_bounds__(INV_THREADS) k_inverse(DhInvParams p) {
     extern __shared__ float2 sm[];
     const int unit = blockIdx.x;
@@ -217,6 +223,15 @@ __global__ void __launch_bounds__(INV_THREADS) k_inverse(DhInvParams p) {
         }
         __syncthreads();
         fft_dit(fld, H, ld, 1, p.logW, true, false, p.twiddle);
+    }
+    if (p.refCal) {
+        // reference-wave calibration of the IFFT output (digHolo.cpp:8736-8758, 8770-8782)
+        const float2* cal = p.refCal + (size_t)pol * npix;
+        for (int e = threadIdx.x; e < npix; e += blockDim.x) {
+            const int y = e >> lognx, x = e & (nx - 1);
+            fld[y * ld + x] = calMul(fld[y * ld + x], cal[e]);
+        }
+        __syncthreads();
     }
 
     // Field statistics over the whole untilted field (windowRadius = 0,
@@ -419,7 +434,9 @@ __global__ void __launch_bounds__(DFT_THREADS) k_inverse_dft(DhInvParams p) {
             t += y;
             if (t >= ny) t -= ny;
         }
-        fld[y * ld + x] = make_float2(ar, ai);
+        // reference-wave calibration of the IFFT output (digHolo.cpp:8736-8758)
+        fld[y * ld + x] = p.refCal ? calMul(make_float2(ar, ai), p.refCal[(size_t)pol * npix + e])
+                                   : make_float2(ar, ai);
     }
     __syncthreads();
 
@@ -689,6 +706,7 @@ size_t dh_inverse_smem_bytes(const DhInvParams& p) {
 cudaError_t dh_launch_inverse(const DhInvParams& p, cudaStream_t s) {
     if (p.w != (1 << p.logw) || p.h != (1 << p.logh)) return cudaErrorNotSupported;   // power-of-two windows only
     const size_t smem = dh_inverse_smem_bytes(p);
+    if (smem > 227 * 1024) return cudaErrorNotSupported;
     cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse), (int)smem);
     if (e != cudaSuccess) return e;
     // small (low-resolution) fields: one thread per pair of pixels, at least two warps

@@ -275,6 +275,10 @@ int objInitDevice(Object& o) {
     DH_CUDA(o, cudaStreamCreateWithFlags(&o.copyStream2, cudaStreamNonBlocking));
     DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy2[0], cudaEventDisableTiming));
     DH_CUDA(o, cudaEventCreateWithFlags(&o.evCopy2[1], cudaEventDisableTiming));
+    DH_CUDA(o, cudaStreamCreateWithFlags(&o.d2hStream, cudaStreamNonBlocking));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evChunk[0], cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evChunk[1], cudaEventDisableTiming));
+    DH_CUDA(o, cudaEventCreateWithFlags(&o.evD2H, cudaEventDisableTiming));
     DH_CUDA(o, cudaEventCreate(&o.evStart));
     DH_CUDA(o, cudaEventCreate(&o.evStop));
     // twiddle(k) = exp(-2 pi i k / 4096), double precision rounded to float
@@ -769,6 +773,20 @@ static void inverseParams(Object& o, DhInvParams& ip, int withOverlap) {
     ip.twiddle = o.dTwiddle.as<float2>();
 }
 
+// The reference-wave calibration planes of this batch, where a calibration
+// applies (digHolo.cpp:8242-8246); lookupOnly: planes computed by an earlier
+// batch only (nothing is allocated).
+static int calParams(Object& o, DhInvParams& ip, bool lookupOnly = false) {
+    if (!objRefCalApplies(o)) return ERR_SUCCESS;
+    int r = objRefCalCheckShape(o, ip);
+    if (r) return r;
+    const float2* planes = nullptr;
+    r = objRefCalPlanes(o, o.sweepLambda >= 0 ? o.sweepLambda : 0, &planes, lookupOnly);
+    if (r) return r;
+    ip.refCal = planes;
+    return ERR_SUCCESS;
+}
+
 // Forward stage: the TMA-fed persistent kernel where the shape and the
 // alignment allow it, else the register kernel, else the generic one.
 static cudaError_t launchForward(Object& o, const DhFwdParams& fp, bool mayAlloc = true) {
@@ -860,6 +878,16 @@ static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) 
 // block-per-unit kernel; low-resolution fields whose sides are not powers of
 // two: the DFT kernel.
 static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc = true) {
+    if (ip.refCal) {
+        // the calibration multiplies the IFFT output in the block-per-unit kernels
+        cudaError_t e = dh_launch_inverse(ip, o.stream);
+        if (e == cudaSuccess) { o.lastInverseKernel = 1; o.lastOverlapKernel = 1; return e; }
+        if (e != cudaErrorNotSupported || !ip.lowres) return e;
+        cudaGetLastError();
+        e = dh_launch_inverse_dft(ip, o.stream);
+        if (e == cudaSuccess) { o.lastInverseKernel = 6; o.lastOverlapKernel = 1; }
+        return e;
+    }
     if (o.inverseKernel == 2) return launchBands(o, ip, mayAlloc);
     if (o.inverseKernel == 0 || o.inverseKernel == 3) {   // 3: as 0 where not fused
         cudaError_t e = dh_launch_inverse_lo(ip, o.stream);
@@ -948,7 +976,7 @@ static int launchChunk(Object& o, const DhFwdParams& fp0, const DhInvParams& ip0
         // tensor-core forward with 16 x 16 low-resolution fields.  Measured
         // slower than the two launches, whose inverse kernel runs many more
         // units at once than the forward kernel's epilogue groups can.
-        if ((o.forwardKernel == 0 || o.forwardKernel == 4) && o.inverseKernel == 3) {
+        if ((o.forwardKernel == 0 || o.forwardKernel == 4) && o.inverseKernel == 3 && !ip.refCal) {
             cudaError_t fe = dh_launch_forward_i8_fused(fp, ip, o.stream);
             if (fe == cudaSuccess) {
                 o.lastForwardKernel = 4;
@@ -1212,8 +1240,10 @@ static int launchBatchDevice(Object& o, const DhFwdParams& fp, const DhInvParams
 }
 
 // Full pipeline for the batch: stage -> forward -> inverse (+overlap).
-// With host frames the batch is split in chunks whose window copies overlap
-// the previous chunk's kernels.
+// With host frames the batch is split in two chunks: the kernels of the
+// first run while the second's window copies arrive, so only the small
+// second chunk's kernels follow the last copy.  Each copy operation costs a
+// few microseconds of DMA setup, so more chunks lengthen the copy.
 static int processBatchLocked(Object& o, int syncCoefs);
 
 // Transposed uint16 frames (digHoloSetBatchUint16 with transpose): each frame
@@ -1274,8 +1304,15 @@ static int processSweepLocked(Object& o, int syncCoefs) {
         ~Restore() {
             o.cfg = c; o.frames = f; o.framesOnDevice = d; o.framesTransposed = t;
             o.batchCal = cal; o.batchCalCount = calCount; o.batchCalVersion++;
+            o.sweepLambda = -1; o.batchCalCaller = nullptr;
         }
     } restore{o, saved, o.frames, o.framesOnDevice, o.framesTransposed, calSaved, calCount};
+    // the reference-wave calibration of each sub-batch: its wavelength index,
+    // the batch's centre wavelength and the caller's batch calibration
+    o.sweepCentre = saved.wavelengthCentre;
+    o.batchCalCaller = &restore.cal;
+    o.batchCalCallerCount = calCount;
+    o.batchCalCallerPol = calPol;
     DH_CUDA(o, o.dSweepFrames.ensure((size_t)S * frameBytes));
     int P = 0, M = 0, Mout = 0, nx = 0, ny = 0, keep32 = o.keepField32, active = 0;
     for (int l = 0; l < L; l++) {
@@ -1305,6 +1342,7 @@ static int processSweepLocked(Object& o, int syncCoefs) {
         o.cfg.wavelengthCentre = lams[l];
         o.cfg.lambdaRange[0] = lams[0];
         o.cfg.lambdaRange[1] = lams[L - 1];
+        o.sweepLambda = l;
         r = processBatchLocked(o, 0);
         if (r) return r;
         P = o.polCount; M = o.modeCount; nx = o.geo.nx; ny = o.geo.ny;
@@ -1373,10 +1411,6 @@ static int processSweepLocked(Object& o, int syncCoefs) {
 }
 
 static int processAnyLocked(Object& o, int syncCoefs) {
-    // the reference applies an enabled calibration of the frames' size
-    // (digHolo.cpp:8233-8240); applying it is not built here
-    if (o.refCalEnabled && o.refCalWidth == o.cfg.frameWidth && o.refCalHeight == o.cfg.frameHeight)
-        return fail(o, ERR_ERROR, "reference-wave calibration is set and enabled: applying it is not supported by this library");
     objWavelengthUpdate(o);
     if (o.wavelengths.size() > 1) return processSweepLocked(o, syncCoefs);
     o.cfg.lambdaRange[0] = o.cfg.lambdaRange[1] = 0.f;
@@ -1572,7 +1606,9 @@ static int processBatchLocked(Object& o, int syncCoefs) {
         ~ChoiceRestore() { if (active) { o.forwardKernel = f; o.inverseKernel = i; } }
     } choiceRestore{o, o.forwardKernel, o.inverseKernel, false};
     bool planNeeded = false;
-    if (o.cfg.fftwPlanMode > 0 && o.forwardKernel == 0 && o.inverseKernel == 0 && o.avgCount <= 1 && !o.useSnaps) {
+    bool earlyCoefs = false;
+    if (o.cfg.fftwPlanMode > 0 && o.forwardKernel == 0 && o.inverseKernel == 0 && o.avgCount <= 1 && !o.useSnaps &&
+        !objRefCalApplies(o)) {
         int pf = 0, pi = 0;
         if (objPlanLookup(o, &pf, &pi, nullptr)) {
             o.forwardKernel = pf;
@@ -1589,6 +1625,8 @@ static int processBatchLocked(Object& o, int syncCoefs) {
     forwardParams(o, fp);
     DhInvParams ip;
     inverseParams(o, ip, 1);
+    r = calParams(o, ip);
+    if (r) return r;
     // the last stats column (aggregate over the batch) is filled on request
     if (o.avgCount > 1) {
         r = stageFrames(o, 0, B * o.avgCount, fp, 0);
@@ -1606,10 +1644,20 @@ static int processBatchLocked(Object& o, int syncCoefs) {
         DH_CUDA(o, cudaEventRecord(o.evStart, o.stream));
         DH_CUDA(o, cudaStreamWaitEvent(o.copyStream, o.evStart, 0));
         if (P > 1) DH_CUDA(o, cudaStreamWaitEvent(o.copyStream2, o.evStart, 0));
-        const int chunk = std::max(1, std::min(B, (B + 7) / 8));
+        const int tail = B >= 32 ? std::max(1, B / 16) : 0;
+        const int bounds[3] = {0, B - tail, B};
+        // coefficients of each chunk go to the host as soon as its kernels
+        // end (HG output basis: nothing is applied to them after the loop)
+        const size_t chunkCoef = (size_t)P * o.modeCount * sizeof(float2);
+        earlyCoefs = syncCoefs && o.modeCount > 0 && o.cfg.basisType == 0 && !planNeeded && o.dCoefs.ptr;
+        if (earlyCoefs) {
+            if (!o.hCoefs.ensure((size_t)B * chunkCoef)) return fail(o, ERR_MEMORYALLOCATION, "host coefficient buffer");
+            DH_CUDA(o, cudaStreamWaitEvent(o.d2hStream, o.evStart, 0));
+        }
         int slot = 0;
-        for (int f0 = 0; f0 < B; f0 += chunk) {
-            const int f1 = std::min(B, f0 + chunk);
+        for (int c = 0; c < 2; c++) {
+            const int f0 = bounds[c], f1 = bounds[c + 1];
+            if (f1 <= f0) continue;
             DhFwdParams fpc = fp;
             r = stageFrames(o, f0, f1, fpc, 1);
             if (r) return r;
@@ -1621,7 +1669,18 @@ static int processBatchLocked(Object& o, int syncCoefs) {
             }
             r = launchChunk(o, fpc, ip, f0, f1);
             if (r) return r;
+            if (earlyCoefs) {
+                DH_CUDA(o, cudaEventRecord(o.evChunk[slot], o.stream));
+                DH_CUDA(o, cudaStreamWaitEvent(o.d2hStream, o.evChunk[slot], 0));
+                DH_CUDA(o, cudaMemcpyAsync(o.hCoefs.as<char>() + (size_t)f0 * chunkCoef,
+                                           o.dCoefs.as<char>() + (size_t)f0 * chunkCoef, (size_t)(f1 - f0) * chunkCoef,
+                                           cudaMemcpyDeviceToHost, o.d2hStream));
+            }
             slot ^= 1;
+        }
+        if (earlyCoefs) {
+            DH_CUDA(o, cudaEventRecord(o.evD2H, o.d2hStream));
+            DH_CUDA(o, cudaStreamWaitEvent(o.stream, o.evD2H, 0));
         }
     }
     o.processedFFT = o.processedIFFT = o.processedTilt = 1;
@@ -1662,6 +1721,11 @@ static int processBatchLocked(Object& o, int syncCoefs) {
         if (r) return r;
         r = applyBasis(o);
         if (r) return r;
+    }
+    if (earlyCoefs) {
+        // the coefficients are already on their way (the stream waits for them)
+        DH_CUDA(o, cudaStreamSynchronize(o.stream));
+        return objCheckStatus(o);
     }
     if (syncCoefs) return objCoefsToHost(o);
     return ERR_SUCCESS;
@@ -1711,6 +1775,10 @@ int objProcessNoAlloc(Object& o, const void* frames, int B, int u16, float2* win
     fp.window = window;
     DhInvParams ip;
     inverseParams(o, ip, o.cfg.maxMG > 0);
+    {
+        const int rc = calParams(o, ip, true);
+        if (rc) return rc;
+    }
     ip.window = window;
     ip.frameCount = B;
     ip.fieldR = fieldR;
@@ -1741,6 +1809,10 @@ int objInverseAux(Object& o, const float2* window, int frameCount, float2* field
                   float* scratchStats) {
     DhInvParams ip;
     inverseParams(o, ip, 0);
+    {
+        const int rc = calParams(o, ip);
+        if (rc) return rc;
+    }
     ip.frameCount = frameCount;
     ip.statsStride = frameCount + 1;
     ip.window = window;
@@ -1822,6 +1894,8 @@ static int runStages(Object& o, int withInverse, int withOverlap) {
     if (r) return r;
     DhInvParams ip;
     inverseParams(o, ip, withOverlap);
+    r = calParams(o, ip);
+    if (r) return r;
     if (!withInverse) ip.fieldR = nullptr;
     r = o.avgCount > 1 ? launchAveraged(o, fp, ip) : launchChunk(o, fp, ip, 0, o.batchCount);
     if (r) return r;

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "dh_params.h"
@@ -131,6 +132,11 @@ struct Object {
     // second DMA queue next to the first)
     cudaStream_t copyStream2 = nullptr;
     cudaEvent_t evCopy2[2] = {nullptr, nullptr};
+    // coefficients of finished chunks leave for the host on their own stream
+    // (the device-to-host DMA direction) while later chunks' frames arrive
+    cudaStream_t d2hStream = nullptr;
+    cudaEvent_t evChunk[2] = {nullptr, nullptr};
+    cudaEvent_t evD2H = nullptr;
     cudaEvent_t evStart = nullptr, evStop = nullptr;
     int userStream = 0;                 // stream supplied by digHoloB200SetStream (not owned)
     int timing = 0;                     // record per-stage events in ProcessBatch
@@ -222,6 +228,25 @@ struct Object {
     // digHolo.cpp:5309-5540): the stored per-pixel factors [L][height][width]
     std::vector<float> refCal;
     int refCalWidth = 0, refCalHeight = 0, refCalCount = 0, refCalEnabled = 0;
+    int refCalGen = 0;                  // advanced by every calibration setter
+    DevBuf dRefCalFrames;               // the stored factors on the device
+    int refCalFramesGen = -1;
+    DevBuf dRefCalScratch, dRefCalTables;
+    // reconstructed calibration planes [pol][ny][nx], one per calibration
+    // item, wavelength and geometry in use (key: every input of the planes)
+    struct RefCalPlanes {
+        std::vector<unsigned char> key;
+        DevBuf planes;
+    };
+    std::vector<std::unique_ptr<RefCalPlanes>> refCalPlanes;
+    HostBuf hRefCalFields;
+    std::vector<float> hRefCalX, hRefCalY;
+    // during a multi-wavelength batch: the sub-batch's wavelength index and
+    // the batch calibration as the caller set it (the sub-batches rewrite it)
+    int sweepLambda = -1;
+    float sweepCentre = 0.f;
+    const std::vector<float>* batchCalCaller = nullptr;
+    int batchCalCallerCount = 0, batchCalCallerPol = 0;
     // frames loaded by digHoloSetFrameBufferFromFile (owned, float32)
     std::vector<float> ownFrames;
     // digHoloConfigBackupSave / Load
@@ -290,6 +315,11 @@ int objCalcMetrics(Object& o);
 float objAutoAlign(Object& o);
 // The wavelength array in use (digHoloWavelengthUpdate, digHolo.cpp:7823-7862).
 void objWavelengthUpdate(Object& o);
+// Reference-wave calibration (dh_refcal.cpp).
+bool objRefCalApplies(const Object& o);
+int objRefCalCheckShape(Object& o, const DhInvParams& ip);
+int objRefCalPlanes(Object& o, int item, const float2** out, bool lookupOnly);
+int objRefCalFieldsToHost(Object& o);
 
 // Geometry helpers (host, float32 emulation of the reference).
 void fftWindowGeometry(const Config& c, int polCount, Geometry& g);

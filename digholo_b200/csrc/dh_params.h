@@ -79,6 +79,29 @@ struct DhInvParams {
     float2* coefs;          // out: [frame][pol*modeCount + mode]
     const float2* twiddle;
     int* status;            // set by a kernel whose bounded wait expired (host-mapped)
+    // optional reference-wave calibration [pol][ny][nx]: multiplies the IFFT
+    // output before the statistics and the tilt removal (block-per-unit kernels)
+    const float2* refCal;
+};
+
+// Separable DFT stage of the calibration planes: out[u][a][b] =
+// sum_k in[u inU + a inA + b inB + k inK] exp(sign 2 pi i fo fk / N), fo the
+// frequency of the output index (a or b), fk that of k (each an index table
+// per polarisation u % fP, or the index itself), accumulated in FP64 and
+// rounded to FP32; then optionally times ufac[u] (complex) and fac[u % fP][a][b].
+struct DhCalDft {
+    const float2* in;
+    long long inU, inA, inB, inK;
+    float2* out;            // dense [U][A][B]
+    int U, A, B, K;
+    const int* freqOut;     // [fP][A or B] or null
+    int outOnA;             // 1: freqOut indexes a, 0: b
+    const int* freqK;       // [fP][K] or null
+    int fP;                 // period of u for the per-polarisation tables (>= 1)
+    int N;                  // transform length (<= 4096; frequencies are non-negative)
+    int sign;               // -1 forward, +1 inverse
+    const float2* ufac;     // [U] or null
+    const float* fac;       // [fP][A][B] or null
 };
 
 // FP64 Hermite-Gaussian basis along one axis (digHolo.cpp:1269-1484).

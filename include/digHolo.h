@@ -337,10 +337,15 @@ complex64* digHoloProcessBatchFrequencySweepLinear(int handleIdx, int* batchCoun
 complex64* digHoloProcessBatchWavelengthSweepArbitrary(int handleIdx, int* batchCount, int* modeCount, int* polCount,
                                                        float* wavelengths, int lambdaCount);
 /* replace digHolo.h:369, 384, 400, 409, 417, 437: the reference-wave
- * calibration is stored (as the reference normalises and inverts it) and can
- * be enabled and disabled, but applying it to the fields is not built: a
- * batch whose frames have the calibration's size fails while it is enabled,
- * and GetRefCalibrationFields returns NULL */
+ * calibration, stored as the reference normalises and inverts it; while
+ * enabled and of the frames' size, its reconstructed planes (c2c FFT of the
+ * FFT windows, Fourier window at zero tilt, IFFT; digHolo.cpp:6729-6830,
+ * 8253-8285) multiply every frame's IFFT output before the field analysis
+ * (digHolo.cpp:8736-8758).  Applied by the block-per-unit inverse kernels:
+ * full-resolution fields up to 128 x 128 and low-resolution fields up to
+ * about 112 x 112; larger fields fail with DIGHOLO_ERROR_INVALIDDIMENSION.
+ * GetRefCalibrationFields returns the planes [item][pol][height][width] for
+ * the last batch's geometry, NULL before one. */
 int digHoloConfigSetRefCalibrationIntensity(int handleIdx, unsigned short* cal, int wavelengthCount, int width,
                                             int height);
 int digHoloConfigSetRefCalibrationField(int handleIdx, complex64* cal, int wavelengthCount, int width, int height);

@@ -29,6 +29,8 @@ It restates, step by step, the work of digHoloProcessBatch
   auto_align_snap     AutoAlign parameter estimate    digHolo.cpp:11517-11970
   auto_focus          its focus search                digHolo.cpp:11181-11499
   dct2_redft          FFTW REDFT10 / REDFT01 (2D)     digHolo.cpp:7393-7420
+  ref_cal_store       reference-wave calibration      digHolo.cpp:5419-5555
+  ref_cal_planes      its reconstructed planes        digHolo.cpp:6729-6830, 8253-8285
 
 Two flavours are produced by :func:`process_batch`:
 
@@ -63,7 +65,7 @@ class Config:
                  fft_window=(0, 0), window_radius_deg=0.4, resolution_mode=0,
                  wavelength=1565e-9, beam_centre=None, tilt_deg=None, defocus=None,
                  waist=None, max_mg=0, fill_factor=1, pol_lock_tilt=0, pol_lock_defocus=0,
-                 pol_lock_waist=1, avg_count=1, avg_mode=0, batch_cal=None):
+                 pol_lock_waist=1, avg_count=1, avg_mode=0, batch_cal=None, ref_cal=None):
         self.frame_width = frame_width
         self.frame_height = frame_height
         self.pixel_size = F32(pixel_size)
@@ -87,6 +89,9 @@ class Config:
         self.avg_mode = avg_mode
         # digHoloConfigSetBatchCalibration: complex (polCount, batchCount) factors
         self.batch_cal = None if batch_cal is None else np.asarray(batch_cal, dtype=np.complex64)
+        # digHoloConfigSetRefCalibration*: the stored factors (count, frameHeight,
+        # frameWidth) complex, as ref_cal_store forms them
+        self.ref_cal = ref_cal
         while len(self.beam_centre) < 2:
             self.beam_centre.append([F32(0), F32(0)])
         while len(self.tilt_deg) < 2:
@@ -160,15 +165,18 @@ def _tilts_rad(cfg):
     return out
 
 
-def ifft_windows(cfg, W, H, kx, ky):
-    """IFFT window size and corners (digHolo.cpp:7868-8048), single wavelength."""
+def ifft_windows(cfg, W, H, kx, ky, zero_tilt=False):
+    """IFFT window size and corners (digHolo.cpp:7868-8048), single wavelength.
+
+    zero_tilt: the calibration's window (no zernCoefs: tilt 0, and a c2c
+    plane, so no clamp to the positive kx half; digHolo.cpp:6812-6818)."""
     lam = cfg.wavelength
     k0max = F32(F32(2) * PI_F / lam)
     k0min = k0max
     dkx = F32(kx[1] - kx[0])
     dky = F32(ky[1] - ky[0])
     r0 = F32(cfg.window_radius_deg * UNIT_ANGLE)
-    tilts = _tilts_rad(cfg)
+    tilts = [(F32(0), F32(0))] * cfg.pol_count if zero_tilt else _tilts_rad(cfg)
     woi_cx, woi_cy, ww, wh = [], [], [], []
     for pol in range(cfg.pol_count):
         tx, ty = tilts[pol]
@@ -189,7 +197,7 @@ def ifft_windows(cfg, W, H, kx, ky):
     sx, sy = [], []
     for pol in range(cfg.pol_count):
         nsx = int(woi_cx[pol] - w / 2.0)
-        if nsx < W // 2:
+        if nsx < W // 2 and not zero_tilt:
             nsx = W // 2
         if nsx < 0:
             nsx = 0
@@ -587,6 +595,99 @@ def average_windows(win, batch, avg, mode, lowres, W, H, w, h, SX, SY, cal=None)
     return out
 
 
+def ref_cal_store(intensity=None, field=None):
+    """The factors the reference stores for a reference-wave calibration
+    (digHolo.cpp:5419-5555), in float32: from uint16 intensities I,
+    sqrt(1 / (I / max I)); from complex fields E, the componentwise
+    (1 / (re / max|E|), -1 / (im / max|E|)) -- not the complex inverse --
+    with both parts 0 where either is NaN or infinite.  Returns complex64
+    (count, height, width)."""
+    if intensity is not None:
+        I = np.asarray(intensity, dtype=np.uint16)
+        scale = F32(F32(1.0) / F32(int(I.max())))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            v = (F32(1.0) / (I.astype(F32) * scale)).astype(F32)
+        v[~np.isfinite(v)] = 0
+        return np.sqrt(v).astype(F32).astype(np.complex64)
+    E = np.asarray(field, dtype=np.complex64)
+    re, im = E.real.astype(F32), E.imag.astype(F32)
+    mx = F32(np.sqrt(F32((re * re + im * im).astype(F32).max())))
+    scale = F32(F32(1.0) / mx)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        vr = (F32(1.0) / (re * scale)).astype(F32)
+        vi = (F32(-1.0) / (im * scale)).astype(F32)
+    bad = ~(np.isfinite(vr) & np.isfinite(vi))
+    vr[bad] = 0
+    vi[bad] = 0
+    return (vr + 1j * vi).astype(np.complex64)
+
+
+def ref_cal_planes(cfg):
+    """The reconstructed calibration planes (count, P, ny, nx) that multiply
+    the IFFT output of every frame before the field analysis and the tilt
+    removal (digHolo.cpp:8736-8758), one wavelength.
+
+    Each stored calibration frame goes through the batch path with the
+    frames' FFT windows, as a complex frame: a c2c FFT of each
+    polarisation's window (digHolo.cpp:6729-6784), the Fourier window at
+    zero tilt with no beam-centre phase -- the window placed around kx = ky = 0,
+    the aperture mask centred there, the inverse pixel sinc, the batch
+    calibration of item `count index`, and the normalisation
+    sqrt(res / (W H)) / sqrt(W H ifftLength) (digHolo.cpp:8253-8285, and
+    digHoloCopyWindow's c2c branches, digHolo.cpp:1808-2122) -- and an
+    unnormalised IFFT of the field's size.  Low resolution places the window
+    fftshifted into an h x w plane, full resolution at its own frequencies in
+    the H x W plane."""
+    cal = np.asarray(cfg.ref_cal)
+    count = cal.shape[0]
+    P = cfg.pol_count
+    lowres = cfg.resolution_mode == 1
+    W, H, cxs, cys = fft_windows(cfg)
+    kx, ky = k_axes(W, H, cfg.pixel_size)
+    w, h, _, _ = ifft_windows(cfg, W, H, kx, ky)
+    _, _, SXc, SYc = ifft_windows(cfg, W, H, kx, ky, zero_tilt=True)
+    nx, ny = (w, h) if lowres else (W, H)
+    norm0 = F32(np.sqrt(F32((1.0 * nx * ny) / (1.0 * W * H))))
+    ifft_len = (w * h) if lowres else (W * H)
+    norm = float(F32(float(norm0) / math.sqrt(float(W * H) * float(ifft_len))))
+    k0 = F32(F32(2) * PI_F / cfg.wavelength)
+    kr = F32(k0 * F32(math.sin(float(F32(cfg.window_radius_deg * UNIT_ANGLE)))))
+    r02 = F32(kr * kr)
+    ky_shift = abs(float(ky[1] - ky[0]) * H)
+    hp = 0.5 * float(cfg.pixel_size)
+    out = np.zeros((count, P, ny, nx), dtype=np.complex128)
+    i = np.arange(w)
+    for c in range(count):
+        for pol in range(P):
+            F = np.fft.fft2(cal[c, cys[pol]:cys[pol] + H, cxs[pol]:cxs[pol] + W].astype(np.complex128))
+            bf = 1.0
+            if getattr(cfg, "batch_cal", None) is not None:
+                bc = cfg.batch_cal
+                bf = complex(bc[pol % bc.shape[0]][c % bc.shape[1]])
+            plane = np.zeros((ny, nx), dtype=np.complex128)
+            col = i + SXc[pol] - W // 2
+            col = np.where(col < 0, col + W, col)
+            ok = (col >= 0) & (col < W)
+            colc = np.clip(col, 0, W - 1)
+            kxv = kx[colc]
+            env_x = xcsc(kxv.astype(np.float64) * hp) if cfg.fill_factor else np.ones(w)
+            for j in range(h):
+                jsy = j + SYc[pol]
+                row = (jsy + H // 2) % H
+                shift = ky_shift if jsy < 0 else (-ky_shift if jsy > H else 0.0)
+                dky = F32(F32(ky[row]) - F32(F32(0) + F32(shift)))
+                dr2 = (kxv * kxv).astype(F32) + F32(dky * dky)
+                inside = (dr2.astype(F32) <= r02) & ok
+                env = env_x * (xcsc(np.array([float(ky[row]) * hp]))[0] if cfg.fill_factor else 1.0)
+                vals = np.where(inside, F[row, colc] * bf * norm * env, 0.0)
+                if lowres:
+                    plane[(j + h // 2) % h, (i + w // 2) % w] = vals
+                else:
+                    plane[row, colc[ok]] = vals[ok]
+            out[c, pol] = np.fft.ifft2(plane) * (nx * ny)
+    return out
+
+
 def r2c_windows(frames, cfg, W, H, cxs, cys):
     """FP64 R2C of each polarisation's FFT window: (B, P, H, W/2+1)."""
     f = np.asarray(frames, dtype=np.float64)
@@ -615,6 +716,10 @@ def process_batch(frames, cfg, quantised=True):
     xax, yax = ifft_axes(cfg, W, H, w, h)
     nx, ny = xax.size, yax.size
     Fplanes = r2c_windows(frames, cfg, W, H, cxs, cys)
+    cal_planes = None
+    rc = getattr(cfg, "ref_cal", None)
+    if rc is not None and rc.shape[1] == cfg.frame_height and rc.shape[2] == cfg.frame_width:
+        cal_planes = ref_cal_planes(cfg)
     res = {"W": W, "H": H, "cx": cxs, "cy": cys, "w": w, "h": h, "SX": SX, "SY": SY,
            "x": xax, "y": yax, "kx": kx, "ky": ky, "fourier": Fplanes,
            "fft_stats": [fourier_analysis(Fplanes[:, p], kx, ky, cfg.wavelength, cfg.window_radius_deg)
@@ -640,6 +745,8 @@ def process_batch(frames, cfg, quantised=True):
             win = win * cal[:, None, None]
         windows[:, pol] = win
         E = np.fft.ifft2(win) * (win.shape[-1] * win.shape[-2])
+        if cal_planes is not None:
+            E = E * cal_planes[0, pol]
         untilted[:, pol] = E
         st = _safe_stats(E, xax, yax)
         stats.append(st)

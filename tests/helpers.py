@@ -26,3 +26,47 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.complex128)
     b = np.asarray(b, dtype=np.complex128)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def ref_calibration(cfg, kind, count=1, seed=3):
+    """A reference-wave calibration of the frame's size: uint16 intensities
+    of a broad Gaussian beam over a floor with noise, or complex fields with
+    ripples in both parts (the reference inverts the parts separately, so
+    neither may be zero).  Returns the raw array for the setter."""
+    rng = np.random.default_rng(seed)
+    fh, fw = cfg.frame_height, cfg.frame_width
+    yy, xx = np.mgrid[0:fh, 0:fw]
+    if kind == "intensity":
+        g = 20000 * np.exp(-((xx - fw / 2) ** 2 + (yy - fh / 2) ** 2) / (2 * (0.4 * fw) ** 2)) + 3000
+        return np.stack([g * (1 + 0.1 * c) + rng.integers(0, 200, (fh, fw)) for c in range(count)]).astype(np.uint16)
+    return np.stack([(1.0 + 0.3 * np.cos(xx / (37.0 + c)) + 0.2j + 0.1j * np.sin(yy / 23.0)) * np.exp(0.3j * (c + 1))
+                     for c in range(count)]).astype(np.complex64)
+
+
+def set_ref_calibration(L, h, cfg, kind, cal):
+    """Apply the calibration through the C ABI and record its stored factors
+    in cfg for the oracle."""
+    import ctypes as C
+    count, fh, fw = cal.shape
+    if kind == "intensity":
+        r = L.digHoloConfigSetRefCalibrationIntensity(h, cal.ctypes.data_as(C.POINTER(C.c_ushort)), count, fw, fh)
+        cfg.ref_cal = O.ref_cal_store(intensity=cal)
+    else:
+        r = L.digHoloConfigSetRefCalibrationField(h, cal.ctypes.data_as(C.POINTER(C.c_float)), count, fw, fh)
+        cfg.ref_cal = O.ref_cal_store(field=cal)
+    assert r == 0
+
+
+def ref_calibration_planes(L, h):
+    """digHoloConfigGetRefCalibrationFields as (count, pol, height, width)
+    complex64, or None."""
+    import ctypes as C
+    n, p, w, hh = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    x, y = C.POINTER(C.c_float)(), C.POINTER(C.c_float)()
+    ptr = L.digHoloConfigGetRefCalibrationFields(h, C.byref(n), C.byref(p), C.byref(x), C.byref(y), C.byref(w),
+                                                  C.byref(hh))
+    if not ptr:
+        return None
+    N = n.value * p.value * w.value * hh.value
+    a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(2 * N,)).copy().view(np.complex64)
+    return a.reshape(n.value, p.value, hh.value, w.value)

@@ -322,3 +322,33 @@ def test_frame_simulator_matches_live_reference(case):
     assert prm["G"] == Gr
     d = np.abs(r32 - o32)
     assert d.max() <= 1 and float((d > 0).mean()) <= 1e-4
+
+
+@pytest.mark.parametrize("workload,mode,kind,count", [
+    ("plain_320x256_f32_1pol", 1, "intensity", 1), ("plain_320x256_f32_1pol", 0, "field", 3),
+    ("batched_640x512_u16_2pol", 1, "field", 1), ("batched_640x512_u16_2pol", 0, "intensity", 2)])
+def test_ref_calibration_matches_live_reference(workload, mode, kind, count):
+    """Reference-wave calibration (digHoloConfigSetRefCalibrationIntensity /
+    Field): the oracle's reconstructed calibration planes against the
+    reference's digHoloConfigGetRefCalibrationFields (relative L2 <= 1e-6),
+    and the calibrated batch's fields and coefficients against the
+    reference's (the usual bounds).  The calibration changes the
+    coefficients by 0.8-9 % here, well above the comparison's bounds."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from helpers import ref_calibration, ref_calibration_planes, set_ref_calibration
+    hol = make_case(workload, 2)
+    cfg = config_for(hol, mode)
+    L = ref_lib.load()
+    h = L.digHoloCreate()
+    ref_lib.configure(L, h, cfg)
+    set_ref_calibration(L, h, cfg, kind, ref_calibration(cfg, kind, count))
+    r = ref_lib.run_batch(L, h, hol.frames)
+    rp = ref_calibration_planes(L, h)
+    op = O.ref_cal_planes(cfg)
+    assert rp is not None and rp.shape == op.shape
+    assert rel_l2(op, rp) <= 1e-6
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
+    plain = O.process_batch(hol.frames, config_for(hol, mode), quantised=True)
+    assert rel_l2(plain["coefs"], o["coefs"]) > 3e-3
