@@ -309,10 +309,12 @@ float objAutoAlignAdjoint(Object& o) {
         for (double v : gz) gn += v * v;
         gn = std::sqrt(gn);
         for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
-        const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.1);   // dB
+        // convergence in dB: half the plain search's termination tolerance
+        // (a sweep gaining at most terminationTol ends it, digHolo.cpp:12416, 12872)
+        const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.5);
         const int maxIter = 80, maxRounds = 8;
         int quiet = 0, round = 0;
-        bool firstUpdate = true;
+        bool firstUpdate = true, restarted = false;
         double lastRoundEnd = f;   // objective at the end of the previous round (before re-selection)
         std::vector<double> d(n), s(n), y(n), Hy(n);
         for (int it = 0; it < maxIter; it++) {
@@ -349,7 +351,21 @@ float objAutoAlignAdjoint(Object& o) {
                 const double tq = -slope * t * t / (2.0 * (ft - f - slope * t));
                 t = std::min(0.5 * t, std::max(0.1 * t, tq));
             }
-            if (!accepted) { apply(z); break; }
+            if (!accepted) {
+                // the quasi-Newton direction failed: once, restart from the
+                // scaled gradient before giving up (the MDL objective bends
+                // where its extreme eigenvalues cross)
+                if (!restarted) {
+                    restarted = true;
+                    firstUpdate = true;
+                    for (size_t i = 0; i < Hi.size(); i++) Hi[i] = 0.0;
+                    for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
+                    continue;
+                }
+                apply(z);
+                break;
+            }
+            restarted = false;
             double sy = 0.0;
             for (int i = 0; i < n; i++) {
                 s[i] = zt[i] - z[i];

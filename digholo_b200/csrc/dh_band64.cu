@@ -599,7 +599,8 @@ struct B64Plan {
 // 512 wide and 64 to 4096 high, IFFT windows of at most 64 x 64 (sides
 // multiples of 16), no overlap or the tensor-core overlap with maxMG <= 32.
 cudaError_t planB64(const DhInvParams& p, int overlapKind, B64Plan& pl) {
-    if (p.lowres) return cudaErrorNotSupported;
+    // a reference-wave calibration is applied by k_field_big, not here
+    if (p.lowres || p.refCal) return cudaErrorNotSupported;
     const int W = 1 << p.logW, H = 1 << p.logH;
     if (W != WF || H < 64 || H > TW_N) return cudaErrorNotSupported;
     if (p.w < 16 || p.h < 16 || p.w > 64 || p.h > 64 || p.w % 16 || p.h % 16) return cudaErrorNotSupported;

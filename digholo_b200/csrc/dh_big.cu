@@ -294,6 +294,16 @@ __global__ void __launch_bounds__(NT, 1) k_field_big(DhInvParams p, BigArgs a) {
             for (int k = 0; k < SL; k++) v[k] = cmul(v[k], xBase[ul * (SL + 1) + k]);
             ifftDIFf<SL>(v);
             const int y = TYc * (r & 15) + yBase + (r >> 4);
+            if (p.refCal) {
+                // reference-wave calibration of the IFFT output (digHolo.cpp:8736-8758, 8770-8782)
+                const float2* cal = p.refCal + ((size_t)pol * H + y) * W;
+#pragma unroll
+                for (int i = 0; i < SL; i++) {
+                    const float2 c = __ldg(&cal[TXc * brevF<4>(i) + ux]);
+                    v[i] = make_float2(__fmaf_rn(v[i].x, c.x, -__fmul_rn(v[i].y, c.y)),
+                                       __fmaf_rn(v[i].x, c.y, __fmul_rn(v[i].y, c.x)));
+                }
+            }
             if (!QUANT) {
                 // statistics over the untilted field (digHolo.cpp:8866-8870)
                 const float yv = p.yAxis[y];

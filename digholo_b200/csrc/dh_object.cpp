@@ -879,11 +879,13 @@ static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) 
 // two: the DFT kernel.
 static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc = true) {
     if (ip.refCal) {
-        // the calibration multiplies the IFFT output in the block-per-unit kernels
+        // the calibration multiplies the IFFT output in the block-per-unit
+        // kernels, or for larger full-resolution fields in k_field_big
         cudaError_t e = dh_launch_inverse(ip, o.stream);
         if (e == cudaSuccess) { o.lastInverseKernel = 1; o.lastOverlapKernel = 1; return e; }
-        if (e != cudaErrorNotSupported || !ip.lowres) return e;
+        if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
+        if (!ip.lowres) return launchBands(o, ip, mayAlloc);   // k_field_big: fields beyond one block
         e = dh_launch_inverse_dft(ip, o.stream);
         if (e == cudaSuccess) { o.lastInverseKernel = 6; o.lastOverlapKernel = 1; }
         return e;

@@ -135,7 +135,7 @@ struct RowRaw {
 // warp, so its exchange needs only warp barriers; the exchange reuses the
 // row's buffer, value (k1, t) at 16 k1 + (t ^ k1).
 template <bool U16>
-__global__ void __launch_bounds__(256, 3) k_plane_rows512(DhFourierParams q, int compact) {
+__global__ void __launch_bounds__(256, U16 ? 4 : 3) k_plane_rows512(DhFourierParams q, int compact) {
     extern __shared__ float2 sp[];
     float2* A = sp;                          // [RR][RN] z, the exchange, then X
     const DhFwdParams& f = q.f;

@@ -12,8 +12,9 @@
 // (low resolution: the window fftshifted into an h x w plane; full
 // resolution: at its own frequencies in the H x W plane).  The resulting
 // plane [pol][ny][nx] multiplies the IFFT output of every frame before the
-// field statistics and the tilt removal, inside the block-per-unit inverse
-// kernels (k_inverse, k_inverse_dft).
+// field statistics and the tilt removal, inside the inverse kernels that
+// carry it (k_inverse, k_inverse_dft, and k_field_big for full-resolution
+// fields beyond one block; the 512-wide band kernel leaves them to it).
 //
 // Item of a frame: 0 for a batch of one wavelength; in a multi-wavelength
 // batch, the sub-batch's wavelength index modulo the item count (the
@@ -84,17 +85,18 @@ bool objRefCalApplies(const Object& o) {
            o.refCalHeight == o.cfg.frameHeight;
 }
 
-// The block-per-unit inverse kernels carry the calibration: power-of-two
-// fields whose k_inverse shared memory fits, or low-resolution fields of the
-// DFT kernel.
+// The kernels that carry the calibration: k_inverse (power-of-two fields
+// whose shared memory fits), k_inverse_dft (low-resolution fields) and
+// k_field_big (full-resolution fields beyond one block).
 int objRefCalCheckShape(Object& o, const DhInvParams& ip) {
+    if (!ip.lowres) return ERR_SUCCESS;
     const bool pow2 = ip.w == (1 << ip.logw) && ip.h == (1 << ip.logh);
     if (pow2 && dh_inverse_smem_bytes(ip) <= 227 * 1024) return ERR_SUCCESS;
-    if (ip.lowres && ip.w % 16 == 0 && ip.h % 16 == 0 && dh_inverse_dft_smem_bytes(ip.w, ip.h, ip.maxMG) <= 227 * 1024)
+    if (ip.w % 16 == 0 && ip.h % 16 == 0 && dh_inverse_dft_smem_bytes(ip.w, ip.h, ip.maxMG) <= 227 * 1024)
         return ERR_SUCCESS;
     return fail(o, ERR_INVALIDDIMENSION,
-                "reference-wave calibration: this build applies it to fields of the block-per-unit inverse kernels "
-                "(full resolution up to 128 x 128, low resolution up to about 112 x 112)");
+                "reference-wave calibration: low-resolution fields above about 112 x 112 are not supported by this "
+                "build");
 }
 
 // Planes [pol][ny][nx] of calibration item `item` for the geometry in use.

@@ -202,9 +202,18 @@ WORKLOADS = {
                                      dtype="uint16", seed=1002),
     # frames excite columns of a Haar-random 120x120 transfer matrix with per-mode loss
     # (coefficients from transfer_coefs); frames are not normalised individually
+    # carrier (0.55, 0.45) of Nyquist: the Fourier window (radius |tilt| / 3)
+    # then holds all 120 modes of each polarisation at this waist (with the
+    # (0.25, 0.2) carrier the higher mode groups fall outside it and the batch
+    # coefficient matrix loses rank)
     "align_640x512_f32_2pol": dict(frame_count=512, frame_width=640, frame_height=512, pol_count=2,
                                    max_mg=15, waist=250e-6, snr_db=30, window=(128, 128),
-                                   dtype="float32", seed=1004, normalise_frames=False),
+                                   carrier=(0.55, 0.45), dtype="float32", seed=1004, normalise_frames=False),
+    # the same frames with the (0.25, 0.2) carrier: the parameter-estimate
+    # (snap) tests, whose parity with the reference was established on them
+    "snap_640x512_f32_2pol": dict(frame_count=512, frame_width=640, frame_height=512, pol_count=2,
+                                  max_mg=15, waist=250e-6, snr_db=30, window=(128, 128),
+                                  dtype="float32", seed=1004, normalise_frames=False),
     "largefield_2048_u16_2pol": dict(frame_count=256, frame_width=2048, frame_height=2048, pol_count=2,
                                      max_mg=30, waist=600e-6, snr_db=20, window=(512, 512),
                                      dtype="uint16", seed=1005, taper=True),

@@ -70,3 +70,28 @@ def ref_calibration_planes(L, h):
     N = n.value * p.value * w.value * hh.value
     a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(2 * N,)).copy().view(np.complex64)
     return a.reshape(n.value, p.value, hh.value, w.value)
+
+
+def reference_calibrated(workload, frames, mode, kind, count, window=None, sweep=None, tries=2):
+    """The reference build's batch with a reference-wave calibration, run in
+    a child process (refcal_child.py): the reference's calibrated batches
+    occasionally corrupt its heap, so they never run in the test process.  A
+    child that dies is run once more; its outputs are used only when it
+    completed."""
+    import os
+    import subprocess
+    import sys
+    import tempfile
+    child = os.path.join(os.path.dirname(os.path.abspath(__file__)), "refcal_child.py")
+    args = [str(workload), str(frames), str(mode), kind, str(count), str(window) if window else "-",
+            ",".join("%.6e" % v for v in sweep) if sweep else "-"]
+    last = ""
+    for _ in range(tries):
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "r.npz")
+            r = subprocess.run([sys.executable, child, out] + args, capture_output=True, text=True, timeout=900)
+            if r.returncode == 0 and os.path.exists(out):
+                z = np.load(out)
+                return {k: z[k] for k in z.files}
+            last = (r.stdout + r.stderr)[-2000:]
+    raise RuntimeError("reference child process failed: " + last)

@@ -59,7 +59,7 @@ def lib():
 
 @pytest.fixture(scope="module")
 def hol():
-    kw = dict(synth.WORKLOADS["align_640x512_f32_2pol"])
+    kw = dict(synth.WORKLOADS["snap_640x512_f32_2pol"])
     kw["frame_count"] = FRAMES
     kw["coefs"] = synth.transfer_coefs(FRAMES, 2, kw["max_mg"], 1004)
     return synth.generate(**kw)

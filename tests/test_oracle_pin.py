@@ -248,7 +248,7 @@ def test_snap_estimate_matches_live_reference():
     import ctypes as C
     from digholo_b200 import api, synth
     B = 16
-    kw = dict(synth.WORKLOADS["align_640x512_f32_2pol"])
+    kw = dict(synth.WORKLOADS["snap_640x512_f32_2pol"])
     kw.update(frame_count=B, coefs=synth.transfer_coefs(B, 2, kw["max_mg"], 1004))
     hol = synth.generate(**kw)
     cfg = config_for(hol, 1)
@@ -324,31 +324,35 @@ def test_frame_simulator_matches_live_reference(case):
     assert d.max() <= 1 and float((d > 0).mean()) <= 1e-4
 
 
-@pytest.mark.parametrize("workload,mode,kind,count", [
-    ("plain_320x256_f32_1pol", 1, "intensity", 1), ("plain_320x256_f32_1pol", 0, "field", 3),
-    ("batched_640x512_u16_2pol", 1, "field", 1), ("batched_640x512_u16_2pol", 0, "intensity", 2)])
-def test_ref_calibration_matches_live_reference(workload, mode, kind, count):
+@pytest.mark.parametrize("workload,mode,kind,count,window", [
+    ("plain_320x256_f32_1pol", 1, "intensity", 1, None), ("plain_320x256_f32_1pol", 0, "field", 3, None),
+    ("batched_640x512_u16_2pol", 1, "field", 1, None), ("batched_640x512_u16_2pol", 0, "intensity", 2, None),
+    ("batched_640x512_u16_2pol", 0, "intensity", 1, 256), ("largefield_2048_u16_2pol", 0, "intensity", 1, None)])
+def test_ref_calibration_matches_live_reference(workload, mode, kind, count, window):
     """Reference-wave calibration (digHoloConfigSetRefCalibrationIntensity /
     Field): the oracle's reconstructed calibration planes against the
     reference's digHoloConfigGetRefCalibrationFields (relative L2 <= 1e-6),
     and the calibrated batch's fields and coefficients against the
     reference's (the usual bounds).  The calibration changes the
-    coefficients by 0.8-9 % here, well above the comparison's bounds."""
+    coefficients by 0.8-9 % here, well above the comparison's bounds.  The
+    reference runs in a child process (helpers.reference_calibrated)."""
     if not ref_lib.available():
         pytest.skip("reference build (oracle/_ref) not present")
-    from helpers import ref_calibration, ref_calibration_planes, set_ref_calibration
-    hol = make_case(workload, 2)
+    from helpers import ref_calibration, reference_calibrated
+    frames = 1 if workload.startswith("largefield") else 2
+    hol = make_case(workload, frames)
     cfg = config_for(hol, mode)
-    L = ref_lib.load()
-    h = L.digHoloCreate()
-    ref_lib.configure(L, h, cfg)
-    set_ref_calibration(L, h, cfg, kind, ref_calibration(cfg, kind, count))
-    r = ref_lib.run_batch(L, h, hol.frames)
-    rp = ref_calibration_planes(L, h)
+    if window:
+        cfg.fft_window = (window, window)
+    cfg.ref_cal = (O.ref_cal_store(intensity=ref_calibration(cfg, kind, count)) if kind == "intensity"
+                   else O.ref_cal_store(field=ref_calibration(cfg, kind, count)))
+    r = reference_calibrated(workload, frames, mode, kind, count, window)
     op = O.ref_cal_planes(cfg)
-    assert rp is not None and rp.shape == op.shape
-    assert rel_l2(op, rp) <= 1e-6
+    assert r["planes"].shape == op.shape
+    assert rel_l2(op, r["planes"]) <= 1e-6
     o = O.process_batch(hol.frames, cfg, quantised=True)
     _check(o, cfg, r["coefs"], r["R"], r["I"], r["scale"], r["x"], r["y"])
-    plain = O.process_batch(hol.frames, config_for(hol, mode), quantised=True)
-    assert rel_l2(plain["coefs"], o["coefs"]) > 3e-3
+    plain = config_for(hol, mode)
+    if window:
+        plain.fft_window = (window, window)
+    assert rel_l2(O.process_batch(hol.frames, plain, quantised=True)["coefs"], o["coefs"]) > 3e-3
