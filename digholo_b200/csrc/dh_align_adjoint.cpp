@@ -309,9 +309,15 @@ float objAutoAlignAdjoint(Object& o) {
         for (double v : gz) gn += v * v;
         gn = std::sqrt(gn);
         for (int i = 0; i < n; i++) Hi[(size_t)i * n + i] = 1.0 / std::max(gn, 1e-12);
-        // convergence in dB: half the plain search's termination tolerance
-        // (a sweep gaining at most terminationTol ends it, digHolo.cpp:12416, 12872)
-        const double tol = std::max(1e-4, (double)c.autoAlignTol * 0.5);
+        // convergence in dB, after the plain search's termination rule (a sweep
+        // gaining at most the tolerance ends a pass, digHolo.cpp:12416, 12872):
+        // the goal's pass at the user's tolerance (a tenth of it for MDL, whose
+        // objective bends where its extreme eigenvalues cross), the IL pass
+        // before an MDL goal at the reference's loose first-pass tolerance
+        // 0.1 + 10 tol (digHolo.cpp:12462)
+        const double userTol = (double)c.autoAlignTol;
+        const double tol = pass + 1 < passes ? std::max(1e-4, 0.1 + 10.0 * userTol)
+                           : std::max(1e-4, metric == METRIC_MDL ? 0.1 * userTol : userTol);
         const int maxIter = 80, maxRounds = 8;
         int quiet = 0, round = 0;
         bool firstUpdate = true, restarted = false;
