@@ -378,7 +378,12 @@ __host__ __device__ inline DftSmem dftSmem(int w, int h, int G) {
     return s;
 }
 
-__global__ void __launch_bounds__(DFT_THREADS) k_inverse_dft(DhInvParams p) {
+// GLOB: the two planes (window / field, and the row transforms / overlap
+// tables) of each unit in global scratch, at unit * dftSmem(...).tw bytes,
+// for fields whose planes exceed shared memory; the twiddles and the
+// reduction scratch stay in shared memory.
+template <bool GLOB>
+__global__ void __launch_bounds__(DFT_THREADS) k_inverse_dft_t(DhInvParams p, unsigned char* gplanes) {
     extern __shared__ __align__(16) unsigned char dsm[];
     const int unit = blockIdx.x;
     const int pol = unit % p.polCount;
@@ -388,11 +393,13 @@ __global__ void __launch_bounds__(DFT_THREADS) k_inverse_dft(DhInvParams p) {
     const int ld = nx + 1;
     const int G = p.maxMG > 0 ? p.maxMG : 0;
     const DftSmem L = dftSmem(nx, ny, G);
-    float2* fld = reinterpret_cast<float2*>(dsm + L.win);    // window, then the field [ny][ld]
-    float2* tmp = reinterpret_cast<float2*>(dsm + L.tmp);    // row transforms [ny][ld]; later the overlap tables
-    float2* twx = reinterpret_cast<float2*>(dsm + L.tw);     // exp(+2 pi i j / nx)
-    float2* twy = twx + nx;                                  // exp(+2 pi i j / ny)
-    Stat6* scratch = reinterpret_cast<Stat6*>(dsm + L.scratch);
+    unsigned char* pl = GLOB ? gplanes + (size_t)unit * L.tw : dsm;
+    const size_t shOff = GLOB ? L.tw : 0;                    // shared memory holds only the twiddles and scratch
+    float2* fld = reinterpret_cast<float2*>(pl + L.win);     // window, then the field [ny][ld]
+    float2* tmp = reinterpret_cast<float2*>(pl + L.tmp);     // row transforms [ny][ld]; later the overlap tables
+    float2* twx = reinterpret_cast<float2*>(dsm + (L.tw - shOff));        // exp(+2 pi i j / nx)
+    float2* twy = twx + nx;                                                // exp(+2 pi i j / ny)
+    Stat6* scratch = reinterpret_cast<Stat6*>(dsm + (L.scratch - shOff));
     const float2* win = p.window + (size_t)unit * npix;
     for (int e = threadIdx.x; e < npix; e += blockDim.x) {
         const int j = e / nx, c = e - j * nx;
@@ -730,10 +737,35 @@ cudaError_t dh_launch_inverse_dft(const DhInvParams& p, cudaStream_t s) {
     if (!p.lowres || p.w < 16 || p.h < 16 || p.w % 16 || p.h % 16) return cudaErrorNotSupported;
     const size_t smem = dh_inverse_dft_smem_bytes(p.w, p.h, p.maxMG);
     if (smem > 227 * 1024) return cudaErrorNotSupported;
-    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_dft), (int)smem);
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_dft_t<false>), (int)smem);
     if (e != cudaSuccess) return e;
     if (p.frameCount * p.polCount <= 0) return cudaSuccess;
-    k_inverse_dft<<<(unsigned)(p.frameCount * p.polCount), DFT_THREADS, smem, s>>>(p);
+    k_inverse_dft_t<false><<<(unsigned)(p.frameCount * p.polCount), DFT_THREADS, smem, s>>>(p, nullptr);
+    return cudaGetLastError();
+}
+
+// Scratch of the global-plane variant: each unit's two planes.
+size_t dh_inverse_dft_global_bytes(const DhInvParams& p) {
+    if (!p.lowres || p.w < 16 || p.h < 16 || p.w % 16 || p.h % 16) return 0;
+    return dftSmem(p.w, p.h, p.maxMG > 0 ? p.maxMG : 0).tw * (size_t)(p.frameCount * p.polCount);
+}
+
+// Low-resolution fields of any multiple of 16 whose planes exceed shared
+// memory: the same kernel with the planes in global scratch
+// (dh_inverse_dft_global_bytes); cudaErrorNotSupported outside its shapes.
+cudaError_t dh_launch_inverse_dft_global(const DhInvParams& p, void* scratch, size_t scratchBytes, cudaStream_t s) {
+    if (!p.lowres || p.w < 16 || p.h < 16 || p.w % 16 || p.h % 16 || p.w > 4096 || p.h > 4096)
+        return cudaErrorNotSupported;
+    if (p.frameCount * p.polCount <= 0) return cudaSuccess;
+    const DftSmem L = dftSmem(p.w, p.h, p.maxMG > 0 ? p.maxMG : 0);
+    if (!scratch || scratchBytes < L.tw * (size_t)(p.frameCount * p.polCount) ||
+        (reinterpret_cast<uintptr_t>(scratch) & 15))
+        return cudaErrorInvalidValue;
+    const size_t smem = L.total - L.tw;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_inverse_dft_t<true>), (int)smem);
+    if (e != cudaSuccess) return e;
+    k_inverse_dft_t<true><<<(unsigned)(p.frameCount * p.polCount), DFT_THREADS, smem, s>>>(
+        p, static_cast<unsigned char*>(scratch));
     return cudaGetLastError();
 }
 

@@ -44,6 +44,8 @@ size_t dh_inverse_dft_smem_bytes(int w, int h, int G);
 cudaError_t dh_launch_basis_transform(const float2* in, float2* out, const float2* T, int rows, int M, int din, int dout,
                                       cudaStream_t s);
 cudaError_t dh_launch_inverse_dft(const DhInvParams& p, cudaStream_t s);
+size_t dh_inverse_dft_global_bytes(const DhInvParams& p);
+cudaError_t dh_launch_inverse_dft_global(const DhInvParams& p, void* scratch, size_t scratchBytes, cudaStream_t s);
 cudaError_t dh_launch_basis(const DhBasisParams& p, cudaStream_t s);
 cudaError_t dh_launch_untranspose_u16(const unsigned short* in, unsigned short* out, int Nx, int Ny, int frames,
                                       cudaStream_t s);
@@ -313,16 +315,16 @@ static int checkSupported(Object& o) {
     // IFFT windows whose sides are multiples of 16 but not powers of two:
     // the full-plane forward, then at full resolution the band kernels (FFT
     // windows of at least 64 x 64), in low-resolution mode the DFT kernel
-    // (fields that fit its shared memory: up to 112 x 112 with 15 mode groups)
+    // (its planes in shared memory up to about 112 x 112 with 15 mode
+    // groups, in global scratch beyond)
     if (!isPow2(g.w) || !isPow2(g.h)) {
         const bool m16 = g.w % 16 == 0 && g.h % 16 == 0;
         const bool bands = o.cfg.resolutionIdx == 0 && g.W >= 64 && g.H >= 64 && m16;
-        const bool dft = o.cfg.resolutionIdx != 0 && m16 &&
-                         dh_inverse_dft_smem_bytes(g.w, g.h, o.cfg.maxMG) <= 227 * 1024;
+        const bool dft = o.cfg.resolutionIdx != 0 && m16;
         if (!bands && !dft)
             return fail(o, ERR_INVALIDDIMENSION,
                         "IFFT window sides that are not powers of two need an FFT window of at least 64 x 64 at full "
-                        "resolution, or a low-resolution field that fits the DFT kernel's shared memory, on this build");
+                        "resolution on this build");
     }
     if (o.avgCount < 1 || o.cfg.avgMode < 0 || o.cfg.avgMode > 2)
         return fail(o, ERR_INVALIDARGUMENT, "frame averaging: avgCount must be at least 1 and avgMode 0, 1 or 2");
@@ -872,6 +874,23 @@ static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) 
     return e;
 }
 
+// Low-resolution fields of the DFT kernel: its planes in shared memory where
+// they fit, else in global scratch (which grows here unless the caller may
+// not allocate).
+static cudaError_t launchDft(Object& o, const DhInvParams& ip, bool mayAlloc) {
+    cudaError_t e = dh_launch_inverse_dft(ip, o.stream);
+    if (e != cudaErrorNotSupported) return e;
+    cudaGetLastError();
+    const size_t need = dh_inverse_dft_global_bytes(ip);
+    if (need == 0) return cudaErrorNotSupported;
+    if (o.dBigScratch.bytes < need) {
+        if (!mayAlloc) return cudaErrorMemoryAllocation;
+        e = o.dBigScratch.ensure(need);
+        if (e != cudaSuccess) return e;
+    }
+    return dh_launch_inverse_dft_global(ip, o.dBigScratch.ptr, o.dBigScratch.bytes, o.stream);
+}
+
 // Inverse stage: the warp-per-unit kernels for 16/32-pixel low-resolution
 // fields; for full-resolution fields the pruned field kernel (fields up to
 // 128 x 128) followed by the overlap kernel, else the band kernels; else the
@@ -886,7 +905,7 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
         if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
         if (!ip.lowres) return launchBands(o, ip, mayAlloc);   // k_field_big: fields beyond one block
-        e = dh_launch_inverse_dft(ip, o.stream);
+        e = launchDft(o, ip, mayAlloc);
         if (e == cudaSuccess) { o.lastInverseKernel = 6; o.lastOverlapKernel = 1; }
         return e;
     }
@@ -927,7 +946,7 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
     if (e != cudaErrorNotSupported || !ip.lowres) return e;
     // low-resolution fields whose sides are not powers of two
     cudaGetLastError();
-    e = dh_launch_inverse_dft(ip, o.stream);
+    e = launchDft(o, ip, mayAlloc);
     if (e == cudaSuccess) { o.lastInverseKernel = 6; o.lastOverlapKernel = 1; }
     return e;
 }
@@ -1289,8 +1308,6 @@ static int processSweepLocked(Object& o, int syncCoefs) {
     const Config saved = o.cfg;
     const int B = std::max(1, saved.batchCount);
     if (!o.frames) return fail(o, ERR_NULLPOINTER, "frame buffer not set");
-    if (saved.avgCount > 1)
-        return fail(o, ERR_INVALIDARGUMENT, "multi-wavelength batches: frame averaging is not supported with them");
     if (B % L)
         return fail(o, ERR_INVALIDDIMENSION, "multi-wavelength batches: the batch count must be a multiple of the wavelength count");
     const int S = B / L;
@@ -1315,13 +1332,28 @@ static int processSweepLocked(Object& o, int syncCoefs) {
     o.batchCalCaller = &restore.cal;
     o.batchCalCallerCount = calCount;
     o.batchCalCallerPol = calPol;
-    DH_CUDA(o, o.dSweepFrames.ensure((size_t)S * frameBytes));
+    // frame averaging: each item's A frames, gathered per sub-batch in the
+    // sequential order (item j's k-th frame at j A + k); the reference's
+    // frame of input item b and average k (digHolo.cpp:8661-8672): b A + k
+    // (sequential), k B + b (interlaced), b + k L (sweeps)
+    const int A = std::max(1, saved.avgCount);
+    const int avgMode = saved.avgMode;
+    DH_CUDA(o, o.dSweepFrames.ensure((size_t)S * A * frameBytes));
     int P = 0, M = 0, Mout = 0, nx = 0, ny = 0, keep32 = o.keepField32, active = 0;
     for (int l = 0; l < L; l++) {
-        const char* src = static_cast<const char*>(framesIn) + (size_t)(inFast ? l : l * S) * frameBytes;
-        DH_CUDA(o, cudaMemcpy2DAsync(o.dSweepFrames.ptr, frameBytes, src, inFast ? (size_t)L * frameBytes : frameBytes,
-                                     frameBytes, S, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                     o.stream));
+        const size_t in0 = inFast ? (size_t)l : (size_t)l * S, inStep = inFast ? (size_t)L : 1;
+        for (int k = 0; k < A; k++) {
+            size_t first = in0, stride = inStep;   // in frames
+            if (A > 1) {
+                if (avgMode == 0) { first = in0 * A + k; stride = inStep * A; }
+                else if (avgMode == 1) first = (size_t)k * B + in0;
+                else first = in0 + (size_t)k * L;
+            }
+            const char* src = static_cast<const char*>(framesIn) + first * frameBytes;
+            DH_CUDA(o, cudaMemcpy2DAsync(static_cast<char*>(o.dSweepFrames.ptr) + (size_t)k * frameBytes,
+                                         (size_t)A * frameBytes, src, stride * frameBytes, frameBytes, S,
+                                         onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, o.stream));
+        }
         if (calEnabled && calCount > 0) {
             // the batch calibration of each frame's input index
             std::vector<float> c((size_t)calPol * S * 2);
@@ -1341,6 +1373,7 @@ static int processSweepLocked(Object& o, int syncCoefs) {
         o.framesTransposed = 0;
         o.cfg = saved;
         o.cfg.batchCount = S;
+        o.cfg.avgMode = 0;   // gathered in the sequential order above
         o.cfg.wavelengthCentre = lams[l];
         o.cfg.lambdaRange[0] = lams[0];
         o.cfg.lambdaRange[1] = lams[L - 1];

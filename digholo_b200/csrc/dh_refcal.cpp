@@ -86,17 +86,13 @@ bool objRefCalApplies(const Object& o) {
 }
 
 // The kernels that carry the calibration: k_inverse (power-of-two fields
-// whose shared memory fits), k_inverse_dft (low-resolution fields) and
-// k_field_big (full-resolution fields beyond one block).
+// whose shared memory fits), k_inverse_dft (low-resolution fields, planes in
+// shared memory or global scratch) and k_field_big (full-resolution fields
+// beyond one block): every shape this build processes.
 int objRefCalCheckShape(Object& o, const DhInvParams& ip) {
-    if (!ip.lowres) return ERR_SUCCESS;
-    const bool pow2 = ip.w == (1 << ip.logw) && ip.h == (1 << ip.logh);
-    if (pow2 && dh_inverse_smem_bytes(ip) <= 227 * 1024) return ERR_SUCCESS;
-    if (ip.w % 16 == 0 && ip.h % 16 == 0 && dh_inverse_dft_smem_bytes(ip.w, ip.h, ip.maxMG) <= 227 * 1024)
-        return ERR_SUCCESS;
-    return fail(o, ERR_INVALIDDIMENSION,
-                "reference-wave calibration: low-resolution fields above about 112 x 112 are not supported by this "
-                "build");
+    (void)o;
+    (void)ip;
+    return ERR_SUCCESS;
 }
 
 // Planes [pol][ny][nx] of calibration item `item` for the geometry in use.

@@ -341,8 +341,7 @@ complex64* digHoloProcessBatchWavelengthSweepArbitrary(int handleIdx, int* batch
  * enabled and of the frames' size, its reconstructed planes (c2c FFT of the
  * FFT windows, Fourier window at zero tilt, IFFT; digHolo.cpp:6729-6830,
  * 8253-8285) multiply every frame's IFFT output before the field analysis
- * (digHolo.cpp:8736-8758).  Low-resolution fields above about 112 x 112
- * fail with DIGHOLO_ERROR_INVALIDDIMENSION while a calibration applies.
+ * (digHolo.cpp:8736-8758).
  * GetRefCalibrationFields returns the planes [item][pol][height][width] for
  * the last batch's geometry, NULL before one. */
 int digHoloConfigSetRefCalibrationIntensity(int handleIdx, unsigned short* cal, int wavelengthCount, int width,

@@ -172,3 +172,31 @@ def test_non_power_of_two_ifft_window(lib, overlap, frame, window, carrier, wais
     assert rel_l2(g1["field"], o1["field"]) <= 5e-5
     assert rel_l2(g1["coefs"], o1["coefs"]) <= 5e-5
     lib.digHoloDestroy(h)
+
+
+def test_large_low_resolution_non_power_of_two(lib):
+    """A 144 x 144 low-resolution field (FFT windows of 512 pixels, carrier
+    (0.6, 0.48) of Nyquist): the DFT kernel's two planes exceed shared memory
+    and live in global scratch.  int16 fields within 2 LSB of the quantised
+    oracle, scales within 1e-5, fields and coefficients relative L2 <= 5e-5;
+    the same with a reference-wave calibration (planes through the same
+    kernel)."""
+    from helpers import ref_calibration, set_ref_calibration
+    hol = synth.generate(frame_count=3, frame_width=1280, frame_height=1024, pol_count=2, max_mg=9, waist=640e-6,
+                         snr_db=30, window=(512, 512), dtype="float32", seed=2999, carrier=(0.6, 0.48))
+    for calibrated in (False, True):
+        cfg = config_for(hol, 1)
+        h = lib.digHoloCreate()
+        api.configure(lib, h, cfg)
+        if calibrated:
+            set_ref_calibration(lib, h, cfg, "intensity", ref_calibration(cfg, "intensity"))
+        g = api.run_batch(lib, h, hol.frames)
+        assert g["coefs"] is not None, lib.digHoloB200GetLastError(h)
+        assert lib.digHoloB200GetInverseKernel(h) == 6
+        o = O.process_batch(hol.frames, cfg, quantised=True)
+        assert o["R"].shape[-2:] == (144, 144) and g["R"].shape == o["R"].shape
+        assert np.max(np.abs(g["scale"].T - o["scale"]) / o["scale"]) <= 1e-5
+        assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
+        assert rel_l2(g["field"], o["field"]) <= 5e-5
+        assert rel_l2(g["coefs"], o["coefs"]) <= 5e-5
+        lib.digHoloDestroy(h)

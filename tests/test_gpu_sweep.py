@@ -117,3 +117,38 @@ def test_single_wavelength_sweep_is_the_centre_wavelength(lib):
     o = O.process_batch(hol.frames, cfg, quantised=True)
     assert max(np.abs(g["R"].astype(int) - o["R"]).max(), np.abs(g["I"].astype(int) - o["I"]).max()) <= 2
     assert rel_l2(g["coefs"], o["coefs"]) <= 5e-5
+
+
+@pytest.mark.parametrize("avg_mode", [0, 1, 2])
+def test_sweep_with_frame_averaging_matches_reference(lib, avg_mode):
+    """Frame averaging within a multi-wavelength batch: each item's frames
+    are those of the reference's averaging modes (digHolo.cpp:8661-8672:
+    item b's k-th frame at b A + k, k B + b or b + k L), averaged with the
+    phase alignment and processed at the item's wavelength.  Against the
+    reference build on the same frames: int16 fields within 2 LSB, fields
+    and (unscaled 16-row) coefficients relative L2 <= 5e-5."""
+    if not ref_lib.available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    A, B = 2, 6
+    hol = make_case("batched_640x512_u16_2pol", A * B)
+    cfg = config_for(hol, 1)
+    lams = [1550e-9, 1575e-9, 1600e-9]
+    out = []
+    for L in (lib, ref_lib.load()):
+        h = L.digHoloCreate()
+        api.configure(L, h, cfg)
+        frames = np.ascontiguousarray(hol.frames)
+        assert api.set_batch_avg(L, h, frames, A, avg_mode) == 0
+        b, m, p = C.c_int(), C.c_int(), C.c_int()
+        arr = (C.c_float * 3)(*lams)
+        cp = L.digHoloProcessBatchWavelengthSweepArbitrary(h, C.byref(b), C.byref(m), C.byref(p), arr, 3)
+        assert cp, (L.digHoloB200GetLastError(h) if hasattr(L, "digHoloB200GetLastError") else "")
+        out.append(api.read_outputs(L, h, B, cp, m.value, p.value, True))
+    g, r = out
+    dmax = max(np.abs(g["R"].astype(int) - r["R"]).max(), np.abs(g["I"].astype(int) - r["I"]).max())
+    gc = O.reference_unscaled_16(g["coefs"].astype(np.complex128), cfg, {"x": g["x"], "y": g["y"], "scale": g["scale"].T})
+    print("avg mode %d: int16 max diff %d, fields %.2e, coefs %.2e" % (avg_mode, dmax, rel_l2(g["field"], r["field"]),
+                                                                      rel_l2(gc, r["coefs"])))
+    assert dmax <= 2
+    assert rel_l2(g["field"], r["field"]) <= 5e-5
+    assert rel_l2(gc, r["coefs"]) <= 5e-5
