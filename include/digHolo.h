@@ -213,11 +213,16 @@ int digHoloConfigGetAutoAlignMode(int handleIdx);
 int digHoloConfigSetAutoAlignGoalIdx(int handleIdx, int goalIdx);
 /* replaces digHolo.h:1136 */
 int digHoloConfigGetAutoAlignGoalIdx(int handleIdx);
-/* replaces digHolo.h:1152.  Runs the reference's TWEAK coordinate search
- * (tilt, beam centre, defocus, waist; optional Fourier-window radius rule)
- * with every evaluation on the GPU and returns the final value of the goal
- * metric in dB.  FULL and ESTIMATE start the same search from the current
- * settings: the snap estimate from the full Fourier plane is not built. */
+/* replaces digHolo.h:1152.  The reference's AutoAlign with every
+ * evaluation on the GPU, returning the final value of the goal metric in dB:
+ * FULL (the default) and ESTIMATE first run the parameter estimate from the
+ * full Fourier planes (tilt by the DCT correlation of the batch-summed
+ * Fourier intensity, window radius, waist from the effective areas, beam
+ * centre from the camera-plane centre of mass, defocus by the focus search;
+ * digHolo.cpp:11517-11970, 11181-11499); FULL and TWEAK then run the
+ * coordinate search (tilt, beam centre, defocus, waist; optional
+ * Fourier-window radius rule), with a second pass on the goal when the goal
+ * is not IL. */
 float digHoloAutoAlign(int handleIdx);
 /* replaces digHolo.h:1163 */
 float digHoloAutoAlignGetMetric(int handleIdx, int metricIdx);
