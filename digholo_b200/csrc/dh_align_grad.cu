@@ -146,6 +146,128 @@ __global__ void __launch_bounds__(256) k_align_grad(DhGradParams p) {
     }
 }
 
+// The same contraction for G <= GM, register-tiled: each thread owns one
+// column x of the field, with Hx_m(x) and dHx_m/dw(x) for m < GM in
+// registers, and walks the rows y = ty, ty + YS, ...; the row sums U[m][y]
+// and Uw[m][y] sit in shared memory as one float4 per (m, y), which a warp
+// (32 columns of one row) reads as a broadcast.  Rows G <= m < GM of the
+// table are zero, so the unrolled mode loop needs no bound check.  Per pixel
+// and mode: one shared load and six FMAs (the generic kernel above reads
+// four values per pixel and mode).
+template <int GM>
+__global__ void __launch_bounds__(256) k_align_grad_reg(DhGradParams p) {
+    extern __shared__ float4 sg4[];
+    const int unit = blockIdx.x;
+    const int P = p.polCount, G = p.G, M = p.M, nx = p.nx, ny = p.ny;
+    const int pol = unit % P, frame = unit / P;
+    const int GE = G + 2;
+    float4* UU = sg4;                                                 // [GM][ny] {U, Uw}
+    float2* cc = reinterpret_cast<float2*>(UU + (size_t)GM * ny);     // [M] conj(c)
+    float* dhy = reinterpret_cast<float*>(cc + M);                    // [G][ny] Hy'_n
+    float* red = dhy + (size_t)G * ny;                                // [8 warps][7]
+    const float* hxp = p.hx + (size_t)pol * GE * nx;
+    const float* hyp = p.hy + (size_t)pol * GE * ny;
+    const float w0 = p.waist[pol];
+    const float ladder = -1.0f / (2.0f * w0);
+    const int tid = threadIdx.x;
+
+    float spow = 0.f;
+    for (int mode = tid; mode < M; mode += blockDim.x) {
+        const size_t ci = (size_t)frame * P * M + (size_t)pol * M + mode;
+        const float2 c = p.coefs[ci];
+        cc[mode] = p.weights ? p.weights[ci] : make_float2(c.x, -c.y);
+        spow = fmaf(c.x, c.x, fmaf(c.y, c.y, spow));
+    }
+    for (int e = tid; e < G * ny; e += blockDim.x) {
+        const int n = e / ny, y = e - n * ny;
+        float v = 0.f;
+        if (n >= 2) v += sqrtf((float)(n * (n - 1))) * hyp[(n - 2) * ny + y];
+        v -= sqrtf((float)((n + 1) * (n + 2))) * hyp[(n + 2) * ny + y];
+        dhy[e] = v * ladder;
+    }
+    __syncthreads();
+    for (int e = tid; e < GM * ny; e += blockDim.x) {
+        const int m = e / ny, y = e - m * ny;
+        float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int n = 0; m + n < G; n++) {
+            const int g = m + n;
+            const float2 c = cc[g * (g + 1) / 2 + n];
+            const float hv = hyp[n * ny + y], dv = dhy[n * ny + y];
+            u.x = fmaf(c.x, hv, u.x); u.y = fmaf(c.y, hv, u.y);
+            u.z = fmaf(c.x, dv, u.z); u.w = fmaf(c.y, dv, u.w);
+        }
+        UU[e] = u;
+    }
+    __syncthreads();
+
+    const size_t base = (size_t)unit * nx * ny;
+    const float2* Vp = p.V + base;
+    const float2* Vxp = p.Vx + base;
+    const float2* Vyp = p.Vy + base;
+    const int XT = nx < 256 ? nx : 256;   // nx is a power of two
+    const int YS = 256 / XT;
+    const int tx = tid % XT, ty = tid / XT;
+    const float bx = p.bcx[pol], by = p.bcy[pol];
+    // sums: Im(Abar V) (x + bcx), Im(Abar V) (y + bcy), Im(Abar V) (x^2 + y^2),
+    // Re(Abar Vx), Re(Abar Vy), Re(Abar_w V), Im(Abar V)
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f, si = 0.f;
+    for (int x0 = 0; x0 < nx; x0 += XT) {
+        const int x = x0 + tx;
+        float hr[GM], dr[GM];
+#pragma unroll
+        for (int m = 0; m < GM; m++) {
+            hr[m] = 0.f;
+            dr[m] = 0.f;
+            if (m < G) {
+                hr[m] = hxp[m * nx + x];
+                float v = 0.f;
+                if (m >= 2) v += sqrtf((float)(m * (m - 1))) * hxp[(m - 2) * nx + x];
+                v -= sqrtf((float)((m + 1) * (m + 2))) * hxp[(m + 2) * nx + x];
+                dr[m] = v * ladder;
+            }
+        }
+        const float xv = p.xAxis[x];
+        for (int y = ty; y < ny; y += YS) {
+            const size_t e = (size_t)y * nx + x;
+            const float2 v = Vp[e], vx = Vxp[e], vy = Vyp[e];
+            float2 a = make_float2(0.f, 0.f), aw = make_float2(0.f, 0.f);
+            const float4* Uy = UU + y;
+#pragma unroll
+            for (int m = 0; m < GM; m++) {
+                const float4 u = Uy[m * ny];
+                a.x = fmaf(hr[m], u.x, a.x);
+                a.y = fmaf(hr[m], u.y, a.y);
+                aw.x = fmaf(dr[m], u.x, fmaf(hr[m], u.z, aw.x));
+                aw.y = fmaf(dr[m], u.y, fmaf(hr[m], u.w, aw.y));
+            }
+            const float imAV = a.x * v.y + a.y * v.x;
+            const float yv = p.yAxis[y];
+            s0 = fmaf(imAV, xv + bx, s0);
+            s1 = fmaf(imAV, yv + by, s1);
+            s2 = fmaf(imAV, xv * xv + yv * yv, s2);
+            s3 += a.x * vx.x - a.y * vx.y;
+            s4 += a.x * vy.x - a.y * vy.y;
+            s5 += aw.x * v.x - aw.y * v.y;
+            si += imAV;
+        }
+    }
+    const float k0u = p.k0u[pol];
+    // Re(Abar V i) = -Im(Abar V); the beam-centre tangents carry -Im(Abar V) k0 u t
+    float s[7] = {-k0u * s0, -k0u * s1, -p.piOverLambda * s2, s3 - k0u * p.tiltX[pol] * si,
+                  s4 - k0u * p.tiltY[pol] * si, s5, spow};
+#pragma unroll
+    for (int k = 0; k < 7; k++)
+        for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+    if ((tid & 31) == 0)
+        for (int k = 0; k < 7; k++) red[(tid >> 5) * 7 + k] = s[k];
+    __syncthreads();
+    if (tid < 7) {
+        float t = 0.f;
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 7 + tid];
+        p.out[(size_t)unit * 7 + tid] = t;
+    }
+}
+
 // Weights of an eigenvalue's derivative.  For an eigenpair (lambda, u) of
 // the Gram matrix of the block A (rows = modes of pol0 [and pol1], columns
 // = frames; column-major A[b rows + j]), d lambda = 2 Re sum_jb w_jb dA_jb
@@ -207,7 +329,22 @@ cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const floa
     return cudaGetLastError();
 }
 
+template <int GM>
+static cudaError_t launchAlignGradReg(const DhGradParams& p, size_t smem, cudaStream_t s) {
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_align_grad_reg<GM>), (int)smem);
+    if (e != cudaSuccess) return e;
+    k_align_grad_reg<GM><<<(unsigned)(p.frameCount * p.polCount), 256, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s) {
+    const bool pow2 = p.nx > 0 && (p.nx & (p.nx - 1)) == 0;
+    if (pow2 && p.G <= 32) {
+        const int GM = p.G <= 16 ? 16 : 32;
+        const size_t smemReg = sizeof(float4) * (size_t)GM * p.ny + sizeof(float2) * (size_t)p.M +
+                               sizeof(float) * ((size_t)p.G * p.ny + 8 * 7);
+        if (smemReg <= 200 * 1024) return GM == 16 ? launchAlignGradReg<16>(p, smemReg, s) : launchAlignGradReg<32>(p, smemReg, s);
+    }
     const size_t smem = sizeof(float2) * ((size_t)p.M + 2 * (size_t)p.G * p.ny) + sizeof(float) * ((size_t)p.G * (p.nx + p.ny) + 8 * 7);
     if (smem > 200 * 1024) return cudaErrorNotSupported;
     cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_align_grad), (int)smem);

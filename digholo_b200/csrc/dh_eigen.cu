@@ -201,18 +201,32 @@ __global__ void __launch_bounds__(NT, 1) k_heev(HeevArgs a) {
                 const int i = k + 1 + ri;
                 const double2 vpi = havePrev ? vp[i] : make_double2(0.0, 0.0);
                 const double2 xpi = havePrev ? xp[i] : make_double2(0.0, 0.0);
-                for (int j = k + 1 + g; j < n; j += groups) {
-                    double2 e = A[(size_t)j * n + i];
-                    if (havePrev) {
-                        const double2 u1 = cmulD(vpi, make_double2(xp[j].x, -xp[j].y));
-                        const double2 u2 = cmulD(xpi, make_double2(vp[j].x, -vp[j].y));
-                        e.x -= u1.x + u2.x;
-                        e.y -= u1.y + u2.y;
-                        A[(size_t)j * n + i] = e;
+                // CB columns per pass, their loads issued before any store:
+                // the trailing block lives in L2, and one load in flight per
+                // thread would leave each pass waiting on L2 latency CB times
+                constexpr int CB = 4;
+                for (int j0 = k + 1 + g; j0 < n; j0 += CB * groups) {
+                    double2 e[CB];
+#pragma unroll
+                    for (int q = 0; q < CB; q++) {
+                        const int j = j0 + q * groups;
+                        e[q] = j < n ? A[(size_t)j * n + i] : make_double2(0.0, 0.0);
                     }
-                    const double2 p = cmulD(e, vk[j]);
-                    acc.x += p.x;
-                    acc.y += p.y;
+#pragma unroll
+                    for (int q = 0; q < CB; q++) {
+                        const int j = j0 + q * groups;
+                        if (j >= n) break;
+                        if (havePrev) {
+                            const double2 u1 = cmulD(vpi, make_double2(xp[j].x, -xp[j].y));
+                            const double2 u2 = cmulD(xpi, make_double2(vp[j].x, -vp[j].y));
+                            e[q].x -= u1.x + u2.x;
+                            e[q].y -= u1.y + u2.y;
+                            A[(size_t)j * n + i] = e[q];
+                        }
+                        const double2 p = cmulD(e[q], vk[j]);
+                        acc.x += p.x;
+                        acc.y += p.y;
+                    }
                 }
             }
             part[t] = acc;
@@ -277,14 +291,29 @@ __global__ void __launch_bounds__(NT, 1) k_heev(HeevArgs a) {
     lo -= tol;
     hi += tol;
     double* W = a.W + (size_t)blockIdx.x * n;
-    for (int m = t; m < n; m += NT) {
-        double l = lo, h = hi;
-        for (int it = 0; it < 200 && h - l > tol; it++) {
-            const double mid = 0.5 * (l + h);
-            if (sturmCount(D, E2, n, mid, pivmin) > m) h = mid;
-            else l = mid;
+    {
+        // quadrisection, four lanes per eigenvalue: lanes 0-2 of a group
+        // count at the interval's quarter points, the group keeps the
+        // quarter holding eigenvalue m (two bits per Sturm count instead of
+        // one).  Every lane of a group holds the same interval, so the
+        // group's trip count is uniform.
+        const int lane = t & 31, q4 = t & 3;
+        const unsigned gmask = 0xFu << (lane & ~3);
+        for (int m = t >> 2; m < n; m += NT / 4) {
+            double l = lo, h = hi;
+            for (int it = 0; it < 200 && h - l > tol; it++) {
+                const double step = 0.25 * (h - l);
+                const double x = l + step * (double)(q4 + 1);
+                const bool above = q4 < 3 && sturmCount(D, E2, n, x, pivmin) > m;
+                const unsigned bits = (__ballot_sync(gmask, above) >> (lane & ~3)) & 7u;
+                const int f = bits ? __ffs(bits) - 1 : 3;   // first quarter point above eigenvalue m
+                const double nh = f < 3 ? l + step * (double)(f + 1) : h;
+                const double nl = f > 0 ? l + step * (double)f : l;
+                l = nl;
+                h = nh;
+            }
+            if (q4 == 0) W[m] = 0.5 * (l + h);
         }
-        W[m] = 0.5 * (l + h);
     }
     if (!a.vecs) return;
     __syncthreads();

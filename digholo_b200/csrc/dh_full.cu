@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(H * W / 32, 1) k_field_full(DhInvParams p) {
             sI[y * SLD + x] = roundSat16(scale * vi);
         }
     }
+    if (!OVL && p.fieldsOnly) return;   // block-uniform
     __syncthreads();
     // coalesced copy of the int16 planes
     constexpr int CH = W / 8;   // 16-byte chunks per row
@@ -380,7 +381,9 @@ __global__ void __launch_bounds__(256) k_overlap_f32(DhInvParams p, int nx, int 
             }
         }
         float* Tp = T + ((size_t)plane * ny + y) * (G + 1);
-        for (int m = 0; m < G; m++) Tp[m] = acc[m];
+#pragma unroll
+        for (int m = 0; m < GMAX; m++)
+            if (m < G) Tp[m] = acc[m];   // unrolled: acc stays in registers
     }
     __syncthreads();
     const int S = p.statsStride;
@@ -467,11 +470,12 @@ cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fus
 }
 
 // FP32 overlap of the int16 fields [unit][ny][nx]; cudaErrorNotSupported
-// outside its shapes (2 ny <= 256 threads, nx a multiple of 8, G <= 32).
+// outside its shapes (2 ny <= 256 threads, nx a multiple of 8, G <= 64).
 cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStream_t s) {
     if (p.maxMG <= 0 || !p.coefs) return cudaSuccess;
     if (2 * ny > 256 || nx % 8 != 0 || ny < 16) return cudaErrorNotSupported;
     if (p.maxMG <= 16) return launchOverlapF32<16>(p, nx, ny, s);
     if (p.maxMG <= 32) return launchOverlapF32<32>(p, nx, ny, s);
+    if (p.maxMG <= 64) return launchOverlapF32<64>(p, nx, ny, s);
     return cudaErrorNotSupported;
 }

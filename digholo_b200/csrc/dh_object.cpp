@@ -1855,6 +1855,7 @@ int objInverseAux(Object& o, const float2* window, int frameCount, float2* field
     ip.fieldR = scratchR;
     ip.fieldI = scratchI;
     ip.stats = scratchStats;
+    ip.fieldsOnly = 1;
     const int k = o.lastInverseKernel, ov = o.lastOverlapKernel;
     DH_CUDA(o, launchInverse(o, ip));
     o.lastInverseKernel = k;

@@ -82,6 +82,9 @@ struct DhInvParams {
     // optional reference-wave calibration [pol][ny][nx]: multiplies the IFFT
     // output before the statistics and the tilt removal (block-per-unit kernels)
     const float2* refCal;
+    // 1: only field32 is wanted (the adjoint's derivative fields); kernels
+    // that honour it skip the int16 planes (fieldR, fieldI are then unused)
+    int fieldsOnly;
 };
 
 // Separable DFT stage of the calibration planes: out[u][a][b] =

@@ -103,6 +103,22 @@ def test_fields_and_coefs_vs_oracle(lib, workload, frames, mode, kernel):
 
 
 @pytest.mark.parametrize("workload,frames,mode", CASES)
+def test_many_mode_groups_vs_oracle(lib, workload, frames, mode):
+    """maxMG 34 (595 modes per polarisation): beyond the 32 mode groups of
+    the tensor-core overlaps, full-resolution fields take the FP32 overlap's
+    64-group tile; the same tolerances as above."""
+    hol = make_case(workload, frames)
+    cfg = config_for(hol, mode, max_mg=34)
+    g = _run(lib, hol, cfg)
+    o = O.process_batch(hol.frames, cfg, quantised=True)
+    assert g["coefs"].shape == o["coefs"].shape
+    dR = np.abs(g["R"].astype(int) - o["R"])
+    dI = np.abs(g["I"].astype(int) - o["I"])
+    assert max(dR.max(), dI.max()) <= 2
+    assert rel_l2(g["coefs"], o["coefs"]) <= 5e-5
+
+
+@pytest.mark.parametrize("workload,frames,mode", CASES)
 def test_vs_reference_build(lib, workload, frames, mode):
     if not ref_lib.available():
         pytest.skip("reference build (oracle/_ref) not present")
