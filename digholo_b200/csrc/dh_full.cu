@@ -408,6 +408,88 @@ __global__ void __launch_bounds__(256) k_overlap_f32(DhInvParams p, int nx, int 
     }
 }
 
+// The same overlap for any number of mode groups: the x-modes in chunks of
+// OVC (T[y][m] of one chunk in shared memory, the int16 field re-read per
+// chunk), then c_mn for the modes whose m falls in the chunk, with Hy read
+// from global memory.  Per chunk the sums run in k_overlap_f32's order, so
+// the coefficients equal its bit for bit.  The fallback beyond the
+// register-tiled overlaps (more than 64 mode groups, or more than 32 on
+// fields taller than 128 rows).  One block of 256 threads per (frame,
+// polarisation).
+constexpr int OVC = 16;
+__global__ void __launch_bounds__(256) k_overlap_f32_chunked(DhInvParams p, int nx, int ny) {
+    extern __shared__ float smo[];
+    const int G = p.maxMG, M = p.modeCount;
+    const int unit = blockIdx.x;
+    const int P = p.polCount;
+    const int pol = unit % P, frame = unit / P;
+    const int tid = threadIdx.x;
+    float* hx = smo;                                   // [nx][OVC]
+    float* T = hx + (size_t)nx * OVC;                  // [2][ny][OVC + 1]
+    const short* gx = p.hgX + (size_t)pol * G * nx;
+    const short* gy = p.hgY + (size_t)pol * G * ny;
+    const size_t npix = (size_t)nx * ny;
+    const int S = p.statsStride;
+    const float fieldScale = 1.0f / p.stats[3 * P * S + pol * S + frame];
+    const float* sxp = p.hgScaleX + pol * G;
+    const float* syp = p.hgScaleY + pol * G;
+    for (int m0 = 0; m0 < G; m0 += OVC) {
+        __syncthreads();   // the previous chunk's tables are consumed
+        for (int e = tid; e < nx * OVC; e += blockDim.x) {
+            const int x = e / OVC, m = m0 + e % OVC;
+            hx[e] = m < G ? (float)gx[(size_t)m * nx + x] : 0.f;
+        }
+        __syncthreads();
+        for (int r = tid; r < 2 * ny; r += blockDim.x) {
+            const int plane = r / ny, y = r - plane * ny;
+            const short* row = (plane ? p.fieldI : p.fieldR) + (size_t)unit * npix + (size_t)y * nx;
+            float acc[OVC];
+#pragma unroll
+            for (int m = 0; m < OVC; m++) acc[m] = 0.f;
+            for (int x0 = 0; x0 < nx; x0 += 8) {
+                const uint4 raw = __ldg(reinterpret_cast<const uint4*>(row + x0));
+                const unsigned wv[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    const float v = (float)(short)((wv[t >> 1] >> (16 * (t & 1))) & 0xFFFF);
+                    const float4* hv = reinterpret_cast<const float4*>(hx + (x0 + t) * OVC);
+#pragma unroll
+                    for (int m4 = 0; m4 < OVC / 4; m4++) {
+                        const float4 h = hv[m4];
+                        acc[4 * m4 + 0] = fmaf(v, h.x, acc[4 * m4 + 0]);
+                        acc[4 * m4 + 1] = fmaf(v, h.y, acc[4 * m4 + 1]);
+                        acc[4 * m4 + 2] = fmaf(v, h.z, acc[4 * m4 + 2]);
+                        acc[4 * m4 + 3] = fmaf(v, h.w, acc[4 * m4 + 3]);
+                    }
+                }
+            }
+            float* Tp = T + (size_t)r * (OVC + 1);
+#pragma unroll
+            for (int m = 0; m < OVC; m++) Tp[m] = acc[m];
+        }
+        __syncthreads();
+        for (int mode = tid; mode < M; mode += blockDim.x) {
+            int g = (int)((sqrtf(8.0f * mode + 1.0f) - 1.0f) * 0.5f);
+            while ((g + 1) * (g + 2) / 2 <= mode) g++;
+            while (g * (g + 1) / 2 > mode) g--;
+            const int n = mode - g * (g + 1) / 2;
+            const int m = g - n;
+            if (m < m0 || m >= m0 + OVC) continue;
+            const short* hn = gy + (size_t)n * ny;
+            const float* t0 = T + (m - m0);
+            const float* t1 = T + (size_t)ny * (OVC + 1) + (m - m0);
+            float cr = 0.f, ci = 0.f;
+            for (int y = 0; y < ny; y++) {
+                const float hv = (float)hn[y];
+                cr = fmaf(hv, t0[(size_t)y * (OVC + 1)], cr);
+                ci = fmaf(hv, t1[(size_t)y * (OVC + 1)], ci);
+            }
+            const float ms = (float)((double)sxp[m] * (double)syp[n] * (double)fieldScale);
+            p.coefs[(size_t)frame * P * M + (size_t)pol * M + mode] = make_float2(cr * ms, ci * ms);
+        }
+    }
+}
+
 namespace {
 
 template <int W, int H, int WW, bool OVL, int GN>
@@ -478,4 +560,17 @@ cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStre
     if (p.maxMG <= 32) return launchOverlapF32<32>(p, nx, ny, s);
     if (p.maxMG <= 64) return launchOverlapF32<64>(p, nx, ny, s);
     return cudaErrorNotSupported;
+}
+
+// The chunked FP32 overlap (any maxMG); cudaErrorNotSupported when nx is not
+// a multiple of 8 or the chunk tables exceed shared memory.
+cudaError_t dh_launch_overlap_f32_chunked(const DhInvParams& p, int nx, int ny, cudaStream_t s) {
+    if (p.maxMG <= 0 || !p.coefs) return cudaSuccess;
+    if (nx % 8 != 0 || nx < 8 || ny < 1) return cudaErrorNotSupported;
+    const size_t smem = sizeof(float) * ((size_t)nx * OVC + 2 * (size_t)ny * (OVC + 1));
+    if (smem > 227 * 1024) return cudaErrorNotSupported;
+    cudaError_t e = setSmemOnce(reinterpret_cast<const void*>(k_overlap_f32_chunked), (int)smem);
+    if (e != cudaSuccess) return e;
+    k_overlap_f32_chunked<<<(unsigned)(p.frameCount * p.polCount), 256, smem, s>>>(p, nx, ny);
+    return cudaGetLastError();
 }

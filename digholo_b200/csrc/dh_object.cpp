@@ -35,6 +35,7 @@ int dh_forward_i8_npad(int w);
 cudaError_t dh_launch_inverse_lo(const DhInvParams& p, cudaStream_t s);
 cudaError_t dh_launch_field_full(const DhInvParams& p, int withOverlap, int* fused, cudaStream_t s);
 cudaError_t dh_launch_overlap_f32(const DhInvParams& p, int nx, int ny, cudaStream_t s);
+cudaError_t dh_launch_overlap_f32_chunked(const DhInvParams& p, int nx, int ny, cudaStream_t s);
 size_t dh_field_big_scratch_bytes(const DhInvParams& p, int overlapKind);
 cudaError_t dh_launch_field_big(const DhInvParams& p, int overlapKind, void* scratch, size_t scratchBytes,
                                 int* overlapUsed, cudaStream_t s);
@@ -839,6 +840,19 @@ static cudaError_t launchForward(Object& o, const DhFwdParams& fp, bool mayAlloc
 // Full-resolution fields by bands of 64 rows (any field size); its scratch
 // grows here unless the caller may not allocate.
 static cudaError_t launchBands(Object& o, const DhInvParams& ip, bool mayAlloc) {
+    if (ip.maxMG > 32 && ip.coefs) {
+        // more mode groups than the band kernels' overlap tiles hold: the
+        // fields first, then the chunked FP32 overlap of the int16 fields
+        DhInvParams fi = ip;
+        fi.maxMG = 0;
+        fi.modeCount = 0;
+        fi.coefs = nullptr;
+        cudaError_t e = launchBands(o, fi, mayAlloc);
+        if (e != cudaSuccess) return e;
+        e = dh_launch_overlap_f32_chunked(ip, o.geo.nx, o.geo.ny, o.stream);
+        if (e == cudaSuccess) o.lastOverlapKernel = 1;
+        return e;
+    }
     // 512-wide fields with IFFT windows up to 64 x 64: 64-point sub-transforms
     // and the exact integer overlap (dh_band64.cu)
     const size_t need64 = dh_field_band64_scratch_bytes(ip, o.overlapKernel);
@@ -926,6 +940,10 @@ static cudaError_t launchInverse(Object& o, const DhInvParams& ip, bool mayAlloc
         if (e == cudaSuccess) {
             const int nx = 1 << ip.logW, ny = 1 << ip.logH;
             e = dh_launch_overlap_f32(ip, nx, ny, o.stream);
+            if (e == cudaErrorNotSupported) {   // beyond its register tiles
+                cudaGetLastError();
+                e = dh_launch_overlap_f32_chunked(ip, nx, ny, o.stream);
+            }
             if (e == cudaSuccess) { o.lastInverseKernel = 3; o.lastOverlapKernel = 1; return e; }
             if (e != cudaErrorNotSupported) return e;
             cudaGetLastError();

@@ -41,9 +41,12 @@ def _per_group(c, co, G):
     return np.array(per)
 
 
-@pytest.mark.parametrize("mode,overlap", [(1, 0), (0, 0), (0, 1)])
-def test_largefield_vs_oracle_and_reference(lib, hol, mode, overlap):
-    cfg = config_for(hol, mode)
+@pytest.mark.parametrize("mode,overlap,max_mg", [(1, 0, None), (0, 0, None), (0, 1, None), (0, 0, 34)])
+def test_largefield_vs_oracle_and_reference(lib, hol, mode, overlap, max_mg):
+    """maxMG 34 (595 modes) exceeds the band kernels' 32-group overlap
+    tiles: the band pass writes the fields, the chunked FP32 overlap reads
+    them."""
+    cfg = config_for(hol, mode, max_mg=max_mg)
     h = lib.digHoloCreate()
     api.configure(lib, h, cfg)
     assert lib.digHoloB200SetOverlapKernel(h, overlap) == 0
@@ -51,7 +54,9 @@ def test_largefield_vs_oracle_and_reference(lib, hol, mode, overlap):
     assert g["coefs"] is not None, lib.digHoloB200GetLastError(h)
     kern, used = lib.digHoloB200GetInverseKernel(h), lib.digHoloB200GetOverlapKernel(h)
     lib.digHoloDestroy(h)
-    if mode == 0:
+    if mode == 0 and max_mg:
+        assert used == 1   # FP32 (chunked)
+    elif mode == 0:
         # tensor cores: the 64-point band kernel with the exact integer overlap
         assert (kern, used) == ((7, 3) if overlap == 0 else (4, 1))
     o = O.process_batch(hol.frames, cfg, quantised=True)
