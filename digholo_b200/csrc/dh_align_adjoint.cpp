@@ -36,15 +36,28 @@ enum { G_TX = 0, G_TY = 1, G_DEF = 2, G_CX = 3, G_CY = 4, G_WAIST = 5 };
 int objAlignGradient(Object& o, float* grad12, float* ilOut) { return objAlignGradientMetric(o, 0, grad12, ilOut); }
 
 int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
+    return objAlignEvaluate(o, metric, ALIGN_EVAL_FULL, grad12, ilOut);
+}
+
+// stage ALIGN_EVAL_FULL: the batch, the metric and its gradient;
+// ALIGN_EVAL_VALUE: the batch and the metric only (grad12 untouched);
+// ALIGN_EVAL_GRADIENT: the gradient (and the metric) of the batch state a
+// preceding ALIGN_EVAL_VALUE call left on the device, for the same metric.
+// The metric is the same number in every stage.
+int objAlignEvaluate(Object& o, int metric, int stage, float* grad12, float* ilOut) {
     Config& c = o.cfg;
     if (c.maxMG <= 0) return fail(o, ERR_ERROR, "adjoint AutoAlign needs a modal basis (maxMG > 0)");
     using Clock = std::chrono::steady_clock;
     const auto t0 = Clock::now();
-    const int keep = o.keepField32;
-    o.keepField32 = 1;
-    int r = objProcessForAlign(o);
-    o.keepField32 = keep;
-    if (r) return r;
+    int r = ERR_SUCCESS;
+    if (stage != ALIGN_EVAL_GRADIENT) {
+        const int keep = o.keepField32;
+        o.keepField32 = 1;
+        r = objProcessForAlign(o);
+        o.keepField32 = keep;
+        if (r) return r;
+    }
+    const bool valueOnly = stage == ALIGN_EVAL_VALUE;
     const auto t1 = Clock::now();
     const Geometry& g = o.geo;
     if ((g.w & (g.w - 1)) || (g.h & (g.h - 1)))
@@ -56,52 +69,59 @@ int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
     const int w = g.w, h = g.h, W = g.W, H = g.H;
     const size_t npix = (size_t)g.nx * g.ny;
 
-    // beam-centre phase derivatives of the window: i kx per column, i ky per row
-    std::vector<float> tab((size_t)P * (w + h));
-    for (int p = 0; p < P; p++) {
-        const int sx0 = g.SX[p] - W / 2;
-        for (int cc = 0; cc < w; cc++) tab[(size_t)p * w + cc] = g.kx[sx0 + cc];
-        for (int j = 0; j < h; j++) {
-            int row = (j + g.SY[p] + H / 2) % H;
-            if (row < 0) row += H;
-            tab[(size_t)P * w + (size_t)p * h + j] = g.ky[row];
-        }
-    }
-    DH_CUDA(o, o.dGradTab.ensure(tab.size() * sizeof(float)));
-    DH_CUDA(o, cudaMemcpyAsync(o.dGradTab.ptr, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
-    const size_t winElems = (size_t)units * w * h;
-    DH_CUDA(o, o.dGradW.ensure(2 * winElems * sizeof(float2)));
-    float2* Wx = o.dGradW.as<float2>();
-    float2* Wy = Wx + winElems;
-    DH_CUDA(o, dh_launch_window_deriv(o.dWindow.as<float2>(), o.dGradTab.as<float>(), o.dGradTab.as<float>() + (size_t)P * w,
-                                      w, h, P, units, Wx, Wy, o.stream));
-    // fields of the derivative windows
-    DH_CUDA(o, o.dGradV.ensure(2 * (size_t)units * npix * sizeof(float2)));
-    float2* Vx = o.dGradV.as<float2>();
-    float2* Vy = Vx + (size_t)units * npix;
-    // both derivative windows in one launch: a batch of 2B frames (Wy follows Wx, Vy follows Vx)
-    DH_CUDA(o, o.dGradScratch.ensure(4 * (size_t)units * npix * sizeof(short) + (size_t)7 * P * (2 * B + 1) * sizeof(float)));
-    short* sR = o.dGradScratch.as<short>();
-    short* sI = sR + 2 * (size_t)units * npix;
-    float* sStats = reinterpret_cast<float*>(sI + 2 * (size_t)units * npix);
-    r = objInverseAux(o, Wx, 2 * B, Vx, sR, sI, sStats);
-    if (r) return r;
-    const auto t2 = Clock::now();
-    // float modes up to order G + 1 (the waist derivative reaches m + 2)
-    const int GE = G + 2;
-    const int L = std::max(g.nx, g.ny);
-    DH_CUDA(o, o.dGradBasis.ensure((size_t)P * GE * (g.nx + g.ny) * sizeof(float) + (size_t)GE * L * sizeof(short) +
-                                   (size_t)GE * sizeof(float)));
-    float* hx = o.dGradBasis.as<float>();
-    float* hy = hx + (size_t)P * GE * g.nx;
-    float* scale = hy + (size_t)P * GE * g.ny;
-    short* s16 = reinterpret_cast<short*>(scale + GE);
-    r = objBasisFloat(o, GE, hx, hy, s16, scale);
-    if (r) return r;
-    const auto t3 = Clock::now();
-
     DhGradParams gp;
     memset(&gp, 0, sizeof(gp));
+    float2* Vx = nullptr;
+    float2* Vy = nullptr;
+    float* hx = nullptr;
+    float* hy = nullptr;
+    auto t2 = t1, t3 = t1;
+    if (!valueOnly) {
+        // beam-centre phase derivatives of the window: i kx per column, i ky per row
+        std::vector<float> tab((size_t)P * (w + h));
+        for (int p = 0; p < P; p++) {
+            const int sx0 = g.SX[p] - W / 2;
+            for (int cc = 0; cc < w; cc++) tab[(size_t)p * w + cc] = g.kx[sx0 + cc];
+            for (int j = 0; j < h; j++) {
+                int row = (j + g.SY[p] + H / 2) % H;
+                if (row < 0) row += H;
+                tab[(size_t)P * w + (size_t)p * h + j] = g.ky[row];
+            }
+        }
+        DH_CUDA(o, o.dGradTab.ensure(tab.size() * sizeof(float)));
+        DH_CUDA(o, cudaMemcpyAsync(o.dGradTab.ptr, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, o.stream));
+        const size_t winElems = (size_t)units * w * h;
+        DH_CUDA(o, o.dGradW.ensure(2 * winElems * sizeof(float2)));
+        float2* Wx = o.dGradW.as<float2>();
+        float2* Wy = Wx + winElems;
+        DH_CUDA(o, dh_launch_window_deriv(o.dWindow.as<float2>(), o.dGradTab.as<float>(), o.dGradTab.as<float>() + (size_t)P * w,
+                                          w, h, P, units, Wx, Wy, o.stream));
+        // fields of the derivative windows
+        DH_CUDA(o, o.dGradV.ensure(2 * (size_t)units * npix * sizeof(float2)));
+        Vx = o.dGradV.as<float2>();
+        Vy = Vx + (size_t)units * npix;
+        // both derivative windows in one launch: a batch of 2B frames (Wy follows Wx, Vy follows Vx)
+        DH_CUDA(o, o.dGradScratch.ensure(4 * (size_t)units * npix * sizeof(short) + (size_t)7 * P * (2 * B + 1) * sizeof(float)));
+        short* sR = o.dGradScratch.as<short>();
+        short* sI = sR + 2 * (size_t)units * npix;
+        float* sStats = reinterpret_cast<float*>(sI + 2 * (size_t)units * npix);
+        r = objInverseAux(o, Wx, 2 * B, Vx, sR, sI, sStats);
+        if (r) return r;
+        t2 = Clock::now();
+        // float modes up to order G + 1 (the waist derivative reaches m + 2)
+        const int GE = G + 2;
+        const int L = std::max(g.nx, g.ny);
+        DH_CUDA(o, o.dGradBasis.ensure((size_t)P * GE * (g.nx + g.ny) * sizeof(float) + (size_t)GE * L * sizeof(short) +
+                                       (size_t)GE * sizeof(float)));
+        hx = o.dGradBasis.as<float>();
+        hy = hx + (size_t)P * GE * g.nx;
+        float* scale = hy + (size_t)P * GE * g.ny;
+        short* s16 = reinterpret_cast<short*>(scale + GE);
+        r = objBasisFloat(o, GE, hx, hy, s16, scale);
+        if (r) return r;
+        t3 = Clock::now();
+    }
+
     gp.V = o.dField32.as<float2>();
     gp.Vx = Vx;
     gp.Vy = Vy;
@@ -130,14 +150,19 @@ int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
     gp.piOverLambda = (float)(PI_DA / c.wavelengthCentre);
     double mdlDb = 0.0;
     if (metric == 1) {
-        DH_CUDA(o, o.dGradWeights.ensure((size_t)units * M * sizeof(float2)));
-        r = objMdlWeights(o, o.dGradWeights.as<float2>(), &mdlDb);
-        if (r) return fail(o, r, "MDL gradient: eigenvalues of the batch Gram matrix");
+        // the weights of a value stage serve the gradient stage that follows it
+        if (stage != ALIGN_EVAL_GRADIENT) {
+            DH_CUDA(o, o.dGradWeights.ensure((size_t)units * M * sizeof(float2)));
+            r = objMdlWeights(o, o.dGradWeights.as<float2>(), &mdlDb);
+            if (r) return fail(o, r, "MDL gradient: eigenvalues of the batch Gram matrix");
+            o.alignMdlDb = mdlDb;
+        }
+        mdlDb = o.alignMdlDb;
         gp.weights = o.dGradWeights.as<float2>();
     }
     DH_CUDA(o, o.dGradOut.ensure((size_t)units * 7 * sizeof(float)));
     gp.out = o.dGradOut.as<float>();
-    DH_CUDA(o, dh_launch_align_grad(gp, o.stream));
+    DH_CUDA(o, valueOnly ? dh_launch_align_power(gp, o.stream) : dh_launch_align_grad(gp, o.stream));
     if (!o.hGradOut.ensure((size_t)units * 7 * sizeof(float))) return fail(o, ERR_MEMORYALLOCATION, "gradient host buffer");
     const float* part = o.hGradOut.as<float>();
     DH_CUDA(o, cudaMemcpyAsync(o.hGradOut.ptr, gp.out, (size_t)units * 7 * sizeof(float), cudaMemcpyDeviceToHost, o.stream));
@@ -159,6 +184,8 @@ int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
     }
     // d IL / d theta = 10 / ln 10 * dS / S, dS = 2 Re sum conj(c) dc;
     // d MDL / d theta = 20 / ln 10 * Re sum W dc
+    if (ilOut) *ilOut = metric == 1 ? (float)mdlDb : (float)(10.0 * std::log10(S > 0 ? S : 1e-300));
+    if (valueOnly) return ERR_SUCCESS;
     const double f = metric == 1 ? 20.0 / std::log(10.0) : ((S > 0) ? 20.0 / std::log(10.0) / S : 0.0);
     for (int p = 0; p < 2; p++)
         for (int k = 0; k < 6; k++) grad12[p * 6 + k] = p < P ? (float)(f * acc[p][k]) : 0.f;
@@ -168,7 +195,6 @@ int objAlignGradientMetric(Object& o, int metric, float* grad12, float* ilOut) {
         if (c.polLockDefocus) tie(G_DEF);
         if (c.polLockBasisWaist) tie(G_WAIST);
     }
-    if (ilOut) *ilOut = metric == 1 ? (float)mdlDb : (float)(10.0 * std::log10(S > 0 ? S : 1e-300));
     return ERR_SUCCESS;
 }
 
@@ -199,6 +225,27 @@ void setParam(Config& c, const Param& q, double v) {
         case G_CY: c.beamCentreY[q.pol] = (float)v; break;
         default: c.waist[q.pol] = (float)v; break;
     }
+}
+
+// Whether re-selecting the Fourier window with snapshot b gives the batch
+// path of snapshot a: the same window geometry and bit-identical window
+// factors.  The snapshot's tilt enters the path only through the window's
+// position and its mask, and every kernel evaluates the mask with the float32
+// steps of windowFactors, so equal factors mean an identical evaluation.
+bool sameSelection(const Object& o, const Config& a, const Config& b) {
+    Geometry ga, gb;
+    fftWindowGeometry(o.fftSnap, o.polCount, ga);
+    ifftWindowGeometry(a, o.polCount, ga);
+    fftWindowGeometry(o.fftSnap, o.polCount, gb);
+    ifftWindowGeometry(b, o.polCount, gb);
+    if (ga.W != gb.W || ga.H != gb.H || ga.w != gb.w || ga.h != gb.h || ga.nx != gb.nx || ga.ny != gb.ny) return false;
+    for (int p = 0; p < POLMAX; p++)
+        if (ga.cx[p] != gb.cx[p] || ga.cy[p] != gb.cy[p] || ga.SX[p] != gb.SX[p] || ga.SY[p] != gb.SY[p]) return false;
+    if (ga.kx != gb.kx || ga.ky != gb.ky || ga.x != gb.x || ga.y != gb.y) return false;
+    std::vector<float> fa, fb;
+    windowFactors(a, o.cfg, ga, o.polCount, fa);
+    windowFactors(b, o.cfg, gb, o.polCount, fb);
+    return fa.size() == fb.size() && (fa.empty() || memcmp(fa.data(), fb.data(), fa.size() * sizeof(float)) == 0);
 }
 
 }  // namespace
@@ -262,11 +309,18 @@ float objAutoAlignAdjoint(Object& o) {
     // f = -metric (IL, then MDL for goal MDL; minimised) and its gradient in
     // step coordinates
     int metric = 0;
+    // the configuration and window snapshot of the last evaluation (its
+    // coefficients are the ones on the device)
+    Config lastCfg = c, lastSnap = c;
+    bool haveLast = false;
     auto evalF = [&](const std::vector<double>& zz, double& f, std::vector<double>& gg) -> int {
         apply(zz);
         float g12[12], il = 0.f;
         const int r = objAlignGradientMetric(o, metric, g12, &il);
         o.alignEvaluations++;
+        haveLast = r == ERR_SUCCESS;
+        lastCfg = c;
+        lastSnap = o.ifftSnap;
         if (r) return r;
         f = -(double)il;
         for (int i = 0; i < n; i++) gg[i] = -(double)g12[prm[i].pol * 6 + prm[i].kind] * prm[i].scale;
@@ -276,6 +330,28 @@ float objAutoAlignAdjoint(Object& o) {
             for (int i = 0; i < n; i++) fprintf(stderr, " %.4f", zz[i]);
             fprintf(stderr, "\n");
         }
+        return ERR_SUCCESS;
+    };
+    // a line-search trial: the batch and the metric only; its gradient
+    // (evalG, on the batch state the trial left on the device) only once
+    // the trial is accepted
+    auto evalV = [&](const std::vector<double>& zz, double& f) -> int {
+        apply(zz);
+        float il = 0.f;
+        const int r = objAlignEvaluate(o, metric, ALIGN_EVAL_VALUE, nullptr, &il);
+        o.alignEvaluations++;
+        haveLast = r == ERR_SUCCESS;
+        lastCfg = c;
+        lastSnap = o.ifftSnap;
+        if (r) return r;
+        f = -(double)il;
+        return ERR_SUCCESS;
+    };
+    auto evalG = [&](std::vector<double>& gg) -> int {
+        float g12[12], il = 0.f;
+        const int r = objAlignEvaluate(o, metric, ALIGN_EVAL_GRADIENT, g12, &il);
+        if (r) return r;
+        for (int i = 0; i < n; i++) gg[i] = -(double)g12[prm[i].pol * 6 + prm[i].kind] * prm[i].scale;
         return ERR_SUCCESS;
     };
     // The FFT window stays where the first evaluation put it; the Fourier
@@ -351,8 +427,12 @@ float objAutoAlignAdjoint(Object& o) {
                         boxed = true;
                     }
                 }
-                if (evalF(zt, ft, gt)) return -FLT_MAX;
-                if (ft <= f + 1e-4 * t * slope) { accepted = true; break; }
+                if (evalV(zt, ft)) return -FLT_MAX;
+                if (ft <= f + 1e-4 * t * slope) {
+                    if (evalG(gt)) return -FLT_MAX;
+                    accepted = true;
+                    break;
+                }
                 // minimiser of the quadratic through f, slope and ft, kept in [0.1 t, 0.5 t]
                 const double tq = -slope * t * t / (2.0 * (ft - f - slope * t));
                 t = std::min(0.5 * t, std::max(0.1 * t, tq));
@@ -423,10 +503,12 @@ float objAutoAlignAdjoint(Object& o) {
                 const double gain = lastRoundEnd - f;
                 if (++round >= maxRounds || (round > 1 && gain < tol && !boxed)) break;
                 lastRoundEnd = f;
-                const float ap = o.ifftSnap.apertureSize;
-                o.ifftSnap = c;
-                o.ifftSnap.apertureSize = ap;
-                if (evalF(z, f, gz)) return -FLT_MAX;
+                Config snap = c;
+                snap.apertureSize = o.ifftSnap.apertureSize;
+                // a selection that comes out as the held one re-evaluates nothing
+                const bool same = sameSelection(o, o.ifftSnap, snap);
+                o.ifftSnap = snap;
+                if (!same && evalF(z, f, gz)) return -FLT_MAX;
                 if (f < fBest) { fBest = f; zBest = z; }
                 zc = z;
                 quiet = 0;
@@ -435,11 +517,13 @@ float objAutoAlignAdjoint(Object& o) {
         // the reached point with its windows re-selected, against the best
         // re-selected point of the pass
         {
-            const float ap = o.ifftSnap.apertureSize;
-            o.ifftSnap = c;
-            o.ifftSnap.apertureSize = ap;
-            double fz = 0.0;
-            if (evalF(z, fz, gz)) return -FLT_MAX;
+            apply(z);
+            Config snap = c;
+            snap.apertureSize = o.ifftSnap.apertureSize;
+            const bool same = sameSelection(o, o.ifftSnap, snap);
+            o.ifftSnap = snap;
+            double fz = f;
+            if (!same && evalF(z, fz, gz)) return -FLT_MAX;
             if (fz > fBest) z = zBest;
         }
         apply(z);
@@ -449,12 +533,18 @@ float objAutoAlignAdjoint(Object& o) {
     // search found it (the reference's search moves the FFT window only at
     // the next digHoloFFT either)
     {
-        const float ap = o.ifftSnap.apertureSize;
-        o.ifftSnap = c;
-        o.ifftSnap.apertureSize = ap;
+        Config snap = c;
+        snap.apertureSize = o.ifftSnap.apertureSize;
+        o.ifftSnap = snap;
     }
-    if (objProcessForAlign(o)) return -FLT_MAX;
-    o.alignEvaluations++;
+    // the last evaluation already ran this configuration with these windows
+    // (its coefficients are on the device) unless the search returned to an
+    // earlier point
+    const bool current = haveLast && memcmp(&lastCfg, &c, sizeof(Config)) == 0 && sameSelection(o, lastSnap, o.ifftSnap);
+    if (!current) {
+        if (objProcessForAlign(o)) return -FLT_MAX;
+        o.alignEvaluations++;
+    }
     objCalcMetrics(o);
     objCoefsToHost(o);
     return o.autoAlignMetrics[c.autoAlignGoalIdx][0];

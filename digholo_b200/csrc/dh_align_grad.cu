@@ -268,6 +268,38 @@ __global__ void __launch_bounds__(256) k_align_grad_reg(DhGradParams p) {
     }
 }
 
+// The power term of the gradient kernels alone (their first loop and their
+// block reduction, in the same order).
+__global__ void __launch_bounds__(256) k_align_power(DhGradParams p) {
+    __shared__ float red[8 * 7];
+    const int unit = blockIdx.x;
+    const int P = p.polCount, M = p.M;
+    const int pol = unit % P, frame = unit / P;
+    const int tid = threadIdx.x;
+    float spow = 0.f;
+    for (int mode = tid; mode < M; mode += blockDim.x) {
+        const float2 c = p.coefs[(size_t)frame * P * M + (size_t)pol * M + mode];
+        spow = fmaf(c.x, c.x, fmaf(c.y, c.y, spow));
+    }
+    float s[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, spow};
+#pragma unroll
+    for (int k = 0; k < 7; k++)
+        for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+    if ((tid & 31) == 0)
+        for (int k = 0; k < 7; k++) red[(tid >> 5) * 7 + k] = s[k];
+    __syncthreads();
+    if (tid < 7) {
+        float t = 0.f;
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) t += red[wv * 7 + tid];
+        p.out[(size_t)unit * 7 + tid] = t;
+    }
+}
+
+cudaError_t dh_launch_align_power(const DhGradParams& p, cudaStream_t s) {
+    k_align_power<<<(unsigned)(p.frameCount * p.polCount), 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
 // Weights of an eigenvalue's derivative.  For an eigenpair (lambda, u) of
 // the Gram matrix of the block A (rows = modes of pol0 [and pol1], columns
 // = frames; column-major A[b rows + j]), d lambda = 2 Re sum_jb w_jb dA_jb

@@ -24,6 +24,11 @@ struct DhGradParams {
     const float2* weights;
 };
 
+// Per field only the captured power sum |c|^2 into out[unit * 7 + 6] (the
+// other six entries zero), summed in the order of the gradient kernels, so
+// the value equals theirs bit for bit: the value of a line-search trial.
+cudaError_t dh_launch_align_power(const DhGradParams& p, cudaStream_t s);
+
 cudaError_t dh_launch_window_deriv(const float2* W, const float* kxw, const float* kyw, int w, int h, int polCount, int units,
                                    float2* Wx, float2* Wy, cudaStream_t s);
 cudaError_t dh_launch_align_grad(const DhGradParams& p, cudaStream_t s);

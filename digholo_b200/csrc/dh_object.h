@@ -191,6 +191,7 @@ struct Object {
     DevBuf dTransRaw, dTransFrames;     // transposed uint16 input: raw host copy, converted frames
     // adjoint AutoAlign scratch: derivative windows and fields, float bases, partial sums
     DevBuf dGradW, dGradV, dGradScratch, dGradBasis, dGradOut, dGradTab, dGradWeights;
+    double alignMdlDb = 0.0;   // MDL of the batch state the MDL gradient weights belong to
     HostBuf hGradOut;
     DhEigen* eigen = nullptr;
     int alignEvaluations = 0;
@@ -309,6 +310,8 @@ int objInverseAux(Object& o, const float2* window, int frameCount, float2* field
 int objBasisFloat(Object& o, int modes, float* outX, float* outY, short* scratch16, float* scratchScale);
 int objAlignGradient(Object& o, float* grad12, float* ilOut);
 int objAlignGradientMetric(Object& o, int metric, float* grad12, float* valueOut);
+enum { ALIGN_EVAL_FULL = 0, ALIGN_EVAL_VALUE = 1, ALIGN_EVAL_GRADIENT = 2 };
+int objAlignEvaluate(Object& o, int metric, int stage, float* grad12, float* valueOut);
 int objMdlWeights(Object& o, float2* W, double* mdlDb);
 float objAutoAlignAdjoint(Object& o);
 int objCalcMetrics(Object& o);

@@ -108,9 +108,8 @@ def test_many_mode_groups_vs_oracle(lib, workload, frames, mode, max_mg):
     """maxMG 34 (595 modes per polarisation) and 70 (2485): beyond the 32
     mode groups of the tensor-core overlaps, full-resolution fields take the
     FP32 overlap's 64-group register tile, and beyond 64 groups its chunked
-    form; the same tolerances as above."""
-    if max_mg > 64 and mode == 1:
-        pytest.skip("low-resolution fields: the mode tables of 70 groups exceed the inverse kernels' shared memory")
+    form (low-resolution fields: the inverse kernels' own overlap, whose
+    mode tables are sized by maxMG); the same tolerances as above."""
     hol = make_case(workload, frames)
     cfg = config_for(hol, mode, max_mg=max_mg)
     g = _run(lib, hol, cfg)

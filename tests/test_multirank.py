@@ -63,10 +63,12 @@ def test_two_rank_sharding_matches_single_process():
             sys.path.insert(0, p)
     import digholo_oracle as O
     from helpers import config_for, make_case
-    manager = mp.get_context("spawn").Manager()
-    out = manager.dict()
-    port = _free_port()
-    mp.start_processes(_worker, args=(2, port, out), nprocs=2, start_method="spawn", join=True)
+    # the manager process is shut down when the block ends, not at interpreter exit
+    with mp.get_context("spawn").Manager() as manager:
+        shared = manager.dict()
+        port = _free_port()
+        mp.start_processes(_worker, args=(2, port, shared), nprocs=2, start_method="spawn", join=True)
+        out = dict(shared)
     hol = make_case("plain_320x256_f32_1pol", 4)
     cfg = config_for(hol, 0)
     full = O.process_batch(hol.frames, cfg, quantised=True)["coefs"]
