@@ -20,8 +20,7 @@ struct DhEigen;
 cudaError_t dh_launch_gather_block(const float2* src0, const float2* src1, int pol0, int pol1, int polCount, int M,
                                    int rows, int batch, float2* A, cudaStream_t s);
 cudaError_t dh_launch_gram(const float2* A, int rows, int batch, int rowsGram, void* G, cudaStream_t s);
-int dh_eigen_values(DhEigen& e, void* G, int n, double* W, cudaStream_t s);
-int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs, cudaStream_t s);
+int dh_eigen_extremes(DhEigen& e, void* G, int n, int count, double* W, void* vecs, double* trace, cudaStream_t s);
 DhEigen* dh_eigen_create();
 cudaError_t dh_launch_mdl_weights(const float2* A, int rows, int batch, int rowsGram, const double2* u, double alpha,
                                   int pol0, int pol1, int polCount, int M, float2* W, cudaStream_t s);
@@ -45,26 +44,30 @@ struct Block {
     int pol0, pol1, rows;
 };
 
-// Singular values squared (descending) of a block via the eigenvalues of its
-// smaller Gram matrix.
-static int blockSingular2(Object& o, const Block& blk, std::vector<double>& s2) {
+// The smallest and largest squared singular value of a block and the sum of
+// all of them (its squared Frobenius norm), via the extreme eigenvalues and
+// the trace of its smaller Gram matrix.
+static int blockSingular2(Object& o, const Block& blk, double& s2min, double& s2max, double& s2sum) {
     const int B = o.batchCount, M = objOutputModes(o), P = o.polCount;
     const size_t aBytes = (size_t)blk.rows * B * sizeof(float2);
     const int rowsGram = blk.rows <= B;
     const int n = rowsGram ? blk.rows : B;
     if (o.dMetricA.ensure(aBytes) != cudaSuccess) return ERR_MEMORYALLOCATION;
-    if (o.dMetricG.ensure((size_t)n * n * 16 + (size_t)n * sizeof(double)) != cudaSuccess) return ERR_MEMORYALLOCATION;
+    if (o.dMetricG.ensure((size_t)n * n * 16 + (size_t)(n + 1) * sizeof(double)) != cudaSuccess) return ERR_MEMORYALLOCATION;
     if (dh_launch_gather_block(blk.src0, blk.src1, blk.pol0, blk.pol1, P, M, blk.rows, B, o.dMetricA.as<float2>(),
                                o.stream) != cudaSuccess) return ERR_ERROR;
     if (dh_launch_gram(o.dMetricA.as<float2>(), blk.rows, B, rowsGram, o.dMetricG.ptr, o.stream) != cudaSuccess) return ERR_ERROR;
-    double* W = reinterpret_cast<double*>(o.dMetricG.as<char>() + (size_t)n * n * 16);
+    double* W = reinterpret_cast<double*>(o.dMetricG.as<char>() + (size_t)n * n * 16);   // [n] + trace
     if (!o.eigen) o.eigen = dh_eigen_create();
-    if (dh_eigen_values(*o.eigen, o.dMetricG.ptr, n, W, o.stream)) return ERR_ERROR;
-    s2.resize(n);
-    if (cudaMemcpyAsync(s2.data(), W, n * sizeof(double), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess) return ERR_ERROR;
+    if (dh_eigen_extremes(*o.eigen, o.dMetricG.ptr, n, 1, W, nullptr, W + n, o.stream)) return ERR_ERROR;
+    double h[3];
+    if (cudaMemcpyAsync(&h[0], W, sizeof(double), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess ||
+        cudaMemcpyAsync(&h[1], W + n - 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess)
+        return ERR_ERROR;
     if (cudaStreamSynchronize(o.stream) != cudaSuccess) return ERR_ERROR;
-    for (double& v : s2) v = v < 0 ? 0 : v;
-    std::sort(s2.begin(), s2.end(), [](double a, double b) { return a > b; });
+    s2min = h[0] < 0 ? 0 : h[0];
+    s2max = h[1] < 0 ? 0 : h[1];
+    s2sum = h[2] < 0 ? 0 : h[2];
     return ERR_SUCCESS;
 }
 
@@ -103,7 +106,8 @@ int objMdlWeights(Object& o, float2* W, double* mdlDb) {
         if (dh_launch_gather_block(bl.src0, bl.src1, bl.pol0, bl.pol1, P, M, rows, B, A, o.stream) != cudaSuccess) return ERR_ERROR;
         void* Gk = gb + (size_t)k * n * n * 16;
         if (dh_launch_gram(A, rows, B, rowsGram, Gk, o.stream) != cudaSuccess) return ERR_ERROR;
-        if (dh_eigen_solve(*o.eigen, Gk, n, 1, dW + (size_t)k * n, dV + (size_t)k * 2 * n, o.stream)) return ERR_ERROR;
+        if (dh_eigen_extremes(*o.eigen, Gk, n, 1, dW + (size_t)k * n, dV + (size_t)k * 2 * n, nullptr, o.stream))
+            return ERR_ERROR;
     }
     if (cudaMemcpyAsync(ev.data(), dW, ev.size() * sizeof(double), cudaMemcpyDeviceToHost, o.stream) != cudaSuccess)
         return ERR_ERROR;
@@ -270,23 +274,20 @@ int powerMeter(Object& o, float* out, int polIdx, int polsIndependent, const flo
         totalSNR = totalSignal / totalNoise;
     }
     if (doMDL) {  // digHolo.cpp:11012-11062
+        // IL: the mean squared singular value (the trace of the Gram matrix
+        // over its size); MDL: the smallest over the largest, over all blocks
         const int minDim = std::min(svdM, svdN);
-        std::vector<double> all;
+        double sum = 0.0;
+        float maxS = -FLT_MAX, minS = FLT_MAX;
         for (int k = 0; k < svdCount; k++) {
-            std::vector<double> s2;
-            const int r = blockSingular2(o, blocks[k], s2);
+            double lo2 = 0.0, hi2 = 0.0, sum2 = 0.0;
+            const int r = blockSingular2(o, blocks[k], lo2, hi2, sum2);
             if (r) return r;
-            s2.resize(minDim);
-            all.insert(all.end(), s2.begin(), s2.end());
+            sum += sum2;
+            minS = std::min(minS, (float)std::sqrt(lo2));
+            maxS = std::max(maxS, (float)std::sqrt(hi2));
         }
-        float ilv = 0.f, maxS = -FLT_MAX, minS = FLT_MAX;
-        for (double v : all) {
-            const float s = (float)std::sqrt(v);
-            ilv += s * s;
-            minS = std::min(minS, s);
-            maxS = std::max(maxS, s);
-        }
-        il = ilv / (float)all.size();
+        il = (float)(sum / ((double)svdCount * minDim));
         mdl = (minS * minS) / (maxS * maxS);
     } else if (doIL) {  // insertionLoss256, digHolo.cpp:3105-3143
         il = 0.f;

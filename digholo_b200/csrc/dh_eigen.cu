@@ -111,6 +111,8 @@ struct HeevArgs {
     double2* vecs;      // [count][2][n]: eigenvectors of the smallest and largest eigenvalue, or null
     double2* tau;       // [count][n] work
     double* lu;         // [count][2][6 n] work (inverse iteration)
+    int extremes;       // 1: only W[0] and W[n-1] (the other entries untouched)
+    double* trace;      // [count] sum of the eigenvalues (the tridiagonal's diagonal sum), or null
 };
 
 __global__ void __launch_bounds__(NT, 1) k_heev(HeevArgs a) {
@@ -291,7 +293,33 @@ __global__ void __launch_bounds__(NT, 1) k_heev(HeevArgs a) {
     lo -= tol;
     hi += tol;
     double* W = a.W + (size_t)blockIdx.x * n;
-    {
+    if (a.trace && t == 0) {
+        double tr = 0.0;
+        for (int i = 0; i < n; i++) tr += D[i];
+        a.trace[blockIdx.x] = tr;
+    }
+    if (a.extremes) {
+        // the smallest and the largest eigenvalue only (what MDL and its
+        // gradient use): one warp each, 31 count points per pass, five bits
+        // of the interval per Sturm count; every lane holds the same interval
+        const int warp = t >> 5, lane = t & 31;
+        if (warp < 2) {
+            const int m = warp == 0 ? 0 : n - 1;
+            double l = lo, h = hi;
+            for (int it = 0; it < 100 && h - l > tol; it++) {
+                const double step = (h - l) * (1.0 / 32.0);
+                const double x = l + step * (double)(lane + 1);
+                const bool above = lane < 31 && sturmCount(D, E2, n, x, pivmin) > m;
+                const unsigned bits = __ballot_sync(0xffffffffu, above) & 0x7fffffffu;
+                const int f = bits ? __ffs(bits) - 1 : 31;   // first count point above eigenvalue m
+                const double nh = f < 31 ? l + step * (double)(f + 1) : h;
+                const double nl = f > 0 ? l + step * (double)f : l;
+                l = nl;
+                h = nh;
+            }
+            if (lane == 0) W[m] = 0.5 * (l + h);
+        }
+    } else {
         // quadrisection, four lanes per eigenvalue: lanes 0-2 of a group
         // count at the interval's quarter points, the group keeps the
         // quarter holding eigenvalue m (two bits per Sturm count instead of
@@ -446,7 +474,8 @@ int dh_eigen_max_n() { return 2048; }
 // eigenvalues ascending into W[count][n]; with vecs non-null the unit
 // eigenvectors of the smallest and the largest eigenvalue into
 // vecs[count][2][n] (complex double).
-int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs, cudaStream_t s) {
+int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs, cudaStream_t s, int extremes = 0,
+                   double* trace = nullptr) {
     if (n < 1 || n > dh_eigen_max_n() || count < 1) return 2;
     const size_t need = (size_t)count * n * sizeof(double2) + (size_t)count * 2 * 6 * n * sizeof(double);
     if (ensureWork(e, need)) return 3;
@@ -457,6 +486,8 @@ int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs,
     a.vecs = static_cast<double2*>(vecs);
     a.tau = static_cast<double2*>(e.work);
     a.lu = reinterpret_cast<double*>(static_cast<char*>(e.work) + (size_t)count * n * sizeof(double2));
+    a.extremes = extremes;
+    a.trace = trace;
     const size_t smem = heevSmem(n);
     static size_t smemSet = 0;
     if (smem > 48 * 1024 && smem > smemSet) {
@@ -469,6 +500,12 @@ int dh_eigen_solve(DhEigen& e, void* G, int n, int count, double* W, void* vecs,
 
 int dh_eigen_values(DhEigen& e, void* G, int n, double* W, cudaStream_t s) {
     return dh_eigen_solve(e, G, n, 1, W, nullptr, s);
+}
+
+// The smallest and largest eigenvalue (W[0], W[n-1]; the other entries of W
+// untouched), with vecs non-null their eigenvectors, and the eigenvalue sum.
+int dh_eigen_extremes(DhEigen& e, void* G, int n, int count, double* W, void* vecs, double* trace, cudaStream_t s) {
+    return dh_eigen_solve(e, G, n, count, W, vecs, s, 1, trace);
 }
 
 DhEigen* dh_eigen_create() { return new DhEigen(); }
