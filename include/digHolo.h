@@ -472,7 +472,8 @@ int digHoloB200GetForwardKernel(int handleIdx);
  * kernel up to 128 x 128 pixels, bands of 64 rows beyond; else one block),
  * 1 one block per frame and polarisation, 2 full-resolution bands only (the
  * batch fails where they do not apply: low resolution, fields under 64 x 64,
- * windows under 16 pixels, maxMG > 32), 3 as 0 but fused into the
+ * windows under 16 pixels; beyond 32 mode groups the bands write the fields
+ * and the chunked FP32 overlap follows), 3 as 0 but fused into the
  * tensor-core forward kernel where it applies (uint16 frames, 16 x 16
  * low-resolution fields: one launch per batch). */
 int digHoloB200SetInverseKernel(int handleIdx, int kernel);
@@ -481,7 +482,9 @@ int digHoloB200SetInverseKernel(int handleIdx, int kernel);
  * field kernel + overlap kernel, 4 full-resolution bands (statistics pass,
  * quantising pass with the overlap, coefficient sum), 5 fused into the
  * tensor-core forward kernel (inverse choice 3), 6 low-resolution fields
- * whose sides are multiples of 16 but not powers of two (direct DFT). */
+ * whose sides are multiples of 16 but not powers of two (direct DFT),
+ * 7 full-resolution 64-point bands (512-wide fields, IFFT windows up to
+ * 64 x 64). */
 int digHoloB200GetInverseKernel(int handleIdx);
 /* Overlap of full-resolution fields: 0 (default) on the tensor cores in
  * split-BF16 precision (bf16 hi + lo of both int16 operands, three products,
